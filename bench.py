@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Benchmark: RK cell-updates/s (FP64) of the COREFL per-stage RHS + update.
+
+Workload: 3-D viscous single-species wave on a curvilinear single block of
+257^3 nodes (256^3 unique points, node-periodic in all directions),
+x = xi + 0.05 sin(2 pi eta) sin(2 pi zeta), rho = 1 + 0.01 sin(2 pi x), u = 1,
+p = 1/gamma, Sutherland viscosity at Re = 1000, WENO7 characteristic
+(inviscid_scheme 72) + second-order viscous flux, SSP-RK3 with the CFL step
+(CFL 0.5) computed on the device every step.  One "step" is one full
+three-stage RK3 step of the block; the metric counts nodes x steps / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's algorithm on the host cores (the CPU
+oracle, all threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "corefl-cpc_b200"))
+
+import numpy as np  # noqa: E402
+
+import cases  # noqa: E402
+
+METRIC = "RK cell-updates/s (FP64)"
+UNIT = "cell-updates/s"
+N_NODES = 257
+
+# Algorithmic FP64 operations of one WENO7 characteristic face flux (air) plus
+# its share of the staging and flux difference, counted from the arithmetic of
+# the restated routine (each +, -, *, /, sqrt = 1; fma = 2); derivation in
+# DESIGN.md.
+FLOPS_PER_FACE_WENO7_CH = 2980.0
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _upload(ctx, zone, case):
+    """Copy metric, jac and the initial bv of the case into the context's zone."""
+    for name, arr in (("metric", case.metric), ("jac", case.jac), ("bv", case.bv)):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        ctx.h2d(getattr(zone, name), a.ctypes.data, a.nbytes)
+    ctx.sync()
+
+
+def cpu_baseline_sample(target_s: float = 15.0, n: int = 49):
+    """The oracle (the reference's algorithm restated in C, OpenMP on all host
+    threads) on a bounded sample of the workload: the same wave and settings
+    on an n^3 block, stepped until ~target_s of CPU work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle  # test/baseline infrastructure only
+
+    case = cases.sine_wave(n=n, scheme=72, viscous=True, cfl=0.5)
+    z = pyoracle.OracleZone(case)
+    z.initialize()
+    z.step()  # warm
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < target_s:
+        z.step()
+        steps += 1
+    el = time.perf_counter() - t0
+    return {"value": case.N * steps / el, "unit": UNIT, "cores": int(pyoracle.lib().orc_num_threads()),
+            "kind": "port", "sample": f"{n}^3-node block of the same wave, WENO7-ch + viscous, {steps} RK3 steps "
+                                      f"in {el:.1f} s", "steps": steps, "seconds": el}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    # bounded sample per step, sized so that the whole run stays within minutes
+    total = max(args.steps + args.warmup, 1)
+    per = max(3.0, min(20.0, 150.0 / total))
+    res = cpu_baseline_sample(target_s=per * args.steps)
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(res["steps"], 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "3-D viscous sine wave, curvilinear periodic block, WENO7-ch + 2nd-order viscous, "
+                               "SSP-RK3 CFL 0.5", "nodes": f"{N_NODES}^3 (sampled on the host: 49^3)"},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_NODES, help="nodes per direction (default 257)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = _env_rank()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import corefl_b200 as cfk
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    else:
+        torch.cuda.set_device(0)
+
+    n = args.n
+    case = cases.sine_wave(n=n, scheme=72, viscous=True, cfl=0.5)
+    param = dict(case.param)
+    param["device"] = local
+    ctx = cfk.Context(param, case.faces)
+    zone = ctx.alloc_zone(case.mx, case.my, case.mz)
+    _upload(ctx, zone, case)
+    ctx.properties()
+    ctx.boundary_conditions()
+    ctx.properties()
+    ctx.cv_from_bv()
+    ctx.sync()
+
+    for _ in range(args.warmup):
+        ctx.rk3_step(want_dt=False)
+    ctx.sync()
+
+    # ---- timed region: K plain steps, phase events on the launching stream
+    ctx.set_profiling(True)
+    ctx.profile_read()  # clear
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.kernel_launches
+    with ClockSampler(local) as clk:
+        start.record()
+        for _ in range(args.steps):
+            ctx.rk3_step(want_dt=False)
+        stop.record()
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    launches = ctx.kernel_launches - launches0
+    phases = ctx.profile_read()
+    ctx.set_profiling(False)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    nodes = case.N
+    value = nodes * args.steps * world / (ms * 1e-3)
+
+    # ---- roofline of the dominant kernel (the three WENO sweeps)
+    inv_ms, inv_k = phases["inviscid"]
+    faces_per_launch = ((case.mx + 1) * case.my * case.mz + case.mx * (case.my + 1) * case.mz +
+                        case.mx * case.my * (case.mz + 1)) / 3.0
+    avg_launch_ms = inv_ms / max(inv_k, 1)
+    achieved = FLOPS_PER_FACE_WENO7_CH * faces_per_launch / (avg_launch_ms * 1e-3) / 1e12
+    peak = cfk.measure_fp64_peak()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "weno_air_traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get("bytes_per_launch_257")
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "weno_air_flux_diff<dir,7> (x/y/z sweeps)",
+                "peak_source": "measured live: cfk_measure_fp64_peak FMA-chain kernel",
+                "avg_launch_ms": avg_launch_ms, "flops_per_launch": FLOPS_PER_FACE_WENO7_CH * faces_per_launch}
+    hbm_peak = None
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        with open(mp) as f:
+            hbm_peak = json.load(f).get("hbm_gbs")
+
+    # ---- end to end through the C ABI with pinned host buffers
+    P = case.P
+    h2d_bytes = 6 * P * 8
+    d2h_bytes = 5 * P * 8
+    hb_ptr, hc_ptr = ctypes.c_void_p(), ctypes.c_void_p()
+    L = cfk.lib()
+    assert L.cfk_host_alloc(h2d_bytes, ctypes.byref(hb_ptr)) == 0
+    assert L.cfk_host_alloc(d2h_bytes, ctypes.byref(hc_ptr)) == 0
+    ctypes.memmove(hb_ptr, np.ascontiguousarray(case.bv).ctypes.data, h2d_bytes)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.sync()
+    e0.record()
+    for _ in range(args.e2e_steps):
+        ctx.h2d(zone.bv, hb_ptr, h2d_bytes)
+        ctx.cv_from_bv()
+        ctx.rk3_step(want_dt=False)
+        ctx.d2h(hc_ptr, zone.cv, d2h_bytes)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_e2e], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = {"value": nodes * args.e2e_steps * world / (ms_e2e * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+           "path": "cfk_memcpy_h2d(bv, pinned) + cfk_compute_cv_from_bv + cfk_rk3_step + cfk_memcpy_d2h(cv, pinned)"}
+    L.cfk_host_free(hb_ptr)
+    L.cfk_host_free(hc_ptr)
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline_sample()
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3-D viscous sine wave, curvilinear periodic block, WENO7-ch + 2nd-order "
+                                   "viscous, SSP-RK3 CFL 0.5 (device dt)", "nodes": f"{n}^3", "global_nodes": nodes * world,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cv alone "
+                       f"{5 * P * 8 / 1e6:.0f} MB)"},
+            "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "hbm_peak_gbs": hbm_peak,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,217 @@
+"""Input builders for the workloads of this library (host side, numpy).
+
+Each builder returns a :class:`Case`: ghost-padded node coordinates, the
+Jacobian and the nine metric terms in the reference's VectorField3D layout
+(reference src/gxl_lib/Array.cuh:246-322), the initial basic variables
+(rho, u, v, w, p, T) and the settings of the run.
+
+Grid metrics follow Block::compute_jac_metric (reference
+src/Mesh.cpp:244-300): second-order central differences of the coordinates,
+J = det(d(x,y,z)/d(xi,eta,zeta)) and grad(xi) etc. from the cofactors.  Ghost
+coordinates are point reflections through the boundary node (reference
+src/Mesh.cpp:1020-1076), with z(k) = k for 2-D blocks; one extra reflected
+layer lets the central differences reach the outermost ghost node.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+R_U = 8314.462618
+MW_AIR = 28.9647
+GAMMA_AIR = 1.4
+R_AIR = R_U / MW_AIR
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    mx: int
+    my: int
+    mz: int
+    ngg: int
+    metric: np.ndarray  # (9, P)
+    jac: np.ndarray  # (P,)
+    bv: np.ndarray  # (6, P)
+    sv: np.ndarray  # (n_scalar, P)
+    param: dict
+    faces: list  # [(face, direction, label)]
+    x: np.ndarray | None = None  # (P,) node x, for checks against exact solutions
+
+    @property
+    def P(self) -> int:
+        g = self.ngg
+        return (self.mx + 2 * g) * (self.my + 2 * g) * (self.mz + 2 * g)
+
+    @property
+    def N(self) -> int:
+        return self.mx * self.my * self.mz
+
+    def shape(self, g: int | None = None):
+        g = self.ngg if g is None else g
+        return (self.mz + 2 * g, self.my + 2 * g, self.mx + 2 * g)
+
+    def interior(self, a: np.ndarray) -> np.ndarray:
+        """View of the interior nodes of a padded plane, indexed [k, j, i]."""
+        g = self.ngg
+        return a.reshape(self.shape())[g:g + self.mz, g:g + self.my, g:g + self.mx]
+
+
+def _reflect_extend(c: np.ndarray, ext: int, axis: int, two_d_k: bool = False) -> np.ndarray:
+    """Extend a coordinate array by `ext` ghost layers on both sides of `axis`
+    by point reflection through the boundary node."""
+    n = c.shape[axis]
+    if two_d_k:
+        return c
+    lo = [2 * np.take(c, [0], axis=axis) - np.take(c, [q], axis=axis) for q in range(ext, 0, -1)]
+    hi = [2 * np.take(c, [n - 1], axis=axis) - np.take(c, [n - 1 - q], axis=axis) for q in range(1, ext + 1)]
+    return np.concatenate(lo + [c] + hi, axis=axis)
+
+
+def metrics(x: np.ndarray, y: np.ndarray, z: np.ndarray, ngg: int):
+    """Jacobian and metric on the padded grid from interior node coordinates
+    indexed [k, j, i].  Returns (jac (P,), metric (9, P), xg (P,))."""
+    mz, my, mx = x.shape
+    e = ngg + 1
+    coords = []
+    for c in (x, y, z):
+        c = _reflect_extend(c, e, 2)
+        c = _reflect_extend(c, e, 1)
+        if mz > 1:
+            c = _reflect_extend(c, e, 0)
+        coords.append(c)
+    X, Y, Z = coords
+    if mz == 1:
+        # 2-D block: z(k) = z(0) + k (reference src/Mesh.cpp:1066-1077)
+        ks = np.arange(-e, e + 1, dtype=np.float64)
+        X = np.repeat(X, 2 * e + 1, axis=0)
+        Y = np.repeat(Y, 2 * e + 1, axis=0)
+        Z = np.repeat(Z, 2 * e + 1, axis=0) + ks[:, None, None]
+
+    def d(a, axis):
+        sl_p = [slice(1, -1)] * 3
+        sl_m = [slice(1, -1)] * 3
+        sl_p[axis] = slice(2, None)
+        sl_m[axis] = slice(0, -2)
+        return (a[tuple(sl_p)] - a[tuple(sl_m)]) * 0.5
+
+    # derivative w.r.t. (xi, eta, zeta) = array axes (2, 1, 0)
+    dxd1, dyd1, dzd1 = d(X, 2), d(Y, 2), d(Z, 2)
+    dxd2, dyd2, dzd2 = d(X, 1), d(Y, 1), d(Z, 1)
+    dxd3, dyd3, dzd3 = d(X, 0), d(Y, 0), d(Z, 0)
+    jac = (dxd1 * dyd2 * dzd3 + dxd2 * dyd3 * dzd1 + dxd3 * dyd1 * dzd2 - dxd1 * dyd3 * dzd2 -
+           dxd2 * dyd1 * dzd3 - dxd3 * dyd2 * dzd1)
+    if np.any(jac <= 0):
+        raise ValueError("non-positive Jacobian in the generated grid")
+    m = np.empty((9,) + jac.shape)
+    m[0] = (dyd2 * dzd3 - dyd3 * dzd2) / jac
+    m[1] = (dxd3 * dzd2 - dxd2 * dzd3) / jac
+    m[2] = (dxd2 * dyd3 - dxd3 * dyd2) / jac
+    m[3] = (dyd3 * dzd1 - dyd1 * dzd3) / jac
+    m[4] = (dxd1 * dzd3 - dxd3 * dzd1) / jac
+    m[5] = (dxd3 * dyd1 - dxd1 * dyd3) / jac
+    m[6] = (dyd1 * dzd2 - dyd2 * dzd1) / jac
+    m[7] = (dxd2 * dzd1 - dxd1 * dzd2) / jac
+    m[8] = (dxd1 * dyd2 - dxd2 * dyd1) / jac
+    xg = X[1:-1, 1:-1, 1:-1]
+    return jac.reshape(-1).copy(), m.reshape(9, -1).copy(), xg.reshape(-1).copy()
+
+
+def _air_param(**kw) -> dict:
+    p = dict(dim=3, n_var=5, n_spec=0, n_scalar=0, n_reac=0, inviscid_scheme=72, reconstruction=2, limiter=0,
+             viscous_order=0, positive_preserving=0, gradPInDiffusionFlux=0, fixed_dt=0, chem_advance_method=0,
+             entropy_fix_factor=0.125, Pr=0.72, Sc=0.5, cfl=0.5, dt=0.0, weno_eps_scale=1.0, v_ref=1.0, rho_ref=1.0,
+             sensor_threshold=0.0)
+    p.update(kw)
+    return p
+
+
+def _reference_scale(rho: float, u: float, p: float) -> tuple[float, float]:
+    """rho_ref and v_ref of the reference state (reference src/BoundCond.cpp:274-283):
+    v_ref = |u|, or the speed of sound when |u| < 1."""
+    t = p * MW_AIR / (rho * R_U)
+    c = math.sqrt(GAMMA_AIR * R_U / MW_AIR * t)
+    v = abs(u) if abs(u) >= 1 else c
+    return rho, v
+
+
+def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5) -> Case:
+    """Sod shock tube on x in [0,1] as an nx-by-ny 2-D block (the reference
+    runs 1-D problems with 7 nodes in y), outflow on all four faces,
+    left (1,0,1) / right (0.125,0,0.1) split at x = 0.5 (the right state is
+    applied to x in [0.5, 1.5] inclusive, reference src/Field.cu:290)."""
+    ngg = 4 if scheme in (71, 72) else 3
+    xs = np.linspace(0.0, 1.0, nx)
+    ys = np.arange(ny) * 0.01
+    x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
+    y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
+    z = np.zeros_like(x)
+    jac, metric, xg = metrics(x, y, z, ngg)
+    P = jac.size
+    bv = np.zeros((6, P))
+    right = (xg >= 0.5) & (xg <= 1.5)
+    rho = np.where(right, 0.125, 1.0)
+    p = np.where(right, 0.1, 1.0)
+    bv[0] = rho
+    bv[4] = p
+    bv[5] = p * MW_AIR / (rho * R_U)
+    rho_ref, v_ref = _reference_scale(1.0, 0.0, 1.0)
+    param = _air_param(dim=2, inviscid_scheme=scheme, cfl=cfl, weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref,
+                       rho_ref=rho_ref)
+    faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
+    return Case("sod", nx, ny, 1, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg)
+
+
+def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float = 0.05, reynolds: float = 1000.0,
+              dt: float | None = None, cfl: float = 0.5, ny: int | None = None, nz: int | None = None) -> Case:
+    """3-D viscous single-species wave on a curvilinear periodic block:
+    x = xi + amp*sin(2 pi eta) sin(2 pi zeta), y = eta, z = zeta on [0,1]^3
+    with n nodes per direction (node-based periodicity: node 0 and node n-1
+    coincide, so n = 257 gives 256 unique points), rho = 1 + 0.01 sin(2 pi x),
+    u = 1, v = w = 0, p = 1/gamma.  The solver is dimensional with
+    Sutherland's law, so the length is scaled by L = Re * mu(T) / (rho U)
+    to give rho U L / mu = Re.  dt: fixed step; None means CFL-controlled."""
+    ny = n if ny is None else ny
+    nz = n if nz is None else nz
+    ngg = 4 if scheme in (71, 72) else 3
+    p0 = 1.0 / GAMMA_AIR
+    T0 = p0 * MW_AIR / (1.0 * R_U)
+    mu0 = 1.7894e-5 * (T0 / 288.16) ** 1.5 * (288.16 + 110) / (T0 + 110)
+    L = reynolds * mu0 / (1.0 * 1.0) if viscous else 1.0
+    xi = np.linspace(0.0, 1.0, n)
+    eta = np.linspace(0.0, 1.0, ny)
+    zeta = np.linspace(0.0, 1.0, nz)
+    Z3, Y3, X3 = np.meshgrid(zeta, eta, xi, indexing="ij")
+    x = (X3 + amp * np.sin(2 * np.pi * Y3) * np.sin(2 * np.pi * Z3)) * L
+    y = Y3 * L
+    z = Z3 * L
+    jac, metric, xg = metrics(x, y, z, ngg)
+    P = jac.size
+    bv = np.zeros((6, P))
+    xr = xg / L
+    bv[0] = 1.0 + 0.01 * np.sin(2 * np.pi * xr)
+    bv[1] = 1.0
+    bv[4] = p0
+    bv[5] = p0 * MW_AIR / (bv[0] * R_U)
+    rho_ref, v_ref = _reference_scale(1.0, 1.0, p0)
+    param = _air_param(dim=3, inviscid_scheme=scheme, viscous_order=2 if viscous else 0, cfl=cfl,
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref,
+                       fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
+    faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]
+    return Case("sine_wave", n, ny, nz, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg)
+
+
+def perturbed(case: Case, seed: int = 0, amp: float = 1e-3) -> Case:
+    """Copy of `case` with a seeded relative perturbation of rho, u, v, w, p so
+    that parity tests exercise every characteristic field."""
+    rng = np.random.default_rng(seed)
+    bv = case.bv.copy()
+    for l in range(5):
+        scale = np.abs(bv[l]).max() if np.abs(bv[l]).max() > 0 else 1.0
+        bv[l] = bv[l] + amp * scale * rng.standard_normal(bv[l].shape)
+    bv[0] = np.abs(bv[0])
+    bv[4] = np.abs(bv[4])
+    bv[5] = bv[4] * MW_AIR / (bv[0] * R_U)
+    return dataclasses.replace(case, bv=bv)

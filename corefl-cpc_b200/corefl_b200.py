@@ -1,0 +1,207 @@
+"""ctypes binding of libcorefl_b200.so (the C ABI declared in include/corefl_b200.h).
+
+The library is the product: every compute call goes to its sm_100a kernels.
+There is no fallback — if the shared library is missing or no CUDA device is
+present, loading or creating a context fails with an exception.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcorefl_b200.so")
+
+
+class cfk_face(ctypes.Structure):
+    _fields_ = [("face", ctypes.c_int), ("direction", ctypes.c_int), ("label", ctypes.c_int)]
+
+
+class cfk_param(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
+        ("n_reac", ctypes.c_int), ("inviscid_scheme", ctypes.c_int), ("reconstruction", ctypes.c_int),
+        ("limiter", ctypes.c_int), ("viscous_order", ctypes.c_int), ("positive_preserving", ctypes.c_int),
+        ("gradPInDiffusionFlux", ctypes.c_int), ("fixed_dt", ctypes.c_int), ("chem_advance_method", ctypes.c_int),
+        ("n_face", ctypes.c_int), ("faces", cfk_face * 6),
+        ("entropy_fix_factor", ctypes.c_double), ("Pr", ctypes.c_double), ("Sc", ctypes.c_double),
+        ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("weno_eps_scale", ctypes.c_double),
+        ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double), ("sensor_threshold", ctypes.c_double),
+        ("device", ctypes.c_int),
+    ]
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+class cfk_zone(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
+        (n, ctypes.c_void_p) for n in ("jac", "metric", "cv", "bv", "sv", "qn", "mul", "mach", "acoustic_speed",
+                                       "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
+                                       "dt_local", "Cn")
+    ]
+
+
+ZONE_FIELDS = [f for f, _ in cfk_zone._fields_[4:]]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the library once; raise if it is absent (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C corefl-cpc_b200` "
+                               "(or __graft_entry__.build()); there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        sigs = {
+            "cfk_create": (i, [ctypes.POINTER(cfk_param), ctypes.POINTER(vp)]),
+            "cfk_destroy": (i, [vp]),
+            "cfk_last_error": (ctypes.c_char_p, [vp]),
+            "cfk_param_from_setup": (i, [ctypes.c_char_p, ctypes.POINTER(cfk_param), ctypes.c_char_p, ctypes.c_size_t]),
+            "cfk_bind_zone": (i, [vp, ctypes.POINTER(cfk_zone)]),
+            "cfk_alloc_zone": (i, [vp, i, i, i, ctypes.POINTER(cfk_zone)]),
+            "cfk_compute_viscous_flux": (i, [vp, vp]),
+            "cfk_compute_inviscid_flux": (i, [vp, vp]),
+            "cfk_update_cv_and_bv_rk": (i, [vp, d, i, vp]),
+            "cfk_update_physical_properties": (i, [vp, vp]),
+            "cfk_compute_cv_from_bv": (i, [vp, vp]),
+            "cfk_apply_boundary_conditions": (i, [vp, vp]),
+            "cfk_local_time_step": (i, [vp, _DP, vp]),
+            "cfk_rk3_step": (i, [vp, _DP, vp]),
+            "cfk_rk3_step_graph": (i, [vp, _DP, vp]),
+            "cfk_memcpy_h2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
+            "cfk_memcpy_d2h": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
+            "cfk_stream_sync": (i, [vp, vp]),
+            "cfk_host_alloc": (i, [ctypes.c_size_t, ctypes.POINTER(vp)]),
+            "cfk_host_free": (i, [vp]),
+            "cfk_kernel_launches": (ctypes.c_longlong, [vp]),
+            "cfk_set_profiling": (i, [vp, i]),
+            "cfk_profile_read": (i, [vp, _DP, ctypes.POINTER(ctypes.c_longlong)]),
+            "cfk_measure_fp64_peak": (i, [_DP]),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def make_param(p: dict, faces) -> cfk_param:
+    cp = cfk_param()
+    for k, v in p.items():
+        if k in dict(cfk_param._fields_):
+            setattr(cp, k, v)
+    cp.n_face = len(faces)
+    for n, (f, dr, lab) in enumerate(faces):
+        cp.faces[n] = cfk_face(f, dr, lab)
+    return cp
+
+
+class CfkError(RuntimeError):
+    pass
+
+
+class Context:
+    """One solver context: settings, a bound zone, and the per-stage calls."""
+
+    def __init__(self, param: dict, faces):
+        self.L = lib()
+        self.cparam = make_param(param, faces)
+        h = ctypes.c_void_p()
+        rc = self.L.cfk_create(ctypes.byref(self.cparam), ctypes.byref(h))
+        if rc != 0:
+            raise CfkError(f"cfk_create failed with status {rc}")
+        self.h = h
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise CfkError(f"{what}: status {rc}: {self.L.cfk_last_error(self.h).decode()}")
+
+    def close(self):
+        if self.h:
+            self.L.cfk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bind(self, mx, my, mz, ngg, ptrs: dict):
+        z = cfk_zone(mx, my, mz, ngg)
+        for k, v in ptrs.items():
+            setattr(z, k, v)
+        self._ck(self.L.cfk_bind_zone(self.h, ctypes.byref(z)), "cfk_bind_zone")
+
+    def alloc_zone(self, mx, my, mz) -> cfk_zone:
+        z = cfk_zone()
+        self._ck(self.L.cfk_alloc_zone(self.h, mx, my, mz, ctypes.byref(z)), "cfk_alloc_zone")
+        return z
+
+    def viscous(self, stream=None):
+        self._ck(self.L.cfk_compute_viscous_flux(self.h, stream), "viscous")
+
+    def inviscid(self, stream=None):
+        self._ck(self.L.cfk_compute_inviscid_flux(self.h, stream), "inviscid")
+
+    def update_rk(self, dt, rk, stream=None):
+        self._ck(self.L.cfk_update_cv_and_bv_rk(self.h, dt, rk, stream), "update")
+
+    def properties(self, stream=None):
+        self._ck(self.L.cfk_update_physical_properties(self.h, stream), "properties")
+
+    def cv_from_bv(self, stream=None):
+        self._ck(self.L.cfk_compute_cv_from_bv(self.h, stream), "cv_from_bv")
+
+    def boundary_conditions(self, stream=None):
+        self._ck(self.L.cfk_apply_boundary_conditions(self.h, stream), "bc")
+
+    def local_time_step(self, stream=None) -> float:
+        dt = ctypes.c_double()
+        self._ck(self.L.cfk_local_time_step(self.h, ctypes.byref(dt), stream), "local_time_step")
+        return dt.value
+
+    def rk3_step(self, stream=None, graph=False, want_dt=True) -> float:
+        dt = ctypes.c_double(0.0)
+        fn = self.L.cfk_rk3_step_graph if graph else self.L.cfk_rk3_step
+        self._ck(fn(self.h, ctypes.byref(dt) if want_dt else None, stream), "rk3_step")
+        return dt.value
+
+    def sync(self, stream=None):
+        self._ck(self.L.cfk_stream_sync(self.h, stream), "sync")
+
+    def h2d(self, dst, src, nbytes, stream=None):
+        self._ck(self.L.cfk_memcpy_h2d(self.h, dst, src, nbytes, stream), "h2d")
+
+    def d2h(self, dst, src, nbytes, stream=None):
+        self._ck(self.L.cfk_memcpy_d2h(self.h, dst, src, nbytes, stream), "d2h")
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.L.cfk_kernel_launches(self.h))
+
+    def set_profiling(self, on: bool):
+        self._ck(self.L.cfk_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def profile_read(self) -> dict:
+        ms = (ctypes.c_double * NPHASE)()
+        kn = (ctypes.c_longlong * NPHASE)()
+        self._ck(self.L.cfk_profile_read(self.h, ms, kn), "profile_read")
+        return {name: (ms[k], kn[k]) for k, name in enumerate(PHASES)}
+
+
+PHASES = ("inviscid", "viscous", "update", "bc", "properties", "dt")
+NPHASE = len(PHASES)
+
+
+def measure_fp64_peak() -> float:
+    t = ctypes.c_double()
+    rc = lib().cfk_measure_fp64_peak(ctypes.byref(t))
+    if rc != 0:
+        raise CfkError(f"cfk_measure_fp64_peak failed with status {rc}")
+    return t.value

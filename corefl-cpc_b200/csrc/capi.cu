@@ -1,0 +1,448 @@
+// C ABI of the library: context, zone binding, per-stage entry points, whole
+// RK3 steps (plain and CUDA-graph replayed) and host<->device helpers.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cfk_common.cuh"
+#include "thermo.cuh"
+
+namespace cfk {
+cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t weno_air_init_attributes();
+cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
+                             int rk, int *err, cudaStream_t st);
+cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
+cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
+cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
+                            cudaStream_t st);
+cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
+                                       int n_face, cudaStream_t st, int *n_launch);
+}  // namespace cfk
+
+using namespace cfk;
+
+struct cfk_ctx {
+  cfk_param hp{};
+  Param p{};
+  Zone z{};
+  bool bound = false;
+  std::vector<void *> owned;  // device arrays owned by the context
+  Thermo *d_thermo = nullptr;
+  bool have_thermo = false;
+  // device scratch: [0] dt bits (u64), [1] error flags (int)
+  unsigned long long *d_dt_bits = nullptr;
+  int *d_err = nullptr;
+  long long launches = 0;
+  std::string err;
+  // CUDA graph of one RK3 step
+  cudaGraphExec_t graph_exec = nullptr;
+  long long graph_kernels = 0;
+  // phase timing with CUDA events (plain steps only)
+  bool profiling = false;
+  struct Rec { int phase; cudaEvent_t a, b; long long kernels; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t take_event() {
+    if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+};
+
+namespace {
+// Records the events of one phase around the launches issued in its scope.
+struct PhaseScope {
+  cfk_ctx *c;
+  int phase;
+  cudaStream_t st;
+  int *n;
+  int n0;
+  cudaEvent_t a = nullptr;
+  PhaseScope(cfk_ctx *c_, int ph, cudaStream_t s, int *n_) : c(c_), phase(ph), st(s), n(n_), n0(*n_) {
+    if (c->profiling) { a = c->take_event(); cudaEventRecord(a, st); }
+  }
+  ~PhaseScope() {
+    if (!c->profiling) return;
+    cudaEvent_t b = c->take_event();
+    cudaEventRecord(b, st);
+    c->recs.push_back({phase, a, b, (long long)(*n - n0)});
+  }
+};
+}  // namespace
+
+namespace {
+
+int fail(cfk_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(cfk_ctx *c, cudaError_t e, const char *where) {
+  return fail(c, CFK_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CFK_CHECK(ctx, call, where)                \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+  } while (0)
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int validate(const cfk_param *p, std::string &why) {
+  if (p->dim != 2 && p->dim != 3) { why = "dim must be 2 or 3"; return -1; }
+  if (p->n_spec < 0 || p->n_spec > kMaxSpec) { why = "n_spec out of range (0..9)"; return -1; }
+  if (p->n_var != 5 + p->n_scalar) { why = "n_var must equal 5 + n_scalar"; return -1; }
+  if (p->n_scalar < p->n_spec) { why = "n_scalar must be >= n_spec"; return -1; }
+  const int s = p->inviscid_scheme;
+  if (!(s == 52 || s == 72)) { why = "inviscid_scheme " + std::to_string(s) + " is not supported by this build"; return -1; }
+  if (p->viscous_order != 0 && p->viscous_order != 2) { why = "viscous_order must be 0 or 2"; return -1; }
+  if (p->sensor_threshold > 1e-10) { why = "hybrid shock-sensor schemes are not supported (shockSensor_threshold must be 0)"; return -1; }
+  if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
+  if (p->n_spec > 0) { why = "the mixture model needs cfk_set_mechanism (not in this build)"; return -1; }
+  if (p->n_face < 0 || p->n_face > 6) { why = "n_face must be 0..6"; return -1; }
+  for (int n = 0; n < p->n_face; ++n) {
+    const cfk_face &f = p->faces[n];
+    if (f.face < 0 || f.face > 2 || (f.direction != -1 && f.direction != 1) ||
+        !(f.label == 6 || f.label == 8 || f.label == 3)) {
+      why = "unsupported boundary face description";
+      return -1;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfk_create(const cfk_param *param, cfk_ctx **out) {
+  if (!param || !out) return CFK_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  if (validate(param, why) != 0) {
+    fprintf(stderr, "cfk_create: %s\n", why.c_str());
+    return CFK_ERR_ARG;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    fprintf(stderr, "cfk_create: no CUDA device (%s)\n", cudaGetErrorString(e));
+    return CFK_ERR_CUDA;
+  }
+  if (param->device < 0 || param->device >= ndev) {
+    fprintf(stderr, "cfk_create: device %d out of range (%d devices)\n", param->device, ndev);
+    return CFK_ERR_ARG;
+  }
+  e = cudaSetDevice(param->device);
+  if (e != cudaSuccess) return CFK_ERR_CUDA;
+  e = weno_air_init_attributes();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "cfk_create: kernel attribute setup failed (%s)\n", cudaGetErrorString(e));
+    return CFK_ERR_CUDA;
+  }
+  cfk_ctx *c = new cfk_ctx();
+  c->hp = *param;
+  Param &p = c->p;
+  p.dim = param->dim; p.n_var = param->n_var; p.n_spec = param->n_spec; p.n_scalar = param->n_scalar;
+  p.n_reac = param->n_reac; p.inviscid_scheme = param->inviscid_scheme; p.reconstruction = param->reconstruction;
+  p.limiter = param->limiter; p.viscous_order = param->viscous_order;
+  p.positive_preserving = param->positive_preserving; p.gradPInDiffusionFlux = param->gradPInDiffusionFlux;
+  p.fixed_dt = param->fixed_dt; p.entropy_fix_factor = param->entropy_fix_factor; p.Pr = param->Pr;
+  p.Sc = param->Sc; p.cfl = param->cfl; p.weno_eps_scale = param->weno_eps_scale; p.v_ref = param->v_ref;
+  p.rho_ref = param->rho_ref;
+  e = cudaMalloc(&c->d_dt_bits, 64);
+  if (e != cudaSuccess) { delete c; return CFK_ERR_CUDA; }
+  c->d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(c->d_dt_bits) + 8);
+  cudaMemset(c->d_dt_bits, 0, 64);
+  e = cudaMalloc(&c->d_thermo, sizeof(Thermo));
+  if (e != cudaSuccess) { cudaFree(c->d_dt_bits); delete c; return CFK_ERR_CUDA; }
+  cudaMemset(c->d_thermo, 0, sizeof(Thermo));
+  *out = c;
+  return CFK_OK;
+}
+
+int cfk_destroy(cfk_ctx *c) {
+  if (!c) return CFK_OK;
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  for (auto e : c->pool) cudaEventDestroy(e);
+  for (void *ptr : c->owned) cudaFree(ptr);
+  cudaFree(c->d_dt_bits);
+  cudaFree(c->d_thermo);
+  delete c;
+  return CFK_OK;
+}
+
+const char *cfk_last_error(const cfk_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
+  if (!c || !zn) return CFK_ERR_ARG;
+  if (zn->mx < 1 || zn->my < 1 || zn->mz < 1) return fail(c, CFK_ERR_ARG, "zone extents must be positive");
+  const int need_g = c->hp.inviscid_scheme == 72 ? 4 : 3;
+  if (zn->ngg < need_g) return fail(c, CFK_ERR_ARG, "ngg too small for the inviscid scheme");
+  if ((c->hp.dim == 2) != (zn->mz == 1)) return fail(c, CFK_ERR_ARG, "dim does not match mz");
+  if (!zn->cv || !zn->bv || !zn->qn || !zn->dq || !zn->metric || !zn->jac)
+    return fail(c, CFK_ERR_ARG, "cv, bv, qn, dq, metric and jac are required");
+  if (c->hp.viscous_order > 0 && !zn->mul) return fail(c, CFK_ERR_ARG, "mul is required for viscous runs");
+  if (c->hp.n_scalar > 0 && !zn->sv) return fail(c, CFK_ERR_ARG, "sv is required when n_scalar > 0");
+  // 32-bit plane extents, as in the reference's int indexing
+  const double P = (double)(zn->mx + 2 * zn->ngg) * (zn->my + 2 * zn->ngg) * (zn->mz + 2 * zn->ngg);
+  if (P * c->hp.n_var > 2147483647.0) return fail(c, CFK_ERR_ARG, "block too large for 32-bit plane indexing");
+  Zone &z = c->z;
+  z.d = Dims{zn->mx, zn->my, zn->mz, zn->ngg};
+  z.jac = zn->jac; z.metric = zn->metric; z.cv = zn->cv; z.bv = zn->bv; z.sv = zn->sv; z.qn = zn->qn;
+  z.mul = zn->mul; z.mach = zn->mach; z.acoustic_speed = zn->acoustic_speed; z.gamma = zn->gamma;
+  z.thermal_conductivity = zn->thermal_conductivity; z.rho_D = zn->rho_D;
+  z.reaction_timeScale = zn->reaction_timeScale; z.dq = zn->dq; z.dt_local = zn->dt_local; z.Cn = zn->Cn;
+  c->bound = true;
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  return CFK_OK;
+}
+
+int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
+  if (!c || !out) return CFK_ERR_ARG;
+  CFK_CHECK(c, cudaSetDevice(c->hp.device), "cudaSetDevice");
+  const int g = c->hp.inviscid_scheme == 72 ? 4 : 3;
+  cfk_zone zn{};
+  zn.mx = mx; zn.my = my; zn.mz = mz; zn.ngg = g;
+  const size_t P = (size_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g), N = (size_t)mx * my * mz;
+  const int nv = c->hp.n_var, ns = c->hp.n_spec, nsc = c->hp.n_scalar;
+  auto al = [&](double **ptr, size_t n) -> bool {
+    if (n == 0) { *ptr = nullptr; return true; }
+    void *v = nullptr;
+    if (cudaMalloc(&v, n * sizeof(double)) != cudaSuccess) return false;
+    cudaMemset(v, 0, n * sizeof(double));
+    c->owned.push_back(v);
+    *ptr = static_cast<double *>(v);
+    return true;
+  };
+  bool ok = al(&zn.jac, P) && al(&zn.metric, 9 * P) && al(&zn.cv, nv * P) && al(&zn.bv, 6 * P) &&
+            al(&zn.sv, nsc * P) && al(&zn.qn, nv * P) && al(&zn.mul, P) && al(&zn.mach, P) &&
+            al(&zn.dq, nv * N) && al(&zn.dt_local, N);
+  if (ok && ns > 0)
+    ok = al(&zn.acoustic_speed, P) && al(&zn.gamma, P) && al(&zn.thermal_conductivity, P) && al(&zn.rho_D, ns * P) &&
+         al(&zn.reaction_timeScale, P) && al(&zn.Cn, nv * N);
+  if (!ok) return fail(c, CFK_ERR_CUDA, "cudaMalloc failed in cfk_alloc_zone");
+  *out = zn;
+  return cfk_bind_zone(c, &zn);
+}
+
+#define NEED_ZONE(c)                                                              \
+  do {                                                                            \
+    if (!(c)) return CFK_ERR_ARG;                                                 \
+    if (!(c)->bound) return fail(c, CFK_ERR_STATE, "no zone bound");              \
+    CFK_CHECK(c, cudaSetDevice((c)->hp.device), "cudaSetDevice");                 \
+  } while (0)
+
+static const Thermo *thermo_of(cfk_ctx *c) { return c->have_thermo ? c->d_thermo : nullptr; }
+
+int cfk_compute_viscous_flux(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  if (c->hp.viscous_order == 0) return CFK_OK;
+  int n = 0;
+  CFK_CHECK(c, launch_viscous_air(c->z, c->p, S(stream), &n), "viscous flux");
+  c->launches += n;
+  return CFK_OK;
+}
+
+int cfk_compute_inviscid_flux(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  int n = 0;
+  CFK_CHECK(c, launch_weno_air(c->z, c->p, S(stream), &n), "inviscid flux");
+  c->launches += n;
+  return CFK_OK;
+}
+
+int cfk_update_cv_and_bv_rk(cfk_ctx *c, double dt, int rk, void *stream) {
+  NEED_ZONE(c);
+  if (rk < 0 || rk > 2) return fail(c, CFK_ERR_ARG, "rk must be 0, 1 or 2");
+  CFK_CHECK(c, launch_update_rk(c->z, c->p, thermo_of(c), dt, nullptr, rk, c->d_err, S(stream)), "update_cv_and_bv_rk");
+  c->launches += 1;
+  return CFK_OK;
+}
+
+int cfk_update_physical_properties(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  CFK_CHECK(c, launch_update_properties(c->z, c->p, thermo_of(c), S(stream)), "update_physical_properties");
+  c->launches += 1;
+  return CFK_OK;
+}
+
+int cfk_compute_cv_from_bv(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  CFK_CHECK(c, launch_cv_from_bv(c->z, c->p, thermo_of(c), S(stream)), "compute_cv_from_bv");
+  c->launches += 1;
+  return CFK_OK;
+}
+
+int cfk_apply_boundary_conditions(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  int n = 0;
+  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, S(stream), &n),
+            "boundary conditions");
+  c->launches += n;
+  return CFK_OK;
+}
+
+int cfk_local_time_step(cfk_ctx *c, double *dt_out, void *stream) {
+  NEED_ZONE(c);
+  CFK_CHECK(c, launch_local_dt(c->z, c->p, thermo_of(c), c->d_dt_bits, S(stream)), "local_time_step");
+  c->launches += 2;
+  if (dt_out) {
+    CFK_CHECK(c, cudaMemcpyAsync(dt_out, c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, S(stream)), "dt copy");
+    CFK_CHECK(c, cudaStreamSynchronize(S(stream)), "dt sync");
+  }
+  return CFK_OK;
+}
+
+// The body of one RK3 step, issued on one stream with no host synchronisation.
+static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
+  const Zone &z = c->z;
+  const Param &p = c->p;
+  const Thermo *th = thermo_of(c);
+  const size_t P = (size_t)z.d.plane(z.d.ngg), N = (size_t)z.d.plane(0);
+  int n = 0;
+  CFK_CHECK(c, cudaMemcpyAsync(z.qn, z.cv, P * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "qn copy");
+  const double *dt_dev = nullptr;
+  if (!p.fixed_dt) {
+    PhaseScope ps(c, CFK_PH_DT, st, &n);
+    CFK_CHECK(c, launch_local_dt(z, p, th, c->d_dt_bits, st), "local_time_step");
+    n += 2;
+    dt_dev = reinterpret_cast<const double *>(c->d_dt_bits);
+  }
+  for (int rk = 0; rk < 3; ++rk) {
+    CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
+    if (p.viscous_order == 2) {
+      PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
+      CFK_CHECK(c, launch_viscous_air(z, p, st, &n), "viscous flux");
+    }
+    {
+      PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
+      CFK_CHECK(c, launch_weno_air(z, p, st, &n), "inviscid flux");
+    }
+    {
+      PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
+      CFK_CHECK(c, launch_update_rk(z, p, th, c->hp.dt, dt_dev, rk, c->d_err, st), "update");
+      ++n;
+    }
+    {
+      PhaseScope ps(c, CFK_PH_BC, st, &n);
+      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, st, &n), "boundary conditions");
+    }
+    {
+      PhaseScope ps(c, CFK_PH_PROPS, st, &n);
+      CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
+      ++n;
+    }
+  }
+  c->launches += n;
+  return CFK_OK;
+}
+
+int cfk_rk3_step(cfk_ctx *c, double *dt_used, void *stream) {
+  NEED_ZONE(c);
+  int r = rk3_step_async(c, S(stream));
+  if (r != CFK_OK) return r;
+  if (dt_used) {
+    if (c->p.fixed_dt) *dt_used = c->hp.dt;
+    else {
+      CFK_CHECK(c, cudaMemcpyAsync(dt_used, c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, S(stream)), "dt copy");
+      CFK_CHECK(c, cudaStreamSynchronize(S(stream)), "dt sync");
+    }
+  }
+  return CFK_OK;
+}
+
+int cfk_rk3_step_graph(cfk_ctx *c, double *dt_used, void *stream) {
+  NEED_ZONE(c);
+  cudaStream_t st = S(stream);
+  if (!c->graph_exec) {
+    // capture on a private stream so that the caller's legacy stream is never in capture mode
+    cudaStream_t cap;
+    CFK_CHECK(c, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream");
+    cudaGraph_t graph;
+    CFK_CHECK(c, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const long long before = c->launches;
+    const bool prof = c->profiling;
+    c->profiling = false;
+    int r = rk3_step_async(c, cap);
+    c->profiling = prof;
+    cudaError_t e = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    c->graph_kernels = c->launches - before;
+    c->launches = before;
+    if (r != CFK_OK) return r;
+    if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
+    e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+  }
+  CFK_CHECK(c, cudaGraphLaunch(c->graph_exec, st), "graph launch");
+  c->launches += c->graph_kernels;
+  if (dt_used) {
+    if (c->p.fixed_dt) *dt_used = c->hp.dt;
+    else {
+      CFK_CHECK(c, cudaMemcpyAsync(dt_used, c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, st), "dt copy");
+      CFK_CHECK(c, cudaStreamSynchronize(st), "dt sync");
+    }
+  }
+  return CFK_OK;
+}
+
+int cfk_memcpy_h2d(cfk_ctx *c, void *dst, const void *src, size_t bytes, void *stream) {
+  CFK_CHECK(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S(stream)), "h2d");
+  return CFK_OK;
+}
+int cfk_memcpy_d2h(cfk_ctx *c, void *dst, const void *src, size_t bytes, void *stream) {
+  CFK_CHECK(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S(stream)), "d2h");
+  return CFK_OK;
+}
+int cfk_stream_sync(cfk_ctx *c, void *stream) {
+  CFK_CHECK(c, cudaStreamSynchronize(S(stream)), "stream sync");
+  int h_err = 0;
+  if (c && c->d_err) {
+    CFK_CHECK(c, cudaMemcpy(&h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag read");
+    if (h_err) {
+      cudaMemset(c->d_err, 0, sizeof(int));
+      return fail(c, CFK_ERR_NUMERIC, "temperature Newton iteration reached its 1000-iteration cap");
+    }
+  }
+  return CFK_OK;
+}
+int cfk_host_alloc(size_t bytes, void **out) {
+  if (!out) return CFK_ERR_ARG;
+  return cudaMallocHost(out, bytes) == cudaSuccess ? CFK_OK : CFK_ERR_CUDA;
+}
+int cfk_host_free(void *ptr) { return cudaFreeHost(ptr) == cudaSuccess ? CFK_OK : CFK_ERR_CUDA; }
+
+long long cfk_kernel_launches(const cfk_ctx *c) { return c ? c->launches : 0; }
+
+int cfk_set_profiling(cfk_ctx *c, int on) {
+  if (!c) return CFK_ERR_ARG;
+  c->profiling = on != 0;
+  return CFK_OK;
+}
+
+int cfk_profile_read(cfk_ctx *c, double *ms, long long *kernels) {
+  if (!c || !ms || !kernels) return CFK_ERR_ARG;
+  for (int k = 0; k < CFK_NPHASE; ++k) { ms[k] = 0; kernels[k] = 0; }
+  for (auto &r : c->recs) {
+    CFK_CHECK(c, cudaEventSynchronize(r.b), "profile sync");
+    float t = 0;
+    CFK_CHECK(c, cudaEventElapsedTime(&t, r.a, r.b), "profile elapsed");
+    ms[r.phase] += t;
+    kernels[r.phase] += r.kernels;
+    c->pool.push_back(r.a);
+    c->pool.push_back(r.b);
+  }
+  c->recs.clear();
+  return CFK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,409 @@
+// Node-local kernels of the stage: SSP-RK3 update, property update, cv from
+// bv, local CFL step with its grid minimum, boundary faces and the 2-D
+// k-ghost copy.  All are HBM-bound; each touches a node's planes once.
+#include "cfk_common.cuh"
+#include "thermo.cuh"
+
+namespace cfk {
+
+// SSP-RK3 coefficients (reference src/RK.cuh:11-15)
+__constant__ double kRkA[3] = {1.0, 0.75, 1.0 / 3.0};
+__constant__ double kRkB[3] = {0.0, 0.25, 2.0 / 3.0};
+__constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
+
+// ---------------------------------------------------------------------------
+// update_cv_and_bv_rk (reference src/RK.cuh:224-281).  dt comes from the
+// device scalar when dt_dev is non-null (CFL step computed on the device).
+// ---------------------------------------------------------------------------
+template <bool MIX>
+__global__ void __launch_bounds__(256) update_cv_and_bv_rk_kernel(Zone z, Param p, const Thermo *th, double dt_host,
+                                                                  const double *dt_dev, int rk, int *err) {
+  const Dims d = z.d;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  if (i >= d.mx) return;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), szq = d.plane(0);
+  const int64_t id = d.idx(g, i, j, k), iq = d.idx(0, i, j, k);
+  const double dt = dt_dev ? *dt_dev : dt_host;
+  const double a = kRkA[rk], b = kRkB[rk], c = kRkC[rk];
+  const double dt_div_jac = dt / z.jac[id];
+  double cvl[kMaxVar];
+  const int nv = p.n_var;
+#pragma unroll
+  for (int l = 0; l < 5; ++l) cvl[l] = a * z.qn[id + l * sz] + b * z.cv[id + l * sz] + c * dt_div_jac * z.dq[iq + l * szq];
+  if (MIX) {
+    for (int l = 5; l < nv; ++l)
+      cvl[l] = a * z.qn[id + l * sz] + b * z.cv[id + l * sz] + c * dt_div_jac * z.dq[iq + l * szq];
+  }
+  if (d.mz == 1) cvl[3] = 0;
+  const double rho = cvl[0];
+  const double density_inv = 1.0 / rho;
+  const double u = cvl[1] * density_inv, v = cvl[2] * density_inv, w = cvl[3] * density_inv;
+  z.bv[id] = rho;
+  z.bv[id + sz] = u;
+  z.bv[id + 2 * sz] = v;
+  z.bv[id + 3 * sz] = w;
+  const double V2 = u * u + v * v + w * w;
+  if (MIX) {
+    const int ns = p.n_spec;
+    double sum_part_den = 0;
+    for (int l = 0; l < ns; ++l) {
+      if (cvl[5 + l] < 0) cvl[5 + l] = 0;
+      else sum_part_den += cvl[5 + l];
+    }
+    sum_part_den = 1.0 / sum_part_den;
+    const double den_ratio = rho * sum_part_den;
+    double yk[kMaxSpec];
+    for (int l = 0; l < ns; ++l) {
+      yk[l] = cvl[5 + l] * sum_part_den;
+      z.sv[id + l * sz] = yk[l];
+      cvl[5 + l] *= den_ratio;
+    }
+    for (int l = ns; l < p.n_scalar; ++l) z.sv[id + l * sz] = cvl[5 + l] * density_inv;
+    double T = z.bv[id + 5 * sz];
+    double pres;
+    if (!temperature_newton(th, ns, yk, cvl[4], rho, V2, T, pres)) atomicOr(err, 1);
+    z.bv[id + 4 * sz] = pres;
+    z.bv[id + 5 * sz] = T;
+  } else {
+    const double pres = (kGammaAir - 1) * (cvl[4] - 0.5 * rho * V2);
+    z.bv[id + 4 * sz] = pres;
+    z.bv[id + 5 * sz] = pres * kMwAir * density_inv / kRu;
+  }
+  for (int l = 0; l < nv; ++l) z.cv[id + l * sz] = cvl[l];
+}
+
+// ---------------------------------------------------------------------------
+// cv from bv at one node (reference src/FieldOperation.cuh:16-37, 66-84)
+// ---------------------------------------------------------------------------
+template <bool MIX>
+__device__ __forceinline__ void cv_from_bv_point(const Zone &z, const Param &p, const Thermo *th, int64_t id) {
+  const int64_t sz = z.d.plane(z.d.ngg);
+  const double rho = z.bv[id], u = z.bv[id + sz], v = z.bv[id + 2 * sz], w = z.bv[id + 3 * sz];
+  z.cv[id] = rho;
+  z.cv[id + sz] = rho * u;
+  z.cv[id + 2 * sz] = rho * v;
+  z.cv[id + 3 * sz] = rho * w;
+  for (int l = 0; l < p.n_scalar; ++l) z.cv[id + (5 + l) * sz] = rho * z.sv[id + l * sz];
+  const double V2 = u * u + v * v + w * w;
+  double total_energy = 0.5 * V2;
+  if (MIX) {
+    double h[kMaxSpec];
+    compute_enthalpy(th, z.bv[id + 5 * sz], h);
+    for (int l = 0; l < p.n_spec; ++l) total_energy += h[l] * z.sv[id + l * sz];
+    total_energy *= rho;
+    total_energy -= z.bv[id + 4 * sz];
+  } else {
+    total_energy *= rho;
+    total_energy += z.bv[id + 4 * sz] / (kGammaAir - 1);
+  }
+  z.cv[id + 4 * sz] = total_energy;
+}
+
+template <bool MIX>
+__global__ void cv_from_bv_kernel(Zone z, Param p, const Thermo *th) {
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g;
+  const int j = blockIdx.y - g, k = blockIdx.z - g;
+  if (i >= d.mx + g) return;
+  cv_from_bv_point<MIX>(z, p, th, d.idx(g, i, j, k));
+}
+
+// ---------------------------------------------------------------------------
+// update_physical_properties (reference src/FieldOperation.cuh:86-120) over
+// the padded block.  The mixture branch also computes the mixture-averaged
+// transport properties (reference src/Transport.cu:43-165).
+// ---------------------------------------------------------------------------
+template <bool MIX>
+__global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo *th) {
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g;
+  const int j = blockIdx.y - g, k = blockIdx.z - g;
+  if (i >= d.mx + g) return;
+  const int64_t sz = d.plane(g);
+  const int64_t id = d.idx(g, i, j, k);
+  const double t = z.bv[id + 5 * sz];
+  const double V = norm3d(z.bv[id + sz], z.bv[id + 2 * sz], z.bv[id + 3 * sz]);
+  if (MIX) {
+    mixture_properties_point(z, p, th, id, t, V);
+  } else {
+    constexpr double c_temp = kGammaAir * kRu / kMwAir;
+    z.mul[id] = sutherland(t);
+    if (z.mach) z.mach[id] = V / sqrt(c_temp * t);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// local_time_step (reference src/TimeAdvanceFunc.cuh:28-115) fused with the
+// grid minimum of global_time_step (reference src/TimeAdvanceFunc.cu:102-152):
+// a warp/CTA min reduction and one atomicMin on the bit pattern (dt > 0, so
+// the unsigned order of the bits is the order of the values).
+// ---------------------------------------------------------------------------
+template <bool MIX>
+__global__ void __launch_bounds__(256) local_time_step_kernel(Zone z, Param p, const Thermo *th,
+                                                              unsigned long long *dt_min_bits) {
+  const Dims d = z.d;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  double dt = 1e6;
+  if (i < d.mx) {
+    const int g = d.ngg;
+    const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+    const double *mt = z.metric;
+    const int dim = d.mz == 1 ? 2 : 3;
+    const double grad_xi = norm3d(mt[id], mt[id + sz], mt[id + 2 * sz]);
+    const double grad_eta = norm3d(mt[id + 3 * sz], mt[id + 4 * sz], mt[id + 5 * sz]);
+    const double grad_zeta = norm3d(mt[id + 6 * sz], mt[id + 7 * sz], mt[id + 8 * sz]);
+    const double u = z.bv[id + sz], v = z.bv[id + 2 * sz], w = z.bv[id + 3 * sz];
+    const double U = u * mt[id] + v * mt[id + sz] + w * mt[id + 2 * sz];
+    const double V = u * mt[id + 3 * sz] + v * mt[id + 4 * sz] + w * mt[id + 5 * sz];
+    const double W = u * mt[id + 6 * sz] + v * mt[id + 7 * sz] + w * mt[id + 8 * sz];
+    double a;
+    if (MIX) a = z.acoustic_speed[id];
+    else a = sqrt(kGammaAir * kRAir * z.bv[id + 5 * sz]);
+    double msr = max(abs(U) + a * grad_xi, abs(V) + a * grad_eta);
+    if (dim == 3) msr = max(msr, abs(W) + a * grad_zeta);
+    if (p.viscous_order > 0) {
+      double max_length = max(grad_xi, grad_eta);
+      if (dim == 3) max_length = max(max_length, grad_zeta);
+      const double iRho = 1.0 / z.bv[id];
+      double mdv;
+      if (MIX) {
+        mdv = mixture_max_diffuse_vel(z, p, th, id, iRho);
+      } else {
+        mdv = max(kGammaAir, 4.0 / 3.0) * iRho;
+        mdv *= z.mul[id] / p.Pr;
+      }
+      msr = max(msr, max_length * max_length * mdv);
+    }
+    dt = p.cfl / msr;
+    if (MIX && p.n_reac > 0) {
+      const double reaction_dt = p.cfl * z.reaction_timeScale[id];
+      if (reaction_dt > 1e-20 && reaction_dt < 1e-5) dt = min(dt, reaction_dt);
+    }
+    if (z.dt_local) z.dt_local[d.idx(0, i, j, k)] = dt;
+  }
+  for (int o = 16; o > 0; o >>= 1) dt = min(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+  __shared__ double wmin[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) wmin[wid] = dt;
+  __syncthreads();
+  if (wid == 0) {
+    dt = lane < (int)(blockDim.x >> 5) ? wmin[lane] : 1e6;
+    for (int o = 4; o > 0; o >>= 1) dt = min(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+    if (lane == 0) atomicMin(dt_min_bits, (unsigned long long)__double_as_longlong(dt));
+  }
+}
+
+__global__ void reset_dt_kernel(unsigned long long *bits) { *bits = (unsigned long long)__double_as_longlong(1e6); }
+
+// ---------------------------------------------------------------------------
+// Boundary faces (reference src/BoundCond.cu:2002-2171, 3033-3080), each
+// over the face widened by ngg ghosts tangentially (reference
+// src/Mesh.cpp:14-31).  One thread per face node.
+// ---------------------------------------------------------------------------
+struct FaceGeom {
+  int face, direction;
+  int lo[3], n[3];  // range start and extent per axis
+};
+
+__device__ __forceinline__ void face_node(const FaceGeom &fg, int t, int &i, int &j, int &k) {
+  const int a = t % fg.n[0], r = t / fg.n[0];
+  const int b = r % fg.n[1], c = r / fg.n[1];
+  i = fg.lo[0] + a; j = fg.lo[1] + b; k = fg.lo[2] + c;
+}
+
+template <bool MIX>
+__global__ void bc_outflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
+  int i, j, k;
+  face_node(fg, t, i, j, k);
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+  const int64_t s = d.stride(g, fg.face) * fg.direction;
+  for (int gg = 1; gg <= g; ++gg) {
+    const int64_t gi = id + gg * s;
+    for (int l = 0; l < 6; ++l) z.bv[gi + l * sz] = z.bv[id + l * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[id + l * sz];
+    cv_from_bv_point<MIX>(z, p, th, gi);
+  }
+}
+
+template <bool MIX>
+__global__ void bc_symmetry_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
+  int i, j, k;
+  face_node(fg, t, i, j, k);
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+  const int64_t s = d.stride(g, fg.face) * fg.direction;
+  const int64_t in = id - s;
+  const int mf = 3 * fg.face;
+  double k_x = z.metric[id + mf * sz], k_y = z.metric[id + (mf + 1) * sz], k_z = z.metric[id + (mf + 2) * sz];
+  const double k_magnitude = sqrt(k_x * k_x + k_y * k_y + k_z * k_z);
+  k_x /= k_magnitude; k_y /= k_magnitude; k_z /= k_magnitude;
+  const double u1 = z.bv[in + sz], v1 = z.bv[in + 2 * sz], w1 = z.bv[in + 3 * sz];
+  double u_k = k_x * u1 + k_y * v1 + k_z * w1;
+  z.bv[id + sz] = u1 - k_x * u_k;
+  z.bv[id + 2 * sz] = v1 - k_y * u_k;
+  z.bv[id + 3 * sz] = w1 - k_z * u_k;
+  z.bv[id] = z.bv[in];
+  z.bv[id + 4 * sz] = z.bv[in + 4 * sz];
+  z.bv[id + 5 * sz] = z.bv[in + 5 * sz];
+  for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = z.sv[in + l * sz];
+  for (int gg = 1; gg <= g; ++gg) {
+    const int64_t gi = id + gg * s, ii = id - gg * s;
+    z.bv[gi] = z.bv[ii];
+    const double u = z.bv[ii + sz], v = z.bv[ii + 2 * sz], w = z.bv[ii + 3 * sz];
+    u_k = k_x * u + k_y * v + k_z * w;
+    z.bv[gi + sz] = u - 2 * u_k * k_x;
+    z.bv[gi + 2 * sz] = v - 2 * u_k * k_y;
+    z.bv[gi + 3 * sz] = w - 2 * u_k * k_z;
+    z.bv[gi + 4 * sz] = z.bv[ii + 4 * sz];
+    z.bv[gi + 5 * sz] = z.bv[ii + 5 * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[ii + l * sz];
+    cv_from_bv_point<MIX>(z, p, th, gi);
+  }
+}
+
+template <bool MIX>
+__global__ void bc_periodic_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
+  int i, j, k;
+  face_node(fg, t, i, j, k);
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+  const int64_t sd = d.stride(g, fg.face);
+  const int64_t s = sd * fg.direction;
+  const int mface = d.ext(fg.face);
+  const int64_t io = id + (int64_t)(fg.direction < 0 ? (mface - 1) : -(mface - 1)) * sd;
+  for (int l = 0; l < 6; ++l) {
+    const double ave = 0.5 * (z.bv[id + l * sz] + z.bv[io + l * sz]);
+    z.bv[id + l * sz] = ave;
+    z.bv[io + l * sz] = ave;
+  }
+  for (int l = 0; l < p.n_scalar; ++l) {
+    const double ave = 0.5 * (z.sv[id + l * sz] + z.sv[io + l * sz]);
+    z.sv[id + l * sz] = ave;
+    z.sv[io + l * sz] = ave;
+  }
+  cv_from_bv_point<MIX>(z, p, th, id);
+  for (int gg = 1; gg <= g; ++gg) {
+    const int64_t gi = id + gg * s, ii = io + gg * s;
+    for (int l = 0; l < 6; ++l) z.bv[gi + l * sz] = z.bv[ii + l * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[ii + l * sz];
+    cv_from_bv_point<MIX>(z, p, th, gi);
+  }
+}
+
+// eliminate_k_gradient (reference src/FieldOperation.cu:47-72)
+__global__ void eliminate_k_gradient_kernel(Zone z, Param p) {
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - g;
+  const int j = blockIdx.y - g;
+  if (i >= d.mx + g) return;
+  const int64_t sz = d.plane(g), i0 = d.idx(g, i, j, 0);
+  for (int k = 1; k <= g; ++k) {
+    const int64_t ip = d.idx(g, i, j, k), im = d.idx(g, i, j, -k);
+    for (int l = 0; l < 6; ++l) { z.bv[ip + l * sz] = z.bv[i0 + l * sz]; z.bv[im + l * sz] = z.bv[i0 + l * sz]; }
+    for (int l = 0; l < p.n_scalar; ++l) { z.sv[ip + l * sz] = z.sv[i0 + l * sz]; z.sv[im + l * sz] = z.sv[i0 + l * sz]; }
+    for (int l = 0; l < p.n_var; ++l) { z.cv[ip + l * sz] = z.cv[i0 + l * sz]; z.cv[im + l * sz] = z.cv[i0 + l * sz]; }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static dim3 interior_grid(const Dims &d, int tpb) { return dim3((d.mx + tpb - 1) / tpb, d.my, d.mz); }
+static dim3 padded_grid(const Dims &d, int tpb) {
+  return dim3((d.mx + 2 * d.ngg + tpb - 1) / tpb, d.my + 2 * d.ngg, d.mz + 2 * d.ngg);
+}
+
+cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
+                             int rk, int *err, cudaStream_t st) {
+  if (p.n_spec > 0) update_cv_and_bv_rk_kernel<true><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err);
+  else update_cv_and_bv_rk_kernel<false><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st) {
+  if (p.n_spec > 0) cv_from_bv_kernel<true><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
+  else cv_from_bv_kernel<false><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st) {
+  if (p.n_spec > 0) update_physical_properties_kernel<true><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
+  else update_physical_properties_kernel<false><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
+                            cudaStream_t st) {
+  reset_dt_kernel<<<1, 1, 0, st>>>(dt_bits);
+  if (p.n_spec > 0) local_time_step_kernel<true><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits);
+  else local_time_step_kernel<false><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits);
+  return cudaGetLastError();
+}
+
+static FaceGeom make_face(const Dims &d, const cfk_face &f) {
+  FaceGeom fg;
+  fg.face = f.face;
+  fg.direction = f.direction;
+  const int m[3] = {d.mx, d.my, d.mz};
+  for (int a = 0; a < 3; ++a) {
+    if (a == f.face) {
+      fg.lo[a] = f.direction < 0 ? 0 : m[a] - 1;
+      fg.n[a] = 1;
+    } else {
+      fg.lo[a] = -d.ngg;
+      fg.n[a] = m[a] + 2 * d.ngg;
+    }
+  }
+  if (d.mz == 1) { fg.lo[2] = -d.ngg; fg.n[2] = 2 * d.ngg + 1; }
+  return fg;
+}
+
+cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
+                                       int n_face, cudaStream_t st, int *n_launch) {
+  static const int order[3] = {6, 3, 8};  // outflow, symmetry, periodic (reference priority order)
+  for (int o = 0; o < 3; ++o) {
+    for (int n = 0; n < n_face; ++n) {
+      if (faces[n].label != order[o]) continue;
+      const FaceGeom fg = make_face(z.d, faces[n]);
+      const int cnt = fg.n[0] * fg.n[1] * fg.n[2];
+      const int blocks = (cnt + 127) / 128;
+      const bool mix = p.n_spec > 0;
+      if (order[o] == 6) {
+        if (mix) bc_outflow_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
+        else bc_outflow_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);
+      } else if (order[o] == 3) {
+        if (mix) bc_symmetry_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
+        else bc_symmetry_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);
+      } else {
+        if (mix) bc_periodic_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
+        else bc_periodic_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);
+      }
+      ++*n_launch;
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (z.d.mz == 1) {
+    eliminate_k_gradient_kernel<<<dim3((z.d.mx + 2 * z.d.ngg + 127) / 128, z.d.my + 2 * z.d.ngg), 128, 0, st>>>(z, p);
+    ++*n_launch;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace cfk

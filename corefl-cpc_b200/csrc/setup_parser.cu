@@ -1,0 +1,173 @@
+// Reader for the reference's setup.txt (host code).
+//
+// Grammar as in Parameter::read_one_file / read_struct (reference
+// src/Parameter.cpp:38-184): "type name = value" lines for int, real, bool and
+// string; "array type name = { ... }" spanning lines; "struct name { ... }"
+// blocks of typed entries closed by a lone "}".  Defaults follow
+// Parameter::setup_default_settings (reference src/Parameter.cpp:342-523) and
+// the derived quantities deduce_known_info (reference src/Parameter.cpp:186-340)
+// and the reference-state scaling of weno_eps_scale (reference
+// src/BoundCond.cpp:159-283, src/DParameter.cu:25-28).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <variant>
+#include <vector>
+
+#include "corefl_b200.h"
+
+namespace {
+
+using Value = std::variant<std::string, int, double>;
+using Struct = std::map<std::string, Value>;
+
+struct Setup {
+  std::map<std::string, int> ints;
+  std::map<std::string, double> reals;
+  std::map<std::string, bool> bools;
+  std::map<std::string, std::string> strings;
+  std::map<std::string, std::vector<std::string>> arrays;  // all arrays kept as tokens
+  std::map<std::string, Struct> structs;
+};
+
+bool starts_with(const std::string &s, const char *p) { return s.rfind(p, 0) == 0; }
+
+// Reads array tokens until "}"; returns false if the array continues on the next line.
+bool read_array_tokens(std::istringstream &line, std::vector<std::string> &out) {
+  std::string t;
+  while (line >> t) {
+    if (t == "}") return true;
+    if (t == "//") return false;
+    out.push_back(t);
+  }
+  return false;
+}
+
+bool next_line(std::ifstream &f, std::string &input, std::istringstream &line) {
+  while (std::getline(f, input)) {
+    if (input.empty() || starts_with(input, "//") || starts_with(input, "!")) continue;
+    line.clear();
+    line.str(input);
+    return true;
+  }
+  return false;
+}
+
+bool parse(const char *path, Setup &s, std::string &err) {
+  std::ifstream f(path);
+  if (!f) { err = std::string("cannot open ") + path; return false; }
+  std::string input;
+  std::istringstream line;
+  while (std::getline(f, input)) {
+    if (input.empty() || starts_with(input, "//") || starts_with(input, "!")) continue;
+    line.clear();
+    line.str(input);
+    std::string type, key, temp;
+    line >> type >> key >> temp;
+    if (type == "int") { int v = 0; line >> v; s.ints[key] = v; }
+    else if (type == "real") { double v = 0; line >> v; s.reals[key] = v; }
+    else if (type == "bool") { int v = 0; line >> v; s.bools[key] = v != 0; }
+    else if (type == "string") { std::string v; line >> v; s.strings[key] = v; }
+    else if (type == "array" || type == "range") {
+      const std::string name = temp;
+      line >> temp >> temp;  // "=" "{"
+      std::vector<std::string> toks;
+      while (!read_array_tokens(line, toks)) {
+        if (!next_line(f, input, line)) { err = "unterminated array " + name; return false; }
+      }
+      s.arrays[name] = toks;
+    } else if (type == "struct") {
+      Struct st;
+      while (next_line(f, input, line)) {
+        std::string k;
+        line >> k;
+        if (k == "}") break;
+        std::string n, eq;
+        if (k == "string") { std::string v; line >> n >> eq >> v; st.emplace(n, v); }
+        else if (k == "int") { int v = 0; line >> n >> eq >> v; st.emplace(n, v); }
+        else if (k == "real") { double v = 0; line >> n >> eq >> v; st.emplace(n, v); }
+      }
+      s.structs[key] = st;
+    }
+  }
+  return true;
+}
+
+template <class M, class V>
+V get(const M &m, const std::string &k, V dflt) {
+  auto it = m.find(k);
+  return it == m.end() ? dflt : static_cast<V>(it->second);
+}
+
+double struct_real(const Struct &st, const char *k, double dflt) {
+  auto it = st.find(k);
+  if (it == st.end()) return dflt;
+  if (auto p = std::get_if<double>(&it->second)) return *p;
+  if (auto p = std::get_if<int>(&it->second)) return *p;
+  return dflt;
+}
+
+}  // namespace
+
+extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char *errbuf, size_t err_len) {
+  auto report = [&](const std::string &m) {
+    if (errbuf && err_len) {
+      std::snprintf(errbuf, err_len, "%s", m.c_str());
+    }
+    return CFK_ERR_IO;
+  };
+  if (!setup_path || !out) return CFK_ERR_ARG;
+  Setup s;
+  std::string err;
+  if (!parse(setup_path, s, err)) return report(err);
+  cfk_param p;
+  std::memset(&p, 0, sizeof(p));
+  p.dim = get(s.ints, "dimension", 3);
+  p.inviscid_scheme = get(s.ints, "inviscid_scheme", 3);
+  p.reconstruction = get(s.ints, "reconstruction", 2);
+  p.limiter = get(s.ints, "limiter", 0);
+  p.viscous_order = get(s.ints, "viscous_order", 2);
+  p.positive_preserving = get(s.bools, "positive_preserving", false);
+  p.gradPInDiffusionFlux = get(s.bools, "gradPInDiffusionFlux", false);
+  p.fixed_dt = get(s.bools, "fixed_time_step", false);
+  p.chem_advance_method = get(s.ints, "chem_advance_method", 0);
+  p.entropy_fix_factor = get(s.reals, "entropy_fix_factor", 0.125);
+  p.Pr = get(s.reals, "prandtl_number", 0.72);
+  p.Sc = get(s.reals, "schmidt_number", 0.5);
+  p.cfl = get(s.reals, "cfl", 0.8);
+  p.dt = get(s.reals, "dt", 1e-8);
+  p.sensor_threshold = get(s.reals, "shockSensor_threshold", 0.0);
+  const int species = get(s.ints, "species", 0);
+  if (species != 0) return report("species != 0 needs a mechanism; pass n_spec/n_scalar explicitly");
+  p.n_spec = 0;
+  p.n_scalar = 0;
+  p.n_var = 5;
+  p.n_reac = 0;
+  // reference state -> rho_ref, v_ref (air)
+  const std::string ref = get(s.strings, "reference_state", std::string());
+  p.rho_ref = 1.0;
+  p.v_ref = 1.0;
+  auto it = s.structs.find(ref);
+  if (it != s.structs.end()) {
+    const Struct &st = it->second;
+    const double R_u = 8314.462618, mw = 28.9647, gamma = 1.4;
+    double mach = struct_real(st, "mach", -1), pressure = struct_real(st, "pressure", -1);
+    double temperature = struct_real(st, "temperature", -1), velocity = struct_real(st, "velocity", -1);
+    double density = struct_real(st, "density", -1);
+    if (temperature < 0) temperature = pressure * mw / (density * R_u);
+    const double c = std::sqrt(gamma * R_u / mw * temperature);
+    if (mach < 0) mach = velocity / c;
+    else velocity = mach * c;
+    if (density < 0) density = pressure * mw / (R_u * temperature);
+    p.rho_ref = density;
+    p.v_ref = std::fabs(velocity) < 1 ? c : velocity;
+  }
+  p.weno_eps_scale = p.rho_ref * p.v_ref * p.rho_ref * p.v_ref;
+  p.n_face = 0;
+  *out = p;
+  return CFK_OK;
+}

@@ -1,0 +1,162 @@
+/*
+ * corefl_b200 — B200 (sm_100a) implementation of the COREFL per-stage
+ * right-hand side and SSP-RK3 update, behind a plain C ABI.
+ *
+ * Every entry point returns 0 on success and a negative cfk_status on error;
+ * cfk_last_error() gives the message.  Streams are passed as void* so that a
+ * binder needs no CUDA headers (pass a cudaStream_t, or NULL for the legacy
+ * default stream).  All arrays are FP64 device pointers in the reference's
+ * ggxl::VectorField3D layout (reference src/gxl_lib/Array.cuh:246-322):
+ *
+ *   A(i,j,k,l) = a[(k+g)*(my+2g)*(mx+2g) + (j+g)*(mx+2g) + (i+g) + l*sz],
+ *   sz = (mx+2g)(my+2g)(mz+2g),
+ *
+ * g = ngg for cv, bv, sv, qn, metric, jac and the property arrays; g = 0 for
+ * dq, dt_local and Cn — the widths the reference allocates in
+ * Field::setup_device_memory (reference src/Field.cu:422-655).
+ */
+#ifndef COREFL_B200_H
+#define COREFL_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cfk_status {
+  CFK_OK = 0,
+  CFK_ERR_ARG = -1,      /* bad argument or unsupported setting */
+  CFK_ERR_CUDA = -2,     /* a CUDA call failed */
+  CFK_ERR_STATE = -3,    /* call out of order (e.g. no zone bound) */
+  CFK_ERR_NUMERIC = -4,  /* a bounded iteration gave up (see cfk_last_error) */
+  CFK_ERR_IO = -5        /* file could not be read or parsed */
+};
+
+typedef struct cfk_ctx cfk_ctx;
+
+/* A boundary face of the block (reference src/Mesh.cpp:14-31, Boundary).
+ * face 0/1/2 = i/j/k, direction -1 = min side, +1 = max side;
+ * label 6 = outflow, 8 = periodic, 3 = symmetry. */
+typedef struct cfk_face {
+  int face, direction, label;
+} cfk_face;
+
+/* Scalar settings of the path: the DParameter fields it reads
+ * (reference src/DParameter.cuh:13-207) plus the boundary list. */
+typedef struct cfk_param {
+  int dim;                 /* 2 or 3 */
+  int n_var;               /* 5 + n_scalar */
+  int n_spec;              /* 0 for the air model */
+  int n_scalar;
+  int n_reac;
+  int inviscid_scheme;     /* 2 Roe, 3 AUSM+, 4 HLLC (MUSCL/NND2/1st), 51/52/71/72 WENO */
+  int reconstruction;      /* 1 first order, 2 MUSCL, 3 NND2 */
+  int limiter;             /* 0 minmod, 1 van Leer */
+  int viscous_order;       /* 0 or 2 */
+  int positive_preserving;
+  int gradPInDiffusionFlux;
+  int fixed_dt;
+  int chem_advance_method; /* 0 explicit, 1 point implicit */
+  int n_face;
+  cfk_face faces[6];
+  double entropy_fix_factor;
+  double Pr, Sc, cfl, dt;
+  double weno_eps_scale;   /* (rho_ref * v_ref)^2, reference src/DParameter.cu:25-28 */
+  double v_ref, rho_ref;
+  double sensor_threshold; /* <= 1e-10: WENO nonlinear weights everywhere */
+  int device;              /* CUDA device ordinal the context runs on */
+} cfk_param;
+
+/* Device pointers of one block, field for field the arrays of the reference's
+ * DZone (reference src/Field.h:12-130) that this path reads or writes.
+ * Pointers a configuration does not use may be NULL. */
+typedef struct cfk_zone {
+  int mx, my, mz, ngg;
+  double *jac, *metric;          /* 1 and 9 planes, ngg ghosts */
+  double *cv, *bv, *sv, *qn;     /* n_var, 6, n_scalar, n_var planes, ngg ghosts */
+  double *mul, *mach;            /* ngg ghosts */
+  double *acoustic_speed, *gamma, *thermal_conductivity, *rho_D, *reaction_timeScale; /* mixture */
+  double *dq, *dt_local, *Cn;    /* n_var, 1, n_var planes, 0 ghosts */
+} cfk_zone;
+
+/* ---- context ---------------------------------------------------------- */
+int cfk_create(const cfk_param *param, cfk_ctx **out);
+int cfk_destroy(cfk_ctx *ctx);
+const char *cfk_last_error(const cfk_ctx *ctx);
+/* Fill a cfk_param from a reference setup.txt (reference src/Parameter.cpp:38-184,
+ * defaults :342-523, derived values :186-340).  Returns CFK_ERR_IO on failure. */
+int cfk_param_from_setup(const char *setup_path, cfk_param *out, char *err, size_t err_len);
+
+/* Adopt caller-owned device arrays in place, no copies (the reference's
+ * Field::d_ptr / h_ptr arrays). */
+int cfk_bind_zone(cfk_ctx *ctx, const cfk_zone *zone);
+/* Allocate a zone owned by the context (zero-filled) and bind it; its device
+ * pointers are returned in *zone_out. */
+int cfk_alloc_zone(cfk_ctx *ctx, int mx, int my, int mz, cfk_zone *zone_out);
+
+/* ---- per-stage entry points (each replaces the reference call named) ---- */
+/* dq += viscous flux differences.  Replaces compute_viscous_flux<M>
+ * (reference src/ViscousScheme.cu:7-73). */
+int cfk_compute_viscous_flux(cfk_ctx *ctx, void *stream);
+/* dq -= inviscid flux differences, all directions.  Replaces
+ * compute_inviscid_flux<M> (reference src/InviscidScheme.cu:12-26), including
+ * compute_convective_term_weno (reference src/WENO.cu:2914-2946). */
+int cfk_compute_inviscid_flux(cfk_ctx *ctx, void *stream);
+/* SSP-RK3 stage update of cv and bv/sv.  Replaces update_cv_and_bv_rk<M>
+ * (reference src/RK.cuh:224-281). */
+int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);
+/* Replaces update_physical_properties<M> (reference src/FieldOperation.cuh:86-120). */
+int cfk_update_physical_properties(cfk_ctx *ctx, void *stream);
+/* Replaces compute_cv_from_bv<M> (reference src/FieldOperation.cuh:39-64). */
+int cfk_compute_cv_from_bv(cfk_ctx *ctx, void *stream);
+/* Replaces DBoundCond::apply_boundary_conditions<M> for outflow, symmetry and
+ * periodic faces (reference src/BoundCond.cu:3489-3619) and, for 2-D blocks,
+ * eliminate_k_gradient (reference src/FieldOperation.cu:47-72). */
+int cfk_apply_boundary_conditions(cfk_ctx *ctx, void *stream);
+/* Local CFL step into dt_local and its minimum.  Replaces local_time_step<M>
+ * + global_time_step (reference src/TimeAdvanceFunc.cuh:28-115,
+ * src/TimeAdvanceFunc.cu:102-152).  *dt_out is written after a stream sync. */
+int cfk_local_time_step(cfk_ctx *ctx, double *dt_out, void *stream);
+
+/* ---- whole steps ------------------------------------------------------ */
+/* One SSP-RK3 step: qn <- cv, dt (fixed or CFL), three stages of
+ * dq = 0, viscous, inviscid, update, BCs, property update (the loop body of
+ * RK3, reference src/RK.cuh:84-212).  When the CFL step is used the dt stays
+ * on the device: no host round trip inside the step.  *dt_used (may be NULL)
+ * is read back only if non-NULL. */
+int cfk_rk3_step(cfk_ctx *ctx, double *dt_used, void *stream);
+/* Same step replayed from a CUDA graph captured on first use (the graph is
+ * rebuilt if the zone is re-bound). */
+int cfk_rk3_step_graph(cfk_ctx *ctx, double *dt_used, void *stream);
+
+/* ---- host <-> device helpers for callers without a CUDA runtime -------- */
+int cfk_memcpy_h2d(cfk_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes, void *stream);
+int cfk_memcpy_d2h(cfk_ctx *ctx, void *dst_host, const void *src_dev, size_t bytes, void *stream);
+int cfk_stream_sync(cfk_ctx *ctx, void *stream);
+/* pinned host buffers */
+int cfk_host_alloc(size_t bytes, void **out);
+int cfk_host_free(void *ptr);
+
+/* Number of kernels this context launched since creation (for accounting). */
+long long cfk_kernel_launches(const cfk_ctx *ctx);
+
+/* ---- measurement ------------------------------------------------------ */
+/* Phases of a step timed with CUDA events when profiling is on (plain steps
+ * only; graph replays are not instrumented). */
+enum cfk_phase {
+  CFK_PH_INVISCID = 0, CFK_PH_VISCOUS, CFK_PH_UPDATE, CFK_PH_BC, CFK_PH_PROPS, CFK_PH_DT, CFK_NPHASE
+};
+int cfk_set_profiling(cfk_ctx *ctx, int on);
+/* Synchronises the recorded events, writes the summed milliseconds and kernel
+ * counts per phase (arrays of CFK_NPHASE) and clears the record. */
+int cfk_profile_read(cfk_ctx *ctx, double *ms, long long *kernels);
+/* Achievable FP64 FMA throughput of the current device in TFLOP/s, measured
+ * with a register-resident FMA chain kernel (the roofline denominator of the
+ * FP64-bound kernels). */
+int cfk_measure_fp64_peak(double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

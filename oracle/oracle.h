@@ -1,0 +1,117 @@
+/*
+ * CPU oracle for the COREFL per-stage right-hand side and update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C (C99 + OpenMP) restatement of
+ * the reference solver's FP64 routines, written to follow the reference's
+ * arithmetic order so that the CUDA path can be checked against it.  Only the
+ * tests, the smoke check and the CPU-baseline leg of the benchmark may load
+ * it; the product library never links or calls it.
+ *
+ * Layout: every field is a ghost-padded, column-major structure of arrays in
+ * the reference's ggxl::VectorField3D form (src/gxl_lib/Array.cuh:246-322):
+ *   A(i,j,k,l) = a[(k+g)*(my+2g)*(mx+2g) + (j+g)*(mx+2g) + (i+g) + l*sz]
+ * with sz = (mx+2g)(my+2g)(mz+2g) and g the array's ghost width.
+ */
+#ifndef COREFL_ORACLE_H
+#define COREFL_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_MAX_SPEC 20
+#define ORC_MAX_REAC 64
+
+/* Boundary face description (reference src/Mesh.cpp:14-31 register_boundary):
+ * face 0/1/2 = i/j/k, direction -1 (min side) or +1 (max side),
+ * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = adiabatic wall. */
+typedef struct {
+  int face, direction, label;
+} orc_face;
+
+typedef struct {
+  int mx, my, mz, ngg;
+  /* arrays with ngg ghosts */
+  double *cv, *bv, *sv, *qn, *metric, *jac, *mul, *mach;
+  double *fFlux, *gFlux, *hFlux;
+  /* mixture-only arrays with ngg ghosts */
+  double *acoustic_speed, *gamma, *thermal_conductivity, *rho_D, *reaction_timeScale;
+  /* 0 ghosts */
+  double *dq, *dt_local, *Cn;
+  /* 1 ghost */
+  double *vis_flux;
+} orc_zone;
+
+/* Species / mechanism tables (reference src/DParameter.cuh:84-130). */
+typedef struct {
+  int n_spec, n_reac;
+  double mw[ORC_MAX_SPEC], imw[ORC_MAX_SPEC], gas_const[ORC_MAX_SPEC];
+  /* NASA-7 two-range polynomials, Combustion2Part branch (src/Thermo.cu:385-633) */
+  double t_low[ORC_MAX_SPEC], t_mid[ORC_MAX_SPEC], t_high[ORC_MAX_SPEC];
+  double low_coeff[ORC_MAX_SPEC][7], high_coeff[ORC_MAX_SPEC][7];
+  /* transport (src/Transport.cu:43-165) */
+  double geometry[ORC_MAX_SPEC], LJ_potent_inv[ORC_MAX_SPEC], vis_coeff[ORC_MAX_SPEC];
+  double WjDivWi_to_One4th[ORC_MAX_SPEC][ORC_MAX_SPEC];
+  double sqrt_WiDivWjPl1Mul8[ORC_MAX_SPEC][ORC_MAX_SPEC];
+  double binary_diffusivity_coeff[ORC_MAX_SPEC][ORC_MAX_SPEC];
+  double kb_over_eps_jk[ORC_MAX_SPEC][ORC_MAX_SPEC];
+  double ZRotF298[ORC_MAX_SPEC];
+  /* kinetics (src/FiniteRateChem.cu:1466-1605) */
+  int reac_type[ORC_MAX_REAC], rev_type[ORC_MAX_REAC];
+  int stoi_f[ORC_MAX_REAC][ORC_MAX_SPEC], stoi_b[ORC_MAX_REAC][ORC_MAX_SPEC];
+  int reac_order[ORC_MAX_REAC];
+  double A[ORC_MAX_REAC], b[ORC_MAX_REAC], Ea[ORC_MAX_REAC];
+  double A2[ORC_MAX_REAC], b2[ORC_MAX_REAC], Ea2[ORC_MAX_REAC];
+  double third_body_coeff[ORC_MAX_REAC][ORC_MAX_SPEC];
+  double troe_alpha[ORC_MAX_REAC], troe_t3[ORC_MAX_REAC], troe_t1[ORC_MAX_REAC], troe_t2[ORC_MAX_REAC];
+} orc_mech;
+
+typedef struct {
+  int dim, n_var, n_spec, n_scalar, n_reac;
+  int inviscid_scheme;   /* 2 Roe, 3 AUSM+, 4 HLLC, 51/52/71/72 WENO */
+  int reconstruction;    /* 1 first order, 2 MUSCL, 3 NND2 */
+  int limiter;           /* 0 minmod, 1 van Leer */
+  int viscous_order;     /* 0 inviscid, 2 second order */
+  int positive_preserving;
+  int gradPInDiffusionFlux;
+  double entropy_fix_factor;
+  double Pr, Sc, cfl, dt;
+  int fixed_dt;
+  double weno_eps_scale, v_ref, rho_ref;
+  double sensor_threshold;
+  int chem_advance_method;
+  int n_face;
+  orc_face faces[6];
+  const orc_mech *mech;  /* NULL for the calorically perfect air model */
+} orc_param;
+
+/* zone memory management (host, zero-filled) */
+int orc_zone_alloc(orc_zone *z, int mx, int my, int mz, int ngg, int n_var, int n_spec, int n_scalar);
+void orc_zone_free(orc_zone *z);
+
+/* building blocks (each cites its reference routine in oracle.c) */
+void orc_compute_cv_from_bv(orc_zone *z, const orc_param *p);
+void orc_update_physical_properties(orc_zone *z, const orc_param *p);
+void orc_local_time_step(orc_zone *z, const orc_param *p);
+double orc_global_time_step(const orc_zone *z);
+void orc_compute_inviscid_flux(orc_zone *z, const orc_param *p);
+void orc_compute_viscous_flux(orc_zone *z, const orc_param *p);
+void orc_update_cv_and_bv_rk(orc_zone *z, const orc_param *p, double dt, int rk);
+void orc_apply_boundary_conditions(orc_zone *z, const orc_param *p);
+void orc_eliminate_k_gradient(orc_zone *z, const orc_param *p);
+/* One SSP-RK3 step (reference src/RK.cuh:84-212); returns the dt used. */
+double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed);
+
+/* scalar WENO reconstructions (reference src/WENO.cu:3059-3222) */
+double orc_weno5(const double *vp, const double *vm, double eps, int if_shock);
+double orc_weno7(const double *vp, const double *vm, double eps, int if_shock);
+
+/* Sutherland viscosity (reference src/Transport.cu:6-9) */
+double orc_sutherland(double t);
+
+int orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,137 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the tests, the smoke check and the benchmark's CPU
+baseline use it as the checker.  The product (corefl-cpc_b200/) never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+class orc_face(ctypes.Structure):
+    _fields_ = [("face", ctypes.c_int), ("direction", ctypes.c_int), ("label", ctypes.c_int)]
+
+
+class orc_zone(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
+        (n, _DP) for n in ("cv", "bv", "sv", "qn", "metric", "jac", "mul", "mach", "fFlux", "gFlux", "hFlux",
+                           "acoustic_speed", "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
+                           "dt_local", "Cn", "vis_flux")
+    ]
+
+
+class orc_param(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
+        ("n_reac", ctypes.c_int), ("inviscid_scheme", ctypes.c_int), ("reconstruction", ctypes.c_int),
+        ("limiter", ctypes.c_int), ("viscous_order", ctypes.c_int), ("positive_preserving", ctypes.c_int),
+        ("gradPInDiffusionFlux", ctypes.c_int), ("entropy_fix_factor", ctypes.c_double), ("Pr", ctypes.c_double),
+        ("Sc", ctypes.c_double), ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("fixed_dt", ctypes.c_int),
+        ("weno_eps_scale", ctypes.c_double), ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double),
+        ("sensor_threshold", ctypes.c_double), ("chem_advance_method", ctypes.c_int), ("n_face", ctypes.c_int),
+        ("faces", orc_face * 6), ("mech", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-C", _HERE], check=True, capture_output=True)
+        L = ctypes.CDLL(LIB_PATH)
+        zp, pp = ctypes.POINTER(orc_zone), ctypes.POINTER(orc_param)
+        for name in ("orc_compute_cv_from_bv", "orc_update_physical_properties", "orc_local_time_step",
+                     "orc_compute_inviscid_flux", "orc_compute_viscous_flux", "orc_apply_boundary_conditions",
+                     "orc_eliminate_k_gradient"):
+            getattr(L, name).argtypes = [zp, pp]
+            getattr(L, name).restype = None
+        L.orc_update_cv_and_bv_rk.argtypes = [zp, pp, ctypes.c_double, ctypes.c_int]
+        L.orc_update_cv_and_bv_rk.restype = None
+        L.orc_rk3_step.argtypes = [zp, pp, ctypes.c_double]
+        L.orc_rk3_step.restype = ctypes.c_double
+        L.orc_global_time_step.argtypes = [zp]
+        L.orc_global_time_step.restype = ctypes.c_double
+        L.orc_weno5.argtypes = [_DP, _DP, ctypes.c_double, ctypes.c_int]
+        L.orc_weno5.restype = ctypes.c_double
+        L.orc_weno7.argtypes = [_DP, _DP, ctypes.c_double, ctypes.c_int]
+        L.orc_weno7.restype = ctypes.c_double
+        L.orc_sutherland.argtypes = [ctypes.c_double]
+        L.orc_sutherland.restype = ctypes.c_double
+        L.orc_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_DP)
+
+
+class OracleZone:
+    """Host arrays of one block in the reference layout, owned by numpy."""
+
+    def __init__(self, case):
+        c = case
+        g = c.ngg
+        nv = c.param["n_var"]
+        ns = max(c.param["n_spec"], 1)
+        nsc = max(c.param["n_scalar"], 1)
+        P, N = c.P, c.N
+        P1 = (c.mx + 2) * (c.my + 2) * (c.mz + 2)
+        self.case = c
+        self.arrays = {
+            "cv": np.zeros((nv, P)), "bv": c.bv.copy(), "sv": np.zeros((nsc, P)), "qn": np.zeros((nv, P)),
+            "metric": np.ascontiguousarray(c.metric), "jac": np.ascontiguousarray(c.jac), "mul": np.zeros(P),
+            "mach": np.zeros(P), "fFlux": np.zeros((nv, P)), "gFlux": np.zeros((nv, P)), "hFlux": np.zeros((nv, P)),
+            "acoustic_speed": np.zeros(P), "gamma": np.zeros(P), "thermal_conductivity": np.zeros(P),
+            "rho_D": np.zeros((ns, P)), "reaction_timeScale": np.zeros(P), "dq": np.zeros((nv, N)),
+            "dt_local": np.zeros(N), "Cn": np.zeros((nv, N)), "vis_flux": np.zeros((nv - 1, P1)),
+        }
+        if c.sv.shape[0]:
+            self.arrays["sv"][: c.sv.shape[0]] = c.sv
+        self.z = orc_zone(c.mx, c.my, c.mz, g)
+        for k, a in self.arrays.items():
+            setattr(self.z, k, _ptr(a))
+        self.p = orc_param()
+        for k, v in c.param.items():
+            if k in dict(orc_param._fields_):
+                setattr(self.p, k, v)
+        self.p.n_face = len(c.faces)
+        for n, (f, d, lab) in enumerate(c.faces):
+            self.p.faces[n] = orc_face(f, d, lab)
+        self.p.mech = None
+        self.L = lib()
+
+    def __getitem__(self, k):
+        return self.arrays[k]
+
+    def initialize(self):
+        """Start of a run: properties, BCs (+ 2-D k-ghost copy), properties
+        (reference src/Driver.cu:126-211), then cv from bv over the padded
+        block (reference src/RK.cuh:37-46)."""
+        zr, pr = ctypes.byref(self.z), ctypes.byref(self.p)
+        self.L.orc_update_physical_properties(zr, pr)
+        self.L.orc_apply_boundary_conditions(zr, pr)
+        if self.case.mz == 1:
+            self.L.orc_eliminate_k_gradient(zr, pr)
+        self.L.orc_update_physical_properties(zr, pr)
+        self.L.orc_compute_cv_from_bv(zr, pr)
+
+    def step(self) -> float:
+        return self.L.orc_rk3_step(ctypes.byref(self.z), ctypes.byref(self.p), self.p.dt)
+
+    def call(self, name, *args):
+        return getattr(self.L, name)(ctypes.byref(self.z), ctypes.byref(self.p), *args)

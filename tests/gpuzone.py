@@ -1,0 +1,77 @@
+"""Test helpers: device arrays of one block (torch allocations, reference
+layout) bound to a corefl_b200 context, and comparison utilities."""
+from __future__ import annotations
+
+import numpy as np
+
+import corefl_b200 as cfk
+
+
+class GpuZone:
+    def __init__(self, case, param_overrides=None):
+        import torch
+
+        self.torch = torch
+        self.case = case
+        p = dict(case.param)
+        if param_overrides:
+            p.update(param_overrides)
+        self.param = p
+        self.ctx = cfk.Context(p, case.faces)
+        c = case
+        nv, nsc, ns = p["n_var"], p["n_scalar"], p["n_spec"]
+        P, N = c.P, c.N
+        dev = torch.device("cuda:0")
+        z = lambda *s: torch.zeros(s, dtype=torch.float64, device=dev)
+        self.t = {
+            "jac": torch.from_numpy(np.ascontiguousarray(c.jac)).to(dev),
+            "metric": torch.from_numpy(np.ascontiguousarray(c.metric)).to(dev),
+            "cv": z(nv, P), "bv": torch.from_numpy(c.bv.copy()).to(dev), "qn": z(nv, P),
+            "mul": z(P), "mach": z(P), "dq": z(nv, N), "dt_local": z(N),
+        }
+        if nsc:
+            self.t["sv"] = torch.from_numpy(np.ascontiguousarray(c.sv)).to(dev) if c.sv.shape[0] else z(nsc, P)
+        if ns:
+            for k in ("acoustic_speed", "gamma", "thermal_conductivity", "reaction_timeScale"):
+                self.t[k] = z(P)
+            self.t["rho_D"] = z(ns, P)
+            self.t["Cn"] = z(nv, N)
+        self.ctx.bind(c.mx, c.my, c.mz, c.ngg, {k: v.data_ptr() for k, v in self.t.items()})
+
+    def initialize(self):
+        """properties, BCs (with the 2-D k-ghost copy), properties, cv from bv —
+        the same start-of-run sequence the oracle helper uses."""
+        self.ctx.properties()
+        self.ctx.boundary_conditions()
+        self.ctx.properties()
+        self.ctx.cv_from_bv()
+        self.torch.cuda.synchronize()
+
+    def get(self, k) -> np.ndarray:
+        self.torch.cuda.synchronize()
+        return self.t[k].cpu().numpy()
+
+    def load_from(self, oz):
+        """Copy the oracle's state arrays into the device arrays."""
+        for k in ("cv", "bv", "mul", "qn"):
+            self.t[k].copy_(self.torch.from_numpy(oz[k][: self.t[k].shape[0]]).to(self.t[k].device))
+        if "sv" in self.t:
+            self.t["sv"].copy_(self.torch.from_numpy(oz["sv"][: self.t["sv"].shape[0]]))
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    """max |a-b| over max |b|, per variable plane, maximised over planes."""
+    a = np.atleast_2d(a)
+    b = np.atleast_2d(b)
+    worst = 0.0
+    for l in range(b.shape[0]):
+        scale = np.abs(b[l]).max()
+        if scale == 0:
+            scale = 1.0
+        worst = max(worst, float(np.abs(a[l] - b[l]).max() / scale))
+    return worst
+
+
+def interior_planes(case, arr: np.ndarray) -> np.ndarray:
+    """Interior nodes of every plane of a padded (n, P) array, as (n, N)."""
+    return np.stack([case.interior(arr[l]).reshape(-1) for l in range(arr.shape[0])])
