@@ -59,13 +59,20 @@ class GpuZone:
             self.t["sv"].copy_(self.torch.from_numpy(oz["sv"][: self.t["sv"].shape[0]]))
 
 
-def rel_err(a: np.ndarray, b: np.ndarray) -> float:
-    """max |a-b| over max |b|, per variable plane, maximised over planes."""
+def rel_err(a: np.ndarray, b: np.ndarray, momentum=(1, 2, 3)) -> float:
+    """Normwise relative difference, maximised over variable planes:
+    max|a_l - b_l| / scale_l, where scale_l = max|b_l| except that the three
+    momentum planes share one scale (the largest of them), so that a
+    component that is zero up to round-off (v in a 1-D problem) is measured
+    against the momentum magnitude rather than against its own round-off.
+    Pass momentum=() for arrays that are not conserved-variable stacks."""
     a = np.atleast_2d(a)
     b = np.atleast_2d(b)
+    mom = [l for l in momentum if l < b.shape[0]]
+    mom_scale = max((np.abs(b[l]).max() for l in mom), default=0.0)
     worst = 0.0
     for l in range(b.shape[0]):
-        scale = np.abs(b[l]).max()
+        scale = mom_scale if l in mom else np.abs(b[l]).max()
         if scale == 0:
             scale = 1.0
         worst = max(worst, float(np.abs(a[l] - b[l]).max() / scale))
