@@ -106,6 +106,10 @@ int validate(const cfk_param *p, std::string &why) {
   if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
   if (p->n_spec > 0) { why = "the mixture model needs cfk_set_mechanism (not in this build)"; return -1; }
   if (p->n_face < 0 || p->n_face > 6) { why = "n_face must be 0..6"; return -1; }
+  // The WENO weights are normalised through products of two (eps + beta)^2
+  // terms; eps = 1e-40 * weno_eps_scale must stay above 1e-70 so that those
+  // products (>= eps^4) remain normal numbers.
+  if (!(p->weno_eps_scale >= 1e-30)) { why = "weno_eps_scale must be >= 1e-30 ((rho_ref*v_ref)^2)"; return -1; }
   for (int n = 0; n < p->n_face; ++n) {
     const cfk_face &f = p->faces[n];
     if (f.face < 0 || f.face > 2 || (f.direction != -1 && f.direction != 1) ||

@@ -1,41 +1,42 @@
 // Scalar WENO5-JS / WENO7-Z reconstructions of the split characteristic
-// fluxes at i+1/2.  Same formulas and evaluation order as the reference
-// (reference src/WENO.cu:3059-3222); vp[] runs upwind-left to right, vm[]
-// likewise, and the result is f+ + f-.
+// fluxes at i+1/2 (reference src/WENO.cu:3059-3222): same substencils,
+// smoothness indicators and weights; vp[] and vm[] run left to right and the
+// result is f+ + f-.  The weight normalisation is rearranged so that a face
+// costs one division per side pair instead of ten (WENO7) or six (WENO5).
 #pragma once
 
 namespace cfk {
 
-__device__ __forceinline__ double weno5_js(const double *vp, const double *vm, double eps) {
+// WENO5-JS, f+ + f-.  The weights a_k = d_k / (eps + beta_k)^2 enter only
+// through sum(a_k v_k) / sum(a_k); both sums are multiplied through by the
+// product of the three denominators, so one division per side remains.  The
+// sides are not merged into one division: in flat regions the products are
+// O(eps^4) and their cross product would underflow.  Same reconstruction as
+// the reference; the rounding differs at the ulp level.
+__device__ __forceinline__ void weno5_side(double u0, double u1, double u2, double u3, double u4, double eps,
+                                           double d0, double d1, double d2, double &num, double &den) {
   constexpr double one6th{1.0 / 6}, t12{13.0 / 12};
-  double v0 = one6th * (2 * vp[2] + 5 * vp[3] - vp[4]);
-  double v1 = one6th * (-vp[1] + 5 * vp[2] + 2 * vp[3]);
-  double v2 = one6th * (2 * vp[0] - 7 * vp[1] + 11 * vp[2]);
-  double d0 = vp[2] + vp[4] - 2 * vp[3], e0 = 3 * vp[2] - 4 * vp[3] + vp[4];
-  double d1 = vp[1] + vp[3] - 2 * vp[2], e1 = vp[1] - vp[3];
-  double d2 = vp[0] + vp[2] - 2 * vp[1], e2 = vp[0] - 4 * vp[1] + 3 * vp[2];
-  double beta0 = t12 * d0 * d0 + 0.25 * e0 * e0;
-  double beta1 = t12 * d1 * d1 + 0.25 * e1 * e1;
-  double beta2 = t12 * d2 * d2 + 0.25 * e2 * e2;
-  double a0 = 0.3 / ((eps + beta0) * (eps + beta0));
-  double a1 = 0.6 / ((eps + beta1) * (eps + beta1));
-  double a2 = 0.1 / ((eps + beta2) * (eps + beta2));
-  const double fPlus = (a0 * v0 + a1 * v1 + a2 * v2) / (a0 + a1 + a2);
+  const double v0 = one6th * (2 * u2 + 5 * u3 - u4);
+  const double v1 = one6th * (-u1 + 5 * u2 + 2 * u3);
+  const double v2 = one6th * (2 * u0 - 7 * u1 + 11 * u2);
+  const double g0 = u2 + u4 - 2 * u3, h0 = 3 * u2 - 4 * u3 + u4;
+  const double g1 = u1 + u3 - 2 * u2, h1 = u1 - u3;
+  const double g2 = u0 + u2 - 2 * u1, h2 = u0 - 4 * u1 + 3 * u2;
+  const double b0 = eps + (t12 * g0 * g0 + 0.25 * h0 * h0);
+  const double b1 = eps + (t12 * g1 * g1 + 0.25 * h1 * h1);
+  const double b2 = eps + (t12 * g2 * g2 + 0.25 * h2 * h2);
+  const double D0 = b0 * b0, D1 = b1 * b1, D2 = b2 * b2;
+  const double a0 = d0 * (D1 * D2), a1 = d1 * (D0 * D2), a2 = d2 * (D0 * D1);
+  num = a0 * v0 + a1 * v1 + a2 * v2;
+  den = a0 + a1 + a2;
+}
 
-  v0 = one6th * (11 * vm[2] - 7 * vm[3] + 2 * vm[4]);
-  v1 = one6th * (2 * vm[1] + 5 * vm[2] - vm[3]);
-  v2 = one6th * (-vm[0] + 5 * vm[1] + 2 * vm[2]);
-  d0 = vm[2] + vm[4] - 2 * vm[3]; e0 = 3 * vm[2] - 4 * vm[3] + vm[4];
-  d1 = vm[1] + vm[3] - 2 * vm[2]; e1 = vm[1] - vm[3];
-  d2 = vm[0] + vm[2] - 2 * vm[1]; e2 = vm[0] - 4 * vm[1] + 3 * vm[2];
-  beta0 = t12 * d0 * d0 + 0.25 * e0 * e0;
-  beta1 = t12 * d1 * d1 + 0.25 * e1 * e1;
-  beta2 = t12 * d2 * d2 + 0.25 * e2 * e2;
-  a0 = 0.1 / ((eps + beta0) * (eps + beta0));
-  a1 = 0.6 / ((eps + beta1) * (eps + beta1));
-  a2 = 0.3 / ((eps + beta2) * (eps + beta2));
-  const double fMinus = (a0 * v0 + a1 * v1 + a2 * v2) / (a0 + a1 + a2);
-  return fPlus + fMinus;
+__device__ __forceinline__ double weno5_js(const double *vp, const double *vm, double eps) {
+  double np, dp, nm, dm;
+  weno5_side(vp[0], vp[1], vp[2], vp[3], vp[4], eps, 0.3, 0.6, 0.1, np, dp);
+  // mirrored: minus-side substencil k is plus-side substencil 2-k, same linear weights
+  weno5_side(vm[4], vm[3], vm[2], vm[1], vm[0], eps, 0.3, 0.6, 0.1, nm, dm);
+  return np / dp + nm / dm;
 }
 
 __device__ __forceinline__ double weno7_beta(double s1, double s2, double s3) {
@@ -44,9 +45,11 @@ __device__ __forceinline__ double weno7_beta(double s1, double s2, double s3) {
 }
 
 // One side of WENO7-Z: u[0..6] ordered from the far upwind point to the far
-// downwind point of the stencil.
-__device__ __forceinline__ double weno7_z_side(double u0, double u1, double u2, double u3, double u4, double u5,
-                                               double u6, double eps) {
+// downwind point of the stencil.  Returns numerator and denominator of
+// sum(a_k v_k) / sum(a_k) with a_k = c_k (1 + tau / (eps + beta_k)^2); the
+// four reciprocals are formed from two divisions, 1/(D0 D1) and 1/(D2 D3).
+__device__ __forceinline__ void weno7_z_side(double u0, double u1, double u2, double u3, double u4, double u5,
+                                             double u6, double eps, double &num, double &den) {
   constexpr double one6th{1.0 / 6};
   constexpr double c0{1.0 / 35}, c1{12.0 / 35}, c2{18.0 / 35}, c3{4.0 / 35};
   double s1 = one6th * (-2 * u0 + 9 * u1 - 18 * u2 + 11 * u3);
@@ -67,22 +70,29 @@ __device__ __forceinline__ double weno7_z_side(double u0, double u1, double u2, 
   const double beta3 = weno7_beta(s1, s2, s3);
   double tau = beta0 + 3 * beta1 - 3 * beta2 - beta3;
   tau *= tau;
-  const double a0 = c0 + c0 * tau / ((eps + beta0) * (eps + beta0));
-  const double a1 = c1 + c1 * tau / ((eps + beta1) * (eps + beta1));
-  const double a2 = c2 + c2 * tau / ((eps + beta2) * (eps + beta2));
-  const double a3 = c3 + c3 * tau / ((eps + beta3) * (eps + beta3));
+  const double e0 = eps + beta0, e1 = eps + beta1, e2 = eps + beta2, e3 = eps + beta3;
+  const double D0 = e0 * e0, D1 = e1 * e1, D2 = e2 * e2, D3 = e3 * e3;
+  const double r01 = 1.0 / (D0 * D1), r23 = 1.0 / (D2 * D3);
+  const double a0 = c0 + c0 * tau * (D1 * r01);
+  const double a1 = c1 + c1 * tau * (D0 * r01);
+  const double a2 = c2 + c2 * tau * (D3 * r23);
+  const double a3 = c3 + c3 * tau * (D2 * r23);
   const double v0 = -3 * u0 + 13 * u1 - 23 * u2 + 25 * u3;
   const double v1 = u1 - 5 * u2 + 13 * u3 + 3 * u4;
   const double v2 = -u2 + 7 * u3 + 7 * u4 - u5;
   const double v3 = 3 * u3 + 13 * u4 - 5 * u5 + u6;
-  constexpr double one12th{1.0 / 12};
-  return one12th * (a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3) / (a0 + a1 + a2 + a3);
+  num = a0 * v0 + a1 * v1 + a2 * v2 + a3 * v3;
+  den = a0 + a1 + a2 + a3;
 }
 
+// f+ + f-, one division shared by the two sides (each sum(a_k) >= 1/35, so
+// the product of the two denominators cannot underflow).
 __device__ __forceinline__ double weno7_z(const double *vp, const double *vm, double eps) {
-  const double fPlus = weno7_z_side(vp[0], vp[1], vp[2], vp[3], vp[4], vp[5], vp[6], eps);
-  const double fMinus = weno7_z_side(vm[6], vm[5], vm[4], vm[3], vm[2], vm[1], vm[0], eps);
-  return fPlus + fMinus;
+  double np, dp, nm, dm;
+  weno7_z_side(vp[0], vp[1], vp[2], vp[3], vp[4], vp[5], vp[6], eps, np, dp);
+  weno7_z_side(vm[6], vm[5], vm[4], vm[3], vm[2], vm[1], vm[0], eps, nm, dm);
+  constexpr double one12th{1.0 / 12};
+  return one12th * ((np * dm + nm * dp) / (dp * dm));
 }
 
 }  // namespace cfk

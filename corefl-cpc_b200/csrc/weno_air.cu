@@ -51,7 +51,7 @@ struct AirTile {
 }  // namespace
 
 template <int DIR, int ORD>
-__global__ void __launch_bounds__(256, 1) weno_air_flux_diff(Zone z, double eps_ref) {
+__global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_ref) {
   using T = AirTile<DIR, ORD>;
   constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
   extern __shared__ double sm[];
@@ -160,8 +160,11 @@ __global__ void __launch_bounds__(256, 1) weno_air_flux_diff(Zone z, double eps_
     for (int q = 0; q < NPF; ++q) lam = max(lam, s[T::spt(12, c, t + q)]);
 
     double fChar[5];
-#pragma unroll 1
+#pragma unroll
     for (int l = 0; l < 5; ++l) {
+      // keep the stencil in shared memory across the five fields instead of
+      // letting the compiler hoist all 2R+2 points into registers
+      asm volatile("" ::: "memory");
       double L0, L1, L2, L3, L4;
       if (l == 0) {
         L0 = (alpha + Uk_bar * cm) * ic2 * 0.5;
