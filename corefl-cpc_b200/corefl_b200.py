@@ -81,6 +81,8 @@ def lib() -> ctypes.CDLL:
             "cfk_set_profiling": (i, [vp, i]),
             "cfk_profile_read": (i, [vp, _DP, ctypes.POINTER(ctypes.c_longlong)]),
             "cfk_measure_fp64_peak": (i, [_DP]),
+            "cfk_local_time_step_static": (i, [ctypes.POINTER(cfk_param), ctypes.POINTER(cfk_zone), vp, vp,
+                                               ctypes.c_char_p, ctypes.c_size_t]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)

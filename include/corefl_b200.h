@@ -141,6 +141,21 @@ int cfk_host_free(void *ptr);
 /* Number of kernels this context launched since creation (for accounting). */
 long long cfk_kernel_launches(const cfk_ctx *ctx);
 
+/* ---- allocation-free variant ------------------------------------------- */
+/* No counterpart in the reference.  The local CFL step (dt_local and its grid
+ * minimum, written to *dt_min_device) for callers that cannot call
+ * cudaMalloc: a host that is itself building a CUDA graph, a memory-pool
+ * policy that forbids allocation after start-up, or a framework that owns all
+ * device memory.  It needs no context and allocates nothing: its scratch (one
+ * partial minimum per 256-node row segment, ceil(mx/256)*my*mz <= 262144, i.e.
+ * 2 MiB) is a file-scope device array that every GPU loading the library holds
+ * until exit.  The first call on a device looks up that array's device address
+ * (do it before any stream capture).  Calls share the scratch: calls that
+ * overlap on the GPU race.  Air model only; larger zones are rejected with
+ * CFK_ERR_ARG and a message in err. */
+int cfk_local_time_step_static(const cfk_param *param, const cfk_zone *zone, double *dt_min_device, void *stream,
+                               char *err, size_t err_len);
+
 /* ---- measurement ------------------------------------------------------ */
 /* Phases of a step timed with CUDA events when profiling is on (plain steps
  * only; graph replays are not instrumented). */
