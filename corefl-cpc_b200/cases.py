@@ -39,6 +39,7 @@ class Case:
     param: dict
     faces: list  # [(face, direction, label)]
     x: np.ndarray | None = None  # (P,) node x, for checks against exact solutions
+    mech: object = None  # mechanism.Mechanism for the mixture model
 
     @property
     def P(self) -> int:
@@ -215,3 +216,65 @@ def perturbed(case: Case, seed: int = 0, amp: float = 1e-3) -> Case:
     bv[4] = np.abs(bv[4])
     bv[5] = bv[4] * MW_AIR / (bv[0] * R_U)
     return dataclasses.replace(case, bv=bv)
+
+
+def _mix_param(mech, **kw) -> dict:
+    ns = mech.n_spec
+    p = _air_param(n_spec=ns, n_scalar=ns, n_var=5 + ns, n_reac=mech.n_reac, chem_advance_method=1)
+    p.update(kw)
+    return p
+
+
+def mole_to_mass(mech, X: np.ndarray) -> np.ndarray:
+    """Mole fractions -> mass fractions with the mechanism's weights (last axis)."""
+    W = mech.mw
+    num = X * W
+    return num / num.sum(axis=-1, keepdims=True)
+
+
+def reactor(mech, T, p, X, ngg: int = 0) -> Case:
+    """Batch of independent constant-volume 0-D reactors (one per node of an
+    n x 1 x 1 block, zero ghosts by default): rest state, temperature T [K],
+    pressure p [Pa], mole fractions X (n x ns).  Metric and Jacobian are those
+    of a unit cell; Cn = 0 so the Wu reaction step is a pure 0-D integration."""
+    T = np.atleast_1d(np.asarray(T, dtype=np.float64))
+    p = np.broadcast_to(np.asarray(p, dtype=np.float64), T.shape).copy()
+    X = np.atleast_2d(np.asarray(X, dtype=np.float64))
+    X = np.broadcast_to(X, (T.size, mech.n_spec)).copy()
+    n = T.size
+    Y = mole_to_mass(mech, X)
+    W = 1.0 / (Y / mech.mw).sum(axis=1)
+    rho = p * W / (R_U * T)
+    P = (n + 2 * ngg) * (1 + 2 * ngg) * (1 + 2 * ngg)
+    shape = (1 + 2 * ngg, 1 + 2 * ngg, n + 2 * ngg)
+
+    def pad(a):
+        out = np.empty(shape)
+        out[...] = np.pad(a[None, None, :], ((ngg, ngg), (ngg, ngg), (ngg, ngg)), mode="edge")
+        return out.reshape(-1)
+
+    bv = np.zeros((6, P))
+    bv[0] = pad(rho)
+    bv[4] = pad(p)
+    bv[5] = pad(T)
+    sv = np.stack([pad(Y[:, l]) for l in range(mech.n_spec)])
+    metric = np.zeros((9, P))
+    metric[0] = metric[4] = metric[8] = 1.0
+    jac = np.ones(P)
+    param = _mix_param(mech, dim=2 if True else 3, inviscid_scheme=0, cfl=0.5)
+    return Case("reactor", n, 1, 1, ngg, metric, jac, bv, sv, param, [], mech=mech)
+
+
+def reactor_batch(mech, n: int, seed: int = 0) -> Case:
+    """Seeded batch of H2/air reactors: T ~ U[1000, 1600] K, p log-uniform in
+    [1, 10] atm, equivalence ratio ~ U[0.5, 2], H2 : O2 : N2 = 2 phi : 1 : 3.76."""
+    rng = np.random.default_rng(seed)
+    T = rng.uniform(1000.0, 1600.0, n)
+    p = 101325.0 * np.exp(rng.uniform(0.0, np.log(10.0), n))
+    phi = rng.uniform(0.5, 2.0, n)
+    X = np.zeros((n, mech.n_spec))
+    X[:, mech.index("H2")] = 2 * phi
+    X[:, mech.index("O2")] = 1.0
+    X[:, mech.index("N2")] = 3.76
+    X /= X.sum(axis=1, keepdims=True)
+    return reactor(mech, T, p, X)

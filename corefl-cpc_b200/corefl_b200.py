@@ -33,6 +33,65 @@ class cfk_param(ctypes.Structure):
 
 _DP = ctypes.POINTER(ctypes.c_double)
 
+MAX_SPEC, MAX_REAC = 9, 24
+
+
+class cfk_mechanism(ctypes.Structure):
+    _fields_ = [
+        ("n_spec", ctypes.c_int), ("n_reac", ctypes.c_int), ("mw", ctypes.c_double * MAX_SPEC),
+        ("t_low", ctypes.c_double * MAX_SPEC), ("t_mid", ctypes.c_double * MAX_SPEC),
+        ("t_high", ctypes.c_double * MAX_SPEC), ("low", (ctypes.c_double * 7) * MAX_SPEC),
+        ("high", (ctypes.c_double * 7) * MAX_SPEC), ("geometry", ctypes.c_int * MAX_SPEC),
+        ("LJ_potent_inv", ctypes.c_double * MAX_SPEC), ("vis_coeff", ctypes.c_double * MAX_SPEC),
+        ("ZRotF298", ctypes.c_double * MAX_SPEC),
+        ("WjDivWi_to_One4th", (ctypes.c_double * MAX_SPEC) * MAX_SPEC),
+        ("sqrt_WiDivWjPl1Mul8", (ctypes.c_double * MAX_SPEC) * MAX_SPEC),
+        ("binary_diffusivity_coeff", (ctypes.c_double * MAX_SPEC) * MAX_SPEC),
+        ("kb_over_eps_jk", (ctypes.c_double * MAX_SPEC) * MAX_SPEC),
+        ("reac_type", ctypes.c_int * MAX_REAC), ("rev_type", ctypes.c_int * MAX_REAC),
+        ("order", ctypes.c_int * MAX_REAC),
+        ("stoi_f", (ctypes.c_int * MAX_SPEC) * MAX_REAC), ("stoi_b", (ctypes.c_int * MAX_SPEC) * MAX_REAC),
+        ("A", ctypes.c_double * MAX_REAC), ("b", ctypes.c_double * MAX_REAC), ("Ea", ctypes.c_double * MAX_REAC),
+        ("A2", ctypes.c_double * MAX_REAC), ("b2", ctypes.c_double * MAX_REAC), ("Ea2", ctypes.c_double * MAX_REAC),
+        ("third_body_coeff", (ctypes.c_double * MAX_SPEC) * MAX_REAC),
+        ("troe_alpha", ctypes.c_double * MAX_REAC), ("troe_t3", ctypes.c_double * MAX_REAC),
+        ("troe_t1", ctypes.c_double * MAX_REAC), ("troe_t2", ctypes.c_double * MAX_REAC),
+    ]
+
+
+def make_mechanism(m) -> cfk_mechanism:
+    """cfk_mechanism from a mechanism.Mechanism table."""
+    o = cfk_mechanism()
+    o.n_spec, o.n_reac = m.n_spec, m.n_reac
+
+    def f1(name, vals, src=None):
+        arr = getattr(o, name)
+        for i, v in enumerate(vals):
+            arr[i] = v
+
+    def f2(name, vals):
+        arr = getattr(o, name)
+        for i in range(vals.shape[0]):
+            for j in range(vals.shape[1]):
+                arr[i][j] = vals[i, j]
+
+    for k in ("mw", "t_low", "t_mid", "t_high", "LJ_potent_inv", "vis_coeff", "ZRotF298"):
+        f1(k, getattr(m, k))
+    f1("geometry", [int(v) for v in m.geometry])
+    f2("low", m.low)
+    f2("high", m.high)
+    for k in ("WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8", "binary_diffusivity_coeff", "kb_over_eps_jk"):
+        f2(k, getattr(m, k))
+    f1("reac_type", m.reac_type)
+    f1("rev_type", m.rev_type)
+    f1("order", m.order)
+    f2("stoi_f", m.stoi_f)
+    f2("stoi_b", m.stoi_b)
+    for k in ("A", "b", "Ea", "A2", "b2", "Ea2", "troe_alpha", "troe_t3", "troe_t1", "troe_t2"):
+        f1(k, getattr(m, k))
+    f2("third_body_coeff", m.third_body_coeff)
+    return o
+
 
 class cfk_zone(ctypes.Structure):
     _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
@@ -83,6 +142,9 @@ def lib() -> ctypes.CDLL:
             "cfk_measure_fp64_peak": (i, [_DP]),
             "cfk_local_time_step_static": (i, [ctypes.POINTER(cfk_param), ctypes.POINTER(cfk_zone), vp, vp,
                                                ctypes.c_char_p, ctypes.c_size_t]),
+            "cfk_set_mechanism": (i, [vp, ctypes.POINTER(cfk_mechanism)]),
+            "cfk_finite_rate_chemistry": (i, [vp, vp]),
+            "cfk_wu_reaction_step": (i, [vp, d, i, vp, vp]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -144,6 +206,16 @@ class Context:
         z = cfk_zone()
         self._ck(self.L.cfk_alloc_zone(self.h, mx, my, mz, ctypes.byref(z)), "cfk_alloc_zone")
         return z
+
+    def set_mechanism(self, mech):
+        self._mech = make_mechanism(mech)
+        self._ck(self.L.cfk_set_mechanism(self.h, ctypes.byref(self._mech)), "cfk_set_mechanism")
+
+    def finite_rate_chemistry(self, stream=None):
+        self._ck(self.L.cfk_finite_rate_chemistry(self.h, stream), "finite_rate_chemistry")
+
+    def wu_reaction_step(self, dt, schedule=0, nsub_ptr=None, stream=None):
+        self._ck(self.L.cfk_wu_reaction_step(self.h, dt, schedule, nsub_ptr, stream), "wu_reaction_step")
 
     def viscous(self, stream=None):
         self._ck(self.L.cfk_compute_viscous_flux(self.h, stream), "viscous")

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "cfk_common.cuh"
+#include "chem.cuh"
 #include "thermo.cuh"
 
 namespace cfk {
@@ -21,6 +22,9 @@ cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, uns
                             cudaStream_t st);
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
                                        int n_face, cudaStream_t st, int *n_launch);
+cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
+cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, double dt, int schedule, int *nsub_out,
+                               int *err, unsigned int *counter, int n_sm, cudaStream_t st);
 }  // namespace cfk
 
 using namespace cfk;
@@ -31,8 +35,9 @@ struct cfk_ctx {
   Zone z{};
   bool bound = false;
   std::vector<void *> owned;  // device arrays owned by the context
-  Thermo *d_thermo = nullptr;
-  bool have_thermo = false;
+  Mech *d_mech = nullptr;
+  bool have_mech = false;
+  int n_sm = 148;
   // device scratch: [0] dt bits (u64), [1] error flags (int)
   unsigned long long *d_dt_bits = nullptr;
   int *d_err = nullptr;
@@ -100,16 +105,23 @@ int validate(const cfk_param *p, std::string &why) {
   if (p->n_var != 5 + p->n_scalar) { why = "n_var must equal 5 + n_scalar"; return -1; }
   if (p->n_scalar < p->n_spec) { why = "n_scalar must be >= n_spec"; return -1; }
   const int s = p->inviscid_scheme;
-  if (!(s == 52 || s == 72)) { why = "inviscid_scheme " + std::to_string(s) + " is not supported by this build"; return -1; }
+  if (!(s == 52 || s == 72 || s == 0)) {
+    why = "inviscid_scheme " + std::to_string(s) + " is not supported by this build";
+    return -1;
+  }
   if (p->viscous_order != 0 && p->viscous_order != 2) { why = "viscous_order must be 0 or 2"; return -1; }
   if (p->sensor_threshold > 1e-10) { why = "hybrid shock-sensor schemes are not supported (shockSensor_threshold must be 0)"; return -1; }
   if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
-  if (p->n_spec > 0) { why = "the mixture model needs cfk_set_mechanism (not in this build)"; return -1; }
+  if (p->n_spec > 0 && s != 0) {
+    why = "the mixture model is supported for chemistry-only contexts (inviscid_scheme 0) in this build";
+    return -1;
+  }
+  if (s == 0 && p->n_spec == 0) { why = "inviscid_scheme 0 (no flux) is for reacting mixtures only"; return -1; }
   if (p->n_face < 0 || p->n_face > 6) { why = "n_face must be 0..6"; return -1; }
   // The WENO weights are normalised through products of two (eps + beta)^2
   // terms; eps = 1e-40 * weno_eps_scale must stay above 1e-70 so that those
   // products (>= eps^4) remain normal numbers.
-  if (!(p->weno_eps_scale >= 1e-30)) { why = "weno_eps_scale must be >= 1e-30 ((rho_ref*v_ref)^2)"; return -1; }
+  if (s != 0 && !(p->weno_eps_scale >= 1e-30)) { why = "weno_eps_scale must be >= 1e-30 ((rho_ref*v_ref)^2)"; return -1; }
   for (int n = 0; n < p->n_face; ++n) {
     const cfk_face &f = p->faces[n];
     if (f.face < 0 || f.face > 2 || (f.direction != -1 && f.direction != 1) ||
@@ -160,13 +172,15 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   p.fixed_dt = param->fixed_dt; p.entropy_fix_factor = param->entropy_fix_factor; p.Pr = param->Pr;
   p.Sc = param->Sc; p.cfl = param->cfl; p.weno_eps_scale = param->weno_eps_scale; p.v_ref = param->v_ref;
   p.rho_ref = param->rho_ref;
+  p.chem_advance_method = param->chem_advance_method;
   e = cudaMalloc(&c->d_dt_bits, 64);
   if (e != cudaSuccess) { delete c; return CFK_ERR_CUDA; }
   c->d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(c->d_dt_bits) + 8);
   cudaMemset(c->d_dt_bits, 0, 64);
-  e = cudaMalloc(&c->d_thermo, sizeof(Thermo));
+  e = cudaMalloc(&c->d_mech, sizeof(Mech));
   if (e != cudaSuccess) { cudaFree(c->d_dt_bits); delete c; return CFK_ERR_CUDA; }
-  cudaMemset(c->d_thermo, 0, sizeof(Thermo));
+  cudaMemset(c->d_mech, 0, sizeof(Mech));
+  cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, param->device);
   *out = c;
   return CFK_OK;
 }
@@ -178,7 +192,7 @@ int cfk_destroy(cfk_ctx *c) {
   for (auto e : c->pool) cudaEventDestroy(e);
   for (void *ptr : c->owned) cudaFree(ptr);
   cudaFree(c->d_dt_bits);
-  cudaFree(c->d_thermo);
+  cudaFree(c->d_mech);
   delete c;
   return CFK_OK;
 }
@@ -188,11 +202,13 @@ const char *cfk_last_error(const cfk_ctx *c) { return c ? c->err.c_str() : "null
 int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   if (!c || !zn) return CFK_ERR_ARG;
   if (zn->mx < 1 || zn->my < 1 || zn->mz < 1) return fail(c, CFK_ERR_ARG, "zone extents must be positive");
-  const int need_g = c->hp.inviscid_scheme == 72 ? 4 : 3;
+  const int need_g = c->hp.inviscid_scheme == 72 ? 4 : (c->hp.inviscid_scheme == 0 ? 0 : 3);
   if (zn->ngg < need_g) return fail(c, CFK_ERR_ARG, "ngg too small for the inviscid scheme");
   if ((c->hp.dim == 2) != (zn->mz == 1)) return fail(c, CFK_ERR_ARG, "dim does not match mz");
-  if (!zn->cv || !zn->bv || !zn->qn || !zn->dq || !zn->metric || !zn->jac)
+  if (c->hp.inviscid_scheme != 0 && (!zn->cv || !zn->bv || !zn->qn || !zn->dq || !zn->metric || !zn->jac))
     return fail(c, CFK_ERR_ARG, "cv, bv, qn, dq, metric and jac are required");
+  if (c->hp.n_spec > 0 && (!zn->cv || !zn->bv || !zn->sv || !zn->jac || !zn->reaction_timeScale))
+    return fail(c, CFK_ERR_ARG, "cv, bv, sv, jac and reaction_timeScale are required for reacting mixtures");
   if (c->hp.viscous_order > 0 && !zn->mul) return fail(c, CFK_ERR_ARG, "mul is required for viscous runs");
   if (c->hp.n_scalar > 0 && !zn->sv) return fail(c, CFK_ERR_ARG, "sv is required when n_scalar > 0");
   // 32-bit plane extents, as in the reference's int indexing
@@ -212,7 +228,7 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
 int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
   if (!c || !out) return CFK_ERR_ARG;
   CFK_CHECK(c, cudaSetDevice(c->hp.device), "cudaSetDevice");
-  const int g = c->hp.inviscid_scheme == 72 ? 4 : 3;
+  const int g = c->hp.inviscid_scheme == 72 ? 4 : (c->hp.inviscid_scheme == 0 ? 0 : 3);
   cfk_zone zn{};
   zn.mx = mx; zn.my = my; zn.mz = mz; zn.ngg = g;
   const size_t P = (size_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g), N = (size_t)mx * my * mz;
@@ -244,7 +260,89 @@ int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
     CFK_CHECK(c, cudaSetDevice((c)->hp.device), "cudaSetDevice");                 \
   } while (0)
 
-static const Thermo *thermo_of(cfk_ctx *c) { return c->have_thermo ? c->d_thermo : nullptr; }
+static const Thermo *thermo_of(cfk_ctx *c) { return c->have_mech ? &c->d_mech->th : nullptr; }
+
+int cfk_set_mechanism(cfk_ctx *c, const cfk_mechanism *m) {
+  if (!c || !m) return CFK_ERR_ARG;
+  if (m->n_spec != c->hp.n_spec) return fail(c, CFK_ERR_ARG, "mechanism n_spec differs from the context's n_spec");
+  if (m->n_spec < 1 || m->n_spec > kMaxSpec || m->n_reac < 0 || m->n_reac > kMaxReac)
+    return fail(c, CFK_ERR_ARG, "mechanism size out of range");
+  if (m->n_reac != c->hp.n_reac) return fail(c, CFK_ERR_ARG, "mechanism n_reac differs from the context's n_reac");
+  Mech h;
+  std::memset(&h, 0, sizeof(h));
+  Thermo &th = h.th;
+  const int ns = m->n_spec;
+  th.n_spec = ns;
+  const double R_u = 8314.462618;
+  for (int l = 0; l < ns; ++l) {
+    th.mw[l] = m->mw[l];
+    th.imw[l] = 1.0 / m->mw[l];
+    th.gas_const[l] = R_u / m->mw[l];
+    th.t_low[l] = m->t_low[l]; th.t_mid[l] = m->t_mid[l]; th.t_high[l] = m->t_high[l];
+    for (int q = 0; q < 7; ++q) { th.low[l][q] = m->low[l][q]; th.high[l][q] = m->high[l][q]; }
+    th.geometry[l] = m->geometry[l];
+    th.LJ_potent_inv[l] = m->LJ_potent_inv[l];
+    th.vis_coeff[l] = m->vis_coeff[l];
+    th.ZRotF298[l] = m->ZRotF298[l];
+    for (int n = 0; n < ns; ++n) {
+      th.WjDivWi_to_One4th[l][n] = m->WjDivWi_to_One4th[l][n];
+      th.sqrt_WiDivWjPl1Mul8[l][n] = m->sqrt_WiDivWjPl1Mul8[l][n];
+      th.binary_diffusivity_coeff[l][n] = m->binary_diffusivity_coeff[l][n];
+      th.kb_over_eps_jk[l][n] = m->kb_over_eps_jk[l][n];
+    }
+  }
+  Kinetics &kn = h.kn;
+  kn.n_reac = m->n_reac;
+  for (int r = 0; r < m->n_reac; ++r) {
+    kn.type[r] = m->reac_type[r];
+    kn.rev[r] = m->rev_type[r];
+    kn.order[r] = m->order[r];
+    kn.A[r] = m->A[r]; kn.b[r] = m->b[r]; kn.Ea[r] = m->Ea[r];
+    kn.A2[r] = m->A2[r]; kn.b2[r] = m->b2[r]; kn.Ea2[r] = m->Ea2[r];
+    kn.troe_alpha[r] = m->troe_alpha[r]; kn.troe_t3[r] = m->troe_t3[r];
+    kn.troe_t1[r] = m->troe_t1[r]; kn.troe_t2[r] = m->troe_t2[r];
+    int n = 0;
+    for (int l = 0; l < ns; ++l) {
+      kn.tb[r][l] = m->third_body_coeff[r][l];
+      if (m->stoi_f[r][l] != 0 || m->stoi_b[r][l] != 0) {
+        if (n == kMaxInvolved) return fail(c, CFK_ERR_ARG, "a reaction involves more than 6 species");
+        if (m->stoi_f[r][l] < 0 || m->stoi_b[r][l] < 0) return fail(c, CFK_ERR_ARG, "negative stoichiometry");
+        kn.inv_sp[r][n] = l;
+        kn.inv_f[r][n] = m->stoi_f[r][l];
+        kn.inv_b[r][n] = m->stoi_b[r][l];
+        ++n;
+      }
+    }
+    kn.n_inv[r] = n;
+  }
+  CFK_CHECK(c, cudaSetDevice(c->hp.device), "cudaSetDevice");
+  CFK_CHECK(c, cudaMemcpy(c->d_mech, &h, sizeof(Mech), cudaMemcpyHostToDevice), "mechanism upload");
+  c->have_mech = true;
+  return CFK_OK;
+}
+
+int cfk_finite_rate_chemistry(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  if (!c->have_mech || c->hp.n_reac == 0) return fail(c, CFK_ERR_STATE, "no reacting mechanism loaded");
+  if (!c->z.dq) return fail(c, CFK_ERR_ARG, "dq is required");
+  CFK_CHECK(c, launch_finite_rate_chemistry(c->z, c->d_mech, S(stream)), "finite_rate_chemistry");
+  c->launches += 1;
+  return CFK_OK;
+}
+
+int cfk_wu_reaction_step(cfk_ctx *c, double dt, int schedule, int *nsub_out, void *stream) {
+  NEED_ZONE(c);
+  if (!c->have_mech || c->hp.n_reac == 0) return fail(c, CFK_ERR_STATE, "no reacting mechanism loaded");
+  if (schedule != 0 && schedule != 1) return fail(c, CFK_ERR_ARG, "schedule must be 0 or 1");
+  if (c->hp.chem_advance_method != 0 && c->hp.chem_advance_method != 1)
+    return fail(c, CFK_ERR_ARG, "chem_advance_method must be 0 (explicit) or 1 (point implicit)");
+  unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
+  CFK_CHECK(c, launch_wu_reaction(c->z, c->p, c->d_mech, dt, schedule, nsub_out, c->d_err, counter, c->n_sm,
+                                  S(stream)),
+            "wu_reaction_step");
+  c->launches += 1;
+  return CFK_OK;
+}
 
 int cfk_compute_viscous_flux(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
@@ -414,7 +512,10 @@ int cfk_stream_sync(cfk_ctx *c, void *stream) {
     CFK_CHECK(c, cudaMemcpy(&h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag read");
     if (h_err) {
       cudaMemset(c->d_err, 0, sizeof(int));
-      return fail(c, CFK_ERR_NUMERIC, "temperature Newton iteration reached its 1000-iteration cap");
+      std::string msg;
+      if (h_err & 1) msg += "temperature Newton iteration reached its 1000-iteration cap; ";
+      if (h_err & 2) msg += "a node needed more than 100000 reaction substeps (capped); ";
+      return fail(c, CFK_ERR_NUMERIC, msg);
     }
   }
   return CFK_OK;

@@ -48,7 +48,7 @@ struct Zone {
 struct Param {
   int dim, n_var, n_spec, n_scalar, n_reac;
   int inviscid_scheme, reconstruction, limiter, viscous_order;
-  int positive_preserving, gradPInDiffusionFlux, fixed_dt;
+  int positive_preserving, gradPInDiffusionFlux, fixed_dt, chem_advance_method;
   double entropy_fix_factor, Pr, Sc, cfl;
   double weno_eps_scale, v_ref, rho_ref;
 };

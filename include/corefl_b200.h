@@ -80,6 +80,34 @@ typedef struct cfk_zone {
   double *dq, *dt_local, *Cn;    /* n_var, 1, n_var planes, 0 ghosts */
 } cfk_zone;
 
+/* Species, thermo, transport and kinetics tables of a mechanism — the
+ * DParameter tables (reference src/DParameter.cuh:84-130) that the mixture
+ * and chemistry kernels read.  Up to CFK_MAX_SPEC species and CFK_MAX_REAC
+ * reactions; matrices are row-major [reaction][species] or [species][species].
+ * reac_type: 0 irreversible, 1 elementary, 3 merged duplicate, 4 third body,
+ * 5 Lindemann, 6/7 Troe with 3/4 parameters; rev_type 1 = explicit reverse
+ * Arrhenius (REV).  Ea and Ea2 are in K (already divided by R_c). */
+#define CFK_MAX_SPEC 9
+#define CFK_MAX_REAC 24
+typedef struct cfk_mechanism {
+  int n_spec, n_reac;
+  double mw[CFK_MAX_SPEC];
+  double t_low[CFK_MAX_SPEC], t_mid[CFK_MAX_SPEC], t_high[CFK_MAX_SPEC];
+  double low[CFK_MAX_SPEC][7], high[CFK_MAX_SPEC][7];
+  int geometry[CFK_MAX_SPEC];
+  double LJ_potent_inv[CFK_MAX_SPEC], vis_coeff[CFK_MAX_SPEC], ZRotF298[CFK_MAX_SPEC];
+  double WjDivWi_to_One4th[CFK_MAX_SPEC][CFK_MAX_SPEC];
+  double sqrt_WiDivWjPl1Mul8[CFK_MAX_SPEC][CFK_MAX_SPEC];
+  double binary_diffusivity_coeff[CFK_MAX_SPEC][CFK_MAX_SPEC];
+  double kb_over_eps_jk[CFK_MAX_SPEC][CFK_MAX_SPEC];
+  int reac_type[CFK_MAX_REAC], rev_type[CFK_MAX_REAC], order[CFK_MAX_REAC];
+  int stoi_f[CFK_MAX_REAC][CFK_MAX_SPEC], stoi_b[CFK_MAX_REAC][CFK_MAX_SPEC];
+  double A[CFK_MAX_REAC], b[CFK_MAX_REAC], Ea[CFK_MAX_REAC];
+  double A2[CFK_MAX_REAC], b2[CFK_MAX_REAC], Ea2[CFK_MAX_REAC];
+  double third_body_coeff[CFK_MAX_REAC][CFK_MAX_SPEC];
+  double troe_alpha[CFK_MAX_REAC], troe_t3[CFK_MAX_REAC], troe_t1[CFK_MAX_REAC], troe_t2[CFK_MAX_REAC];
+} cfk_mechanism;
+
 /* ---- context ---------------------------------------------------------- */
 int cfk_create(const cfk_param *param, cfk_ctx **out);
 int cfk_destroy(cfk_ctx *ctx);
@@ -118,6 +146,24 @@ int cfk_apply_boundary_conditions(cfk_ctx *ctx, void *stream);
  * + global_time_step (reference src/TimeAdvanceFunc.cuh:28-115,
  * src/TimeAdvanceFunc.cu:102-152).  *dt_out is written after a stream sync. */
 int cfk_local_time_step(cfk_ctx *ctx, double *dt_out, void *stream);
+
+/* Load the mechanism tables (required when n_spec > 0). */
+int cfk_set_mechanism(cfk_ctx *ctx, const cfk_mechanism *mech);
+/* Explicit finite-rate source dq[5+l] += J*omega_l and the reaction time
+ * scale.  Replaces finite_rate_chemistry (reference src/FiniteRateChem.cu:1388-1464). */
+int cfk_finite_rate_chemistry(cfk_ctx *ctx, void *stream);
+/* Reaction step of Wu's splitting over dt at every node: n_sub = int(dt/tau)
+ * substeps of dt/(n_sub+1) plus the remainder, each an explicit
+ * (chem_advance_method 0) or point-implicit (1) 0-D update with the frozen
+ * transport term Cn.  Replaces wu_reaction_step (reference
+ * src/StrangSplitting.cu:373-421, 43-224).  schedule 0 = one thread per
+ * node (the reference's mapping); 1 = persistent work-queue kernel in which
+ * each lane pulls the next node when its node is done, so nodes with uneven
+ * substep counts do not idle the warp.  Both give identical results.
+ * nsub_out (device int[mx*my*mz], may be NULL) receives the substeps per node.
+ * n_sub is capped at 100000 per node; CFK_ERR_NUMERIC is reported by the next
+ * cfk_stream_sync if a node hit the cap. */
+int cfk_wu_reaction_step(cfk_ctx *ctx, double dt, int schedule, int *nsub_out, void *stream);
 
 /* ---- whole steps ------------------------------------------------------ */
 /* One SSP-RK3 step: qn <- cv, dt (fixed or CFL), three stages of

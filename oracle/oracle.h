@@ -111,6 +111,23 @@ double orc_sutherland(double t);
 
 int orc_num_threads(void);
 
+/* mixture thermo and kinetics (oracle_mix.c) */
+void orc_enthalpy_and_cp(const orc_mech *m, double t, double *h, double *cp);
+void orc_cp(const orc_mech *m, double t, double *cp);
+void orc_gibbs_div_rt(const orc_mech *m, double t, double *g);
+void orc_forward_rate(const orc_mech *m, double t, const double *c, double *kf);
+void orc_backward_rate(const orc_mech *m, double t, const double *kf, const double *c, double *kb);
+void orc_rate_of_progress(const orc_mech *m, const double *kf, const double *kb, const double *c, double *q1,
+                          double *q2);
+void orc_chemical_source(const orc_mech *m, const double *q1, const double *q2, double *omega_d, double *omega);
+void orc_solve_chem_system(double *lhs, double *rhs, int dim);
+/* Wu-splitting reaction step over the zone (point implicit when
+ * chem_advance_method == 1); nsub_out (N ints, may be NULL) receives the
+ * number of substeps taken per node. */
+void orc_wu_reaction_step(orc_zone *z, const orc_param *p, double dt, int *nsub_out);
+/* explicit finite-rate source into dq and the reaction time scale */
+void orc_finite_rate_chemistry(orc_zone *z, const orc_param *p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,72 @@ class orc_param(ctypes.Structure):
     ]
 
 
+MAXS, MAXR = 20, 64
+
+
+class orc_mech(ctypes.Structure):
+    _fields_ = [
+        ("n_spec", ctypes.c_int), ("n_reac", ctypes.c_int),
+        ("mw", ctypes.c_double * MAXS), ("imw", ctypes.c_double * MAXS), ("gas_const", ctypes.c_double * MAXS),
+        ("t_low", ctypes.c_double * MAXS), ("t_mid", ctypes.c_double * MAXS), ("t_high", ctypes.c_double * MAXS),
+        ("low_coeff", (ctypes.c_double * 7) * MAXS), ("high_coeff", (ctypes.c_double * 7) * MAXS),
+        ("geometry", ctypes.c_double * MAXS), ("LJ_potent_inv", ctypes.c_double * MAXS),
+        ("vis_coeff", ctypes.c_double * MAXS),
+        ("WjDivWi_to_One4th", (ctypes.c_double * MAXS) * MAXS),
+        ("sqrt_WiDivWjPl1Mul8", (ctypes.c_double * MAXS) * MAXS),
+        ("binary_diffusivity_coeff", (ctypes.c_double * MAXS) * MAXS),
+        ("kb_over_eps_jk", (ctypes.c_double * MAXS) * MAXS),
+        ("ZRotF298", ctypes.c_double * MAXS),
+        ("reac_type", ctypes.c_int * MAXR), ("rev_type", ctypes.c_int * MAXR),
+        ("stoi_f", (ctypes.c_int * MAXS) * MAXR), ("stoi_b", (ctypes.c_int * MAXS) * MAXR),
+        ("reac_order", ctypes.c_int * MAXR),
+        ("A", ctypes.c_double * MAXR), ("b", ctypes.c_double * MAXR), ("Ea", ctypes.c_double * MAXR),
+        ("A2", ctypes.c_double * MAXR), ("b2", ctypes.c_double * MAXR), ("Ea2", ctypes.c_double * MAXR),
+        ("third_body_coeff", (ctypes.c_double * MAXS) * MAXR),
+        ("troe_alpha", ctypes.c_double * MAXR), ("troe_t3", ctypes.c_double * MAXR),
+        ("troe_t1", ctypes.c_double * MAXR), ("troe_t2", ctypes.c_double * MAXR),
+    ]
+
+
+def make_mech(m) -> orc_mech:
+    """orc_mech tables from a mechanism.Mechanism (gas constants R_u/W as the
+    reference's DParameter builds them, src/DParameter.cu:72-83)."""
+    R_U = 8314.462618
+    o = orc_mech()
+    ns, nr = m.n_spec, m.n_reac
+    o.n_spec, o.n_reac = ns, nr
+
+    def fill1(name, vals):
+        arr = getattr(o, name)
+        for i, v in enumerate(vals):
+            arr[i] = v
+
+    def fill2(name, vals):
+        arr = getattr(o, name)
+        for i in range(vals.shape[0]):
+            for j in range(vals.shape[1]):
+                arr[i][j] = vals[i, j]
+
+    fill1("mw", m.mw)
+    fill1("imw", [1.0 / w for w in m.mw])
+    fill1("gas_const", [R_U / w for w in m.mw])
+    for k in ("t_low", "t_mid", "t_high", "geometry", "LJ_potent_inv", "vis_coeff", "ZRotF298"):
+        fill1(k, getattr(m, k))
+    fill2("low_coeff", m.low)
+    fill2("high_coeff", m.high)
+    for k in ("WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8", "binary_diffusivity_coeff", "kb_over_eps_jk"):
+        fill2(k, getattr(m, k))
+    fill1("reac_type", m.reac_type)
+    fill1("rev_type", m.rev_type)
+    fill1("reac_order", m.order)
+    fill2("stoi_f", m.stoi_f)
+    fill2("stoi_b", m.stoi_b)
+    for k in ("A", "b", "Ea", "A2", "b2", "Ea2", "troe_alpha", "troe_t3", "troe_t1", "troe_t2"):
+        fill1(k, getattr(m, k))
+    fill2("third_body_coeff", m.third_body_coeff)
+    return o
+
+
 _lib = None
 
 
@@ -71,6 +137,10 @@ def lib() -> ctypes.CDLL:
         L.orc_sutherland.argtypes = [ctypes.c_double]
         L.orc_sutherland.restype = ctypes.c_double
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_wu_reaction_step.argtypes = [zp, pp, ctypes.c_double, ctypes.c_void_p]
+        L.orc_wu_reaction_step.restype = None
+        L.orc_finite_rate_chemistry.argtypes = [zp, pp]
+        L.orc_finite_rate_chemistry.restype = None
         _lib = L
     return _lib
 
@@ -112,7 +182,8 @@ class OracleZone:
         self.p.n_face = len(c.faces)
         for n, (f, d, lab) in enumerate(c.faces):
             self.p.faces[n] = orc_face(f, d, lab)
-        self.p.mech = None
+        self.mech = make_mech(c.mech) if getattr(c, "mech", None) is not None else None
+        self.p.mech = ctypes.cast(ctypes.pointer(self.mech), ctypes.c_void_p) if self.mech is not None else None
         self.L = lib()
 
     def __getitem__(self, k):
@@ -132,6 +203,14 @@ class OracleZone:
 
     def step(self) -> float:
         return self.L.orc_rk3_step(ctypes.byref(self.z), ctypes.byref(self.p), self.p.dt)
+
+    def reaction_step(self, dt: float, want_nsub: bool = False):
+        """Wu-splitting reaction step over the zone (point implicit when
+        chem_advance_method == 1); optionally returns the substeps per node."""
+        ns = np.zeros(self.case.N, dtype=np.int32) if want_nsub else None
+        self.L.orc_wu_reaction_step(ctypes.byref(self.z), ctypes.byref(self.p), dt,
+                                    ns.ctypes.data if want_nsub else None)
+        return ns
 
     def call(self, name, *args):
         return getattr(self.L, name)(ctypes.byref(self.z), ctypes.byref(self.p), *args)

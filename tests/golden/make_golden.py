@@ -3,6 +3,11 @@ example data (run in a checkout that has the reference at REFERENCE_ROOT).
 
 sod_exact.npz  — exact Riemann solution of the Sod problem at t = 0.2
                  (reference example/sodShockTube/exact.dat: x, u, rho, p).
+reactor_li2004.npz — constant-volume H2/air ignition trajectory of the
+                 reference's 0-D reactor (Li-2004 species, 1000 K, 2 atm,
+                 X = 0.295775 H2 / 0.147887 O2 / 0.556338 N2; reference
+                 example/constantVolumeReactor/const_volume_reactor_output.dat):
+                 t, T, p and mole fractions every 5000 reactor steps.
 """
 import os
 import sys
@@ -22,7 +27,20 @@ def sod_exact():
     print("sod_exact.npz:", vals.shape[0], "points")
 
 
+def reactor():
+    path = os.path.join(REF, "example", "constantVolumeReactor", "const_volume_reactor_output.dat")
+    with open(path) as f:
+        header = f.readline().strip()
+        rows = [[float(v) for v in line.split(",")] for line in f if line.strip()]
+    a = np.array(rows)
+    names = [h.split("<sub>")[1].split("</sub>")[0] for h in header.split(",")[3:-1]]
+    np.savez_compressed(os.path.join(HERE, "reactor_li2004.npz"), t=a[:, 0], T=a[:, 1], p=a[:, 2], X=a[:, 3:-1],
+                        species=np.array(names))
+    print("reactor_li2004.npz:", a.shape[0], "records", names)
+
+
 if __name__ == "__main__":
     if not os.path.isdir(REF):
         sys.exit(f"reference not found at {REF}")
     sod_exact()
+    reactor()

@@ -37,6 +37,8 @@ class GpuZone:
             self.t["rho_D"] = z(ns, P)
             self.t["Cn"] = z(nv, N)
         self.ctx.bind(c.mx, c.my, c.mz, c.ngg, {k: v.data_ptr() for k, v in self.t.items()})
+        if ns:
+            self.ctx.set_mechanism(c.mech)
 
     def initialize(self):
         """properties, BCs (with the 2-D k-ghost copy), properties, cv from bv —
@@ -51,9 +53,9 @@ class GpuZone:
         self.torch.cuda.synchronize()
         return self.t[k].cpu().numpy()
 
-    def load_from(self, oz):
+    def load_from(self, oz, keys=("cv", "bv", "mul", "qn")):
         """Copy the oracle's state arrays into the device arrays."""
-        for k in ("cv", "bv", "mul", "qn"):
+        for k in keys:
             self.t[k].copy_(self.torch.from_numpy(oz[k][: self.t[k].shape[0]]).to(self.t[k].device))
         if "sv" in self.t:
             self.t["sv"].copy_(self.torch.from_numpy(oz["sv"][: self.t["sv"].shape[0]]))
