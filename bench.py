@@ -163,8 +163,8 @@ def reacting_bench(args, local, world, dist):
     import mechanism
 
     mech = mechanism.load("li2004")
-    case = cases.reactor_batch(mech, 1 << 20, seed=2026)
-    out = {"workload": "2^20 constant-volume H2/air reactors, Li-2004 9s/19r, point-implicit Wu substeps, "
+    case = cases.reactor_batch(mech, args.reacting_cells, seed=2026)
+    out = {"workload": f"{case.N} constant-volume H2/air reactors, Li-2004 9s/19r, point-implicit Wu substeps, "
                        "dt 1e-7 s", "cells": case.N, "dtype": "f64"}
     nsub = torch.zeros(case.N, dtype=torch.int32, device=f"cuda:{local}")
     for name, sched in (("plain", 0), ("work_queue", 1)):
@@ -212,6 +212,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reacting", action="store_true")
+    ap.add_argument("--reacting-only", action="store_true", help="only the batched-reactor measurement")
+    ap.add_argument("--reacting-cells", type=int, default=1 << 20)
     args = ap.parse_args()
     rank, world, local = _env_rank()
     args.warmup = max(args.warmup, 3)
@@ -222,6 +224,11 @@ def main():
 
     import torch
     import corefl_b200 as cfk
+
+    if args.reacting_only:
+        torch.cuda.set_device(local)
+        print(json.dumps({"reacting": reacting_bench(args, local, 1, None)}), flush=True)
+        return
 
     dist = None
     if world > 1:
