@@ -103,6 +103,22 @@ class cfk_zone(ctypes.Structure):
 
 ZONE_FIELDS = [f for f, _ in cfk_zone._fields_[4:]]
 
+_FP = ctypes.POINTER(ctypes.c_float)
+SG_NPARAM, SG_NNORM, SG_NIN, SG_NOUT = 41216, 81, 12, 11
+
+
+class cfk_surrogate_gate(ctypes.Structure):
+    _fields_ = [("ood_margin", ctypes.c_double), ("dT_max", ctypes.c_double), ("dT_consistency", ctypes.c_double),
+                ("judge_tol_T", ctypes.c_double), ("judge_tol_bc", ctypes.c_double),
+                ("min_substeps", ctypes.c_double), ("judge_stride", ctypes.c_int), ("revert_steps", ctypes.c_int)]
+
+
+class cfk_surrogate_stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong) for n in ("cells", "surrogate", "fallback_ood", "fallback_ignition",
+                                                 "fallback_consistency", "fallback_revert", "fallback_newton",
+                                                 "fallback_cheap", "judged", "judge_failed")] + \
+               [(n, ctypes.c_double) for n in ("judge_max_dT", "judge_mean_dT", "judge_max_dbc")]
+
 _lib = None
 
 
@@ -145,6 +161,17 @@ def lib() -> ctypes.CDLL:
             "cfk_set_mechanism": (i, [vp, ctypes.POINTER(cfk_mechanism)]),
             "cfk_finite_rate_chemistry": (i, [vp, vp]),
             "cfk_wu_reaction_step": (i, [vp, d, i, vp, vp]),
+            "cfk_surrogate_init": (i, [vp, ctypes.c_ulonglong, i, _DP]),
+            "cfk_surrogate_record": (i, [vp, i, d, vp, vp, vp]),
+            "cfk_surrogate_fit_normalization": (i, [vp, vp, vp, ctypes.c_longlong]),
+            "cfk_surrogate_train": (i, [vp, vp, vp, ctypes.c_longlong, i, i, d, d, ctypes.c_ulonglong, _DP]),
+            "cfk_surrogate_gradients": (i, [vp, vp, vp, ctypes.c_longlong, vp, _DP]),
+            "cfk_surrogate_forward": (i, [vp, vp, ctypes.c_longlong, vp]),
+            "cfk_surrogate_get_params": (i, [vp, _FP, _FP]),
+            "cfk_surrogate_set_params": (i, [vp, _FP, _FP]),
+            "cfk_surrogate_default_gate": (i, [ctypes.POINTER(cfk_surrogate_gate)]),
+            "cfk_surrogate_reaction_step": (i, [vp, d, ctypes.POINTER(cfk_surrogate_gate), i,
+                                                ctypes.POINTER(cfk_surrogate_stats), vp]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -216,6 +243,64 @@ class Context:
 
     def wu_reaction_step(self, dt, schedule=0, nsub_ptr=None, stream=None):
         self._ck(self.L.cfk_wu_reaction_step(self.h, dt, schedule, nsub_ptr, stream), "wu_reaction_step")
+
+    # ---- MLP chemistry surrogate (device pointers are plain ints) --------
+    def surrogate_init(self, seed, elem_mu):
+        import numpy as np
+        mu = np.ascontiguousarray(elem_mu, dtype=np.float64)
+        self._ck(self.L.cfk_surrogate_init(self.h, seed, mu.shape[0], mu.ctypes.data_as(_DP)), "surrogate_init")
+
+    def surrogate_record(self, phase, dt, X=None, G=None, stream=None):
+        self._ck(self.L.cfk_surrogate_record(self.h, phase, dt, X, G, stream), "surrogate_record")
+
+    def surrogate_fit_normalization(self, X, G, n):
+        self._ck(self.L.cfk_surrogate_fit_normalization(self.h, X, G, n), "surrogate_fit_normalization")
+
+    def surrogate_train(self, X, G, n, epochs, batch, lr0, lr1, seed=0):
+        losses = (ctypes.c_double * epochs)()
+        self._ck(self.L.cfk_surrogate_train(self.h, X, G, n, epochs, batch, lr0, lr1, seed, losses), "surrogate_train")
+        return list(losses)
+
+    def surrogate_gradients(self, X, G, n, grad_out) -> float:
+        loss = ctypes.c_double()
+        self._ck(self.L.cfk_surrogate_gradients(self.h, X, G, n, grad_out, ctypes.byref(loss)), "surrogate_gradients")
+        return loss.value
+
+    def surrogate_forward(self, X, n, Y):
+        self._ck(self.L.cfk_surrogate_forward(self.h, X, n, Y), "surrogate_forward")
+
+    def surrogate_get_params(self):
+        import numpy as np
+        w = np.zeros(SG_NPARAM, np.float32)
+        nm = np.zeros(SG_NNORM, np.float32)
+        self._ck(self.L.cfk_surrogate_get_params(self.h, w.ctypes.data_as(_FP), nm.ctypes.data_as(_FP)),
+                 "surrogate_get_params")
+        return w, nm
+
+    def surrogate_set_params(self, weights=None, norm=None):
+        import numpy as np
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+        nm = None if norm is None else np.ascontiguousarray(norm, dtype=np.float32)
+        self._ck(self.L.cfk_surrogate_set_params(self.h, None if w is None else w.ctypes.data_as(_FP),
+                                                 None if nm is None else nm.ctypes.data_as(_FP)),
+                 "surrogate_set_params")
+
+    @staticmethod
+    def surrogate_default_gate(**over) -> cfk_surrogate_gate:
+        g = cfk_surrogate_gate()
+        lib().cfk_surrogate_default_gate(ctypes.byref(g))
+        for k, v in over.items():
+            setattr(g, k, v)
+        return g
+
+    def surrogate_reaction_step(self, dt, gate, step_index=0, want_stats=False, stream=None):
+        st = cfk_surrogate_stats() if want_stats else None
+        self._ck(self.L.cfk_surrogate_reaction_step(self.h, dt, ctypes.byref(gate), step_index,
+                                                    ctypes.byref(st) if st is not None else None, stream),
+                 "surrogate_reaction_step")
+        if st is None:
+            return None
+        return {n: getattr(st, n) for n, _ in cfk_surrogate_stats._fields_}
 
     def viscous(self, stream=None):
         self._ck(self.L.cfk_compute_viscous_flux(self.h, stream), "viscous")

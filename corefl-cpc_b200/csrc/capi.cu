@@ -6,9 +6,7 @@
 #include <string>
 #include <vector>
 
-#include "cfk_common.cuh"
-#include "chem.cuh"
-#include "thermo.cuh"
+#include "ctx.cuh"
 
 namespace cfk {
 cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
@@ -28,36 +26,7 @@ cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, do
 }  // namespace cfk
 
 using namespace cfk;
-
-struct cfk_ctx {
-  cfk_param hp{};
-  Param p{};
-  Zone z{};
-  bool bound = false;
-  std::vector<void *> owned;  // device arrays owned by the context
-  Mech *d_mech = nullptr;
-  bool have_mech = false;
-  int n_sm = 148;
-  // device scratch: [0] dt bits (u64), [1] error flags (int)
-  unsigned long long *d_dt_bits = nullptr;
-  int *d_err = nullptr;
-  long long launches = 0;
-  std::string err;
-  // CUDA graph of one RK3 step
-  cudaGraphExec_t graph_exec = nullptr;
-  long long graph_kernels = 0;
-  // phase timing with CUDA events (plain steps only)
-  bool profiling = false;
-  struct Rec { int phase; cudaEvent_t a, b; long long kernels; };
-  std::vector<Rec> recs;
-  std::vector<cudaEvent_t> pool;
-  cudaEvent_t take_event() {
-    if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    return e;
-  }
-};
+using namespace cfk_detail;
 
 namespace {
 // Records the events of one phase around the launches issued in its scope.
@@ -81,23 +50,6 @@ struct PhaseScope {
 }  // namespace
 
 namespace {
-
-int fail(cfk_ctx *c, int code, const std::string &msg) {
-  if (c) c->err = msg;
-  return code;
-}
-
-int cuda_fail(cfk_ctx *c, cudaError_t e, const char *where) {
-  return fail(c, CFK_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-#define CFK_CHECK(ctx, call, where)                \
-  do {                                             \
-    cudaError_t e_ = (call);                       \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
-  } while (0)
-
-inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 int validate(const cfk_param *p, std::string &why) {
   if (p->dim != 2 && p->dim != 3) { why = "dim must be 2 or 3"; return -1; }
@@ -188,6 +140,7 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
 int cfk_destroy(cfk_ctx *c) {
   if (!c) return CFK_OK;
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->sg) surrogate_destroy(c->sg);
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : c->pool) cudaEventDestroy(e);
   for (void *ptr : c->owned) cudaFree(ptr);
@@ -253,13 +206,6 @@ int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
   return cfk_bind_zone(c, &zn);
 }
 
-#define NEED_ZONE(c)                                                              \
-  do {                                                                            \
-    if (!(c)) return CFK_ERR_ARG;                                                 \
-    if (!(c)->bound) return fail(c, CFK_ERR_STATE, "no zone bound");              \
-    CFK_CHECK(c, cudaSetDevice((c)->hp.device), "cudaSetDevice");                 \
-  } while (0)
-
 static const Thermo *thermo_of(cfk_ctx *c) { return c->have_mech ? &c->d_mech->th : nullptr; }
 
 int cfk_set_mechanism(cfk_ctx *c, const cfk_mechanism *m) {
@@ -306,10 +252,15 @@ int cfk_set_mechanism(cfk_ctx *c, const cfk_mechanism *m) {
       kn.tb[r][l] = m->third_body_coeff[r][l];
       if (m->stoi_f[r][l] != 0 || m->stoi_b[r][l] != 0) {
         if (n == kMaxInvolved) return fail(c, CFK_ERR_ARG, "a reaction involves more than 6 species");
-        if (m->stoi_f[r][l] < 0 || m->stoi_b[r][l] < 0) return fail(c, CFK_ERR_ARG, "negative stoichiometry");
+        if (m->stoi_f[r][l] < 0 || m->stoi_b[r][l] < 0 || m->stoi_f[r][l] > 127 || m->stoi_b[r][l] > 127)
+          return fail(c, CFK_ERR_ARG, "stoichiometric coefficient out of range");
         kn.inv_sp[r][n] = l;
         kn.inv_f[r][n] = m->stoi_f[r][l];
         kn.inv_b[r][n] = m->stoi_b[r][l];
+        kn.stf[r][l] = (signed char)m->stoi_f[r][l];
+        kn.stb[r][l] = (signed char)m->stoi_b[r][l];
+        kn.inv_mask[r] |= 1u << l;
+        if (m->stoi_f[r][l] != m->stoi_b[r][l]) kn.net_mask[r] |= 1u << l;
         ++n;
       }
     }

@@ -4,6 +4,7 @@
 // persistent work-queue kernel for nodes with uneven substep counts.
 #include "cfk_common.cuh"
 #include "chem.cuh"
+#include "chem_fast.cuh"
 #include "thermo.cuh"
 
 namespace cfk {
@@ -202,12 +203,15 @@ __global__ void __launch_bounds__(128) wu_reaction_plain_kernel(Zone z, Param p,
 // shared out with a prefix over the lanes that need work).  All lanes of a
 // warp execute the same substep code in every trip, whatever substep their
 // node is at, so nodes with many substeps do not leave the rest of the warp
-// idle.  The loop ends when the counter passes the node count.
+// idle.  The loop ends when the counter passes the node count.  With a node
+// list, the queue runs over list[0 .. *list_count) instead of all nodes.
 __global__ void __launch_bounds__(128) wu_reaction_queue_kernel(Zone z, Param p, const Mech *mc, double dt,
-                                                                int *nsub_out, int *err, unsigned int *counter) {
+                                                                int *nsub_out, int *err, unsigned int *counter,
+                                                                const unsigned int *list,
+                                                                const unsigned int *list_count) {
   const Dims d = z.d;
   const int ns = mc->th.n_spec;
-  const unsigned int total = (unsigned int)d.mx * d.my * d.mz;
+  const unsigned int total = list ? *list_count : (unsigned int)d.mx * d.my * d.mz;
   const int64_t szp = d.plane(d.ngg);
   const int lane = threadIdx.x & 31;
   NodeState s;
@@ -228,6 +232,7 @@ __global__ void __launch_bounds__(128) wu_reaction_queue_kernel(Zone z, Param p,
       if (need) {
         node = base + __popc(mask & ((1u << lane) - 1));
         if (node < total) {
+          if (list) node = list[node];
           const int i = node % d.mx, rem = node / d.mx, j = rem % d.my, k = rem / d.my;
           id = d.idx(d.ngg, i, j, k);
           iq = d.idx(0, i, j, k);
@@ -266,6 +271,122 @@ __global__ void __launch_bounds__(128) wu_reaction_queue_kernel(Zone z, Param p,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time species count (NS = 9, the bundled H2 mechanisms): the same
+// two schedules over zero_d_substep_ns, with each lane's NS x NS system in
+// shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kFastBlock = 64;
+
+template <int NS>
+__host__ __device__ constexpr int fast_smem_bytes() { return (NS * NS + NS) * kFastBlock * (int)sizeof(double); }
+
+template <int NS>
+__global__ void __launch_bounds__(kFastBlock) wu_reaction_plain_ns_kernel(Zone z, Param p, const Mech *mc, double dt,
+                                                                         int *nsub_out, int *err) {
+  extern __shared__ double sys[];
+  const LaneSlot L{sys + threadIdx.x, kFastBlock}, R{sys + NS * NS * kFastBlock + threadIdx.x, kFastBlock};
+  const Dims d = z.d;
+  const long long q = (long long)blockIdx.x * kFastBlock + threadIdx.x;
+  if (q >= (long long)d.mx * d.my * d.mz) return;
+  const int i = (int)(q % d.mx), rem = (int)(q / d.mx), j = rem % d.my, k = rem / d.my;
+  const int64_t id = d.idx(d.ngg, i, j, k), iq = d.idx(0, i, j, k);
+  NodeStateN<NS> s;
+  double yk[NS], pres;
+  load_node_ns<NS>(z, id, iq, s, yk, pres);
+  int n_sub;
+  double h, h_last;
+  bool capped;
+  substep_plan(dt, s.ts, n_sub, h, h_last, capped);
+  if (capped) atomicOr(err, 2);
+  bool ok = true;
+  for (int n = 0; n < n_sub; ++n) ok &= zero_d_substep_ns<NS>(mc, p.chem_advance_method, h, s, yk, pres, L, R);
+  int taken = n_sub;
+  if (abs(h_last) > 1e-12) {
+    ok &= zero_d_substep_ns<NS>(mc, p.chem_advance_method, h_last, s, yk, pres, L, R);
+    ++taken;
+  }
+  if (!ok) atomicOr(err, 1);
+  store_node_ns<NS>(z, p.n_scalar, id, s, yk, pres);
+  if (nsub_out) nsub_out[iq] = taken;
+}
+
+// Work-queue schedule (see wu_reaction_queue_kernel), optionally over a node list.
+template <int NS>
+__global__ void __launch_bounds__(kFastBlock) wu_reaction_queue_ns_kernel(Zone z, Param p, const Mech *mc, double dt,
+                                                                         int *nsub_out, int *err,
+                                                                         unsigned int *counter,
+                                                                         const unsigned int *list,
+                                                                         const unsigned int *list_count) {
+  extern __shared__ double sys[];
+  const LaneSlot L{sys + threadIdx.x, kFastBlock}, R{sys + NS * NS * kFastBlock + threadIdx.x, kFastBlock};
+  const Dims d = z.d;
+  const unsigned int total = list ? *list_count : (unsigned int)d.mx * d.my * d.mz;
+  const int lane = threadIdx.x & 31;
+  NodeStateN<NS> s;
+  double yk[NS], pres = 0, h = 0, h_last = 0;
+  int n_sub = 0, done = 0, taken = 0;
+  int64_t id = 0, iq = 0;
+  bool ok = true, have = false, exhausted = false;
+  for (;;) {
+    const bool need = !have && !exhausted;
+    const unsigned int mask = __ballot_sync(0xffffffffu, need);
+    if (mask) {
+      unsigned int base = 0;
+      const int leader = __ffs(mask) - 1;
+      if (lane == leader) base = atomicAdd(counter, (unsigned int)__popc(mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        unsigned int node = base + __popc(mask & ((1u << lane) - 1));
+        if (node < total) {
+          if (list) node = list[node];
+          const int i = node % d.mx, rem = node / d.mx, j = rem % d.my, k = rem / d.my;
+          id = d.idx(d.ngg, i, j, k);
+          iq = d.idx(0, i, j, k);
+          load_node_ns<NS>(z, id, iq, s, yk, pres);
+          bool capped;
+          substep_plan(dt, s.ts, n_sub, h, h_last, capped);
+          if (capped) atomicOr(err, 2);
+          done = 0;
+          taken = 0;
+          ok = true;
+          have = true;
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, have)) break;
+    if (have) {
+      const double hh = done < n_sub ? h : h_last;
+      const bool run = done < n_sub || abs(h_last) > 1e-12;
+      if (run) {
+        ok &= zero_d_substep_ns<NS>(mc, p.chem_advance_method, hh, s, yk, pres, L, R);
+        ++taken;
+      }
+      ++done;
+      if (done > n_sub) {
+        if (!ok) atomicOr(err, 1);
+        store_node_ns<NS>(z, p.n_scalar, id, s, yk, pres);
+        if (nsub_out) nsub_out[iq] = taken;
+        have = false;
+      }
+    }
+  }
+}
+
+// Persistent grid of the work-queue kernels: resident blocks per SM x SMs.
+template <class K>
+static long long queue_blocks(K kernel, int block, int smem, int n_sm, long long nodes) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  long long blocks = (long long)n_sm * per_sm;
+  const long long need = (nodes + block - 1) / block;
+  if (blocks > need) blocks = need;
+  return blocks < 1 ? 1 : blocks;
+}
+
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st) {
   finite_rate_chemistry_kernel<<<dim3((z.d.mx + 127) / 128, z.d.my, z.d.mz), 128, 0, st>>>(z, mc);
   return cudaGetLastError();
@@ -273,17 +394,53 @@ cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStre
 
 cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, double dt, int schedule, int *nsub_out,
                                int *err, unsigned int *counter, int n_sm, cudaStream_t st) {
+  const long long total = (long long)z.d.mx * z.d.my * z.d.mz;
+  if (p.n_spec == kMaxSpec) {
+    constexpr int smem = fast_smem_bytes<kMaxSpec>();
+    if (schedule == 0) {
+      wu_reaction_plain_ns_kernel<kMaxSpec><<<(unsigned)((total + kFastBlock - 1) / kFastBlock), kFastBlock, smem, st>>>(
+          z, p, mc, dt, nsub_out, err);
+    } else {
+      cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
+      if (e != cudaSuccess) return e;
+      const long long blocks = queue_blocks(wu_reaction_queue_ns_kernel<kMaxSpec>, kFastBlock, smem, n_sm, total);
+      wu_reaction_queue_ns_kernel<kMaxSpec><<<(unsigned)blocks, kFastBlock, smem, st>>>(z, p, mc, dt, nsub_out, err,
+                                                                                      counter, nullptr, nullptr);
+    }
+    return cudaGetLastError();
+  }
   if (schedule == 0) {
     wu_reaction_plain_kernel<<<dim3((z.d.mx + 127) / 128, z.d.my, z.d.mz), 128, 0, st>>>(z, p, mc, dt, nsub_out, err);
   } else {
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
-    const long long total = (long long)z.d.mx * z.d.my * z.d.mz;
     long long blocks = (long long)n_sm * 8;
     const long long need = (total + 127) / 128;
     if (blocks > need) blocks = need;
-    wu_reaction_queue_kernel<<<(unsigned)blocks, 128, 0, st>>>(z, p, mc, dt, nsub_out, err, counter);
+    wu_reaction_queue_kernel<<<(unsigned)blocks, 128, 0, st>>>(z, p, mc, dt, nsub_out, err, counter, nullptr, nullptr);
   }
+  return cudaGetLastError();
+}
+
+// Work-queue reaction step over the nodes list[0 .. *list_count); the count
+// lives on the device, so the grid covers max_nodes.
+cudaError_t launch_wu_reaction_list(const Zone &z, const Param &p, const Mech *mc, double dt, const unsigned int *list,
+                                    const unsigned int *list_count, long long max_nodes, int *err,
+                                    unsigned int *counter, int n_sm, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return e;
+  if (p.n_spec == kMaxSpec) {
+    constexpr int smem = fast_smem_bytes<kMaxSpec>();
+    const long long blocks = queue_blocks(wu_reaction_queue_ns_kernel<kMaxSpec>, kFastBlock, smem, n_sm, max_nodes);
+    wu_reaction_queue_ns_kernel<kMaxSpec><<<(unsigned)blocks, kFastBlock, smem, st>>>(z, p, mc, dt, nullptr, err,
+                                                                                    counter, list, list_count);
+    return cudaGetLastError();
+  }
+  long long blocks = (long long)n_sm * 8;
+  const long long need = (max_nodes + 127) / 128;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  wu_reaction_queue_kernel<<<(unsigned)blocks, 128, 0, st>>>(z, p, mc, dt, nullptr, err, counter, list, list_count);
   return cudaGetLastError();
 }
 

@@ -27,6 +27,11 @@ struct Kinetics {
   int n_inv[kMaxReac];
   int inv_sp[kMaxReac][kMaxInvolved];
   int inv_f[kMaxReac][kMaxInvolved], inv_b[kMaxReac][kMaxInvolved];
+  // the same stoichiometry dense per species, with bit masks of the species
+  // involved (inv_mask) and of those with a non-zero net coefficient
+  // (net_mask), for loops whose species index is a compile-time constant
+  signed char stf[kMaxReac][kMaxSpec], stb[kMaxReac][kMaxSpec];
+  unsigned int inv_mask[kMaxReac], net_mask[kMaxReac];
 };
 
 // Mixture and mechanism tables in one device block.

@@ -76,6 +76,14 @@ class Mechanism:
     def index(self, name):
         return self.species.index(name.upper())
 
+    def element_mass_fractions(self) -> np.ndarray:
+        """mu[e, k] = a_ek W_e / W_k: mass of element e per mass of species k,
+        so that Z_e = mu @ Y are the element mass fractions (each column sums
+        to 1).  Elements present in no species are dropped."""
+        W_e = np.array([ATOMIC_WEIGHT[el] for el in self.elements])
+        mu = (self.elem_comp * W_e[None, :]).T / self.mw[None, :]
+        return mu[self.elem_comp.sum(axis=0) > 0]
+
     def save(self, path):
         d = {f.name: getattr(self, f.name) for f in dataclasses.fields(self)}
         d["species"] = np.array(self.species)

@@ -202,6 +202,90 @@ long long cfk_kernel_launches(const cfk_ctx *ctx);
 int cfk_local_time_step_static(const cfk_param *param, const cfk_zone *zone, double *dt_min_device, void *stream,
                                char *err, size_t err_len);
 
+/* ---- MLP chemistry surrogate ------------------------------------------- */
+/* No counterpart in the reference: a learned replacement for the reaction
+ * step of cfk_wu_reaction_step, trained on the device from trajectories of
+ * the plain point-implicit integrator.
+ *
+ * Network: 12 standardised inputs (T, ln p, Box-Cox(Y_k) k=0..8, ln dt) ->
+ * three tanh layers of 128 -> 11 outputs (Box-Cox increments of Y_k, dT,
+ * ln of the reaction time scale after the step).  BF16 operands, FP32
+ * accumulation on the tensor cores; everything after the network output
+ * (inverse transform, element-conservation projection, energy-consistent
+ * temperature, gate) is FP64.  Parameters: CFK_SG_NPARAM FP32 weights (four
+ * row-major blocks W0 128x16, W1 128x144, W2 128x144, W3 16x144, biases in
+ * column 15 of W0 and column 128 of the others) and CFK_SG_NNORM floats of
+ * standardisation (in_mean[12], in_rstd[12], out_mean[11], out_std[11],
+ * in_lo[12], in_hi[12], out_scale[11]); output j is learnt as
+ * asinh(g_j / out_scale[j]) standardised (g_j itself where out_scale[j] = 0). */
+#define CFK_SG_NPARAM 41216
+#define CFK_SG_NNORM 81
+#define CFK_SG_NIN 12
+#define CFK_SG_NOUT 11
+
+typedef struct cfk_surrogate_gate {
+  double ood_margin;     /* allowed excursion beyond the training range (standardised units) */
+  double dT_max;         /* |dT| per step (K) above which a node takes the plain integrator */
+  double dT_consistency; /* |network dT - energy-consistent dT| (K) above which it does */
+  double judge_tol_T;    /* judged node: |T_surrogate - T_plain| tolerance (K) */
+  double judge_tol_bc;   /* judged node: max_k |bc(Y_surrogate) - bc(Y_plain)| tolerance (Box-Cox units) */
+  double min_substeps;   /* nodes whose plain step would take fewer substeps (dt / reaction time scale)
+                            stay on the plain integrator: cheap there, and accuracy-critical (induction) */
+  int judge_stride;      /* every judge_stride-th node (rotating by step) also runs the plain integrator; 0 = off */
+  int revert_steps;      /* steps a node that failed the judge stays on the plain integrator */
+} cfk_surrogate_gate;
+
+typedef struct cfk_surrogate_stats {
+  long long cells, surrogate;
+  long long fallback_ood, fallback_ignition, fallback_consistency, fallback_revert, fallback_newton, fallback_cheap;
+  long long judged, judge_failed;
+  double judge_max_dT, judge_mean_dT, judge_max_dbc;
+} cfk_surrogate_stats;
+
+/* Allocate (first call) and initialise the network: Xavier-uniform weights
+ * from seed, zero biases, zero Adam moments.  elem_mu[n_elem][n_spec] holds
+ * the element mass fractions per species (a_ek W_e / W_k) used by the
+ * conservation projection; n_elem <= 4. */
+int cfk_surrogate_init(cfk_ctx *ctx, unsigned long long seed, int n_elem, const double *elem_mu);
+/* Training data from the plain integrator: phase 0 before a reaction step
+ * snapshots (T, p, Y) of every node; phase 1 after it writes one row per node
+ * (node order i fastest) of raw features X[.][12] and targets G[.][11]
+ * (device float arrays). */
+int cfk_surrogate_record(cfk_ctx *ctx, int phase, double dt, float *X, float *G, void *stream);
+/* Standardisation from n rows of (X, G) on the device; the output scales
+ * are the median |g_j| of a strided sample of the rows. */
+int cfk_surrogate_fit_normalization(cfk_ctx *ctx, const float *X, const float *G, long long n);
+/* Adam on the mean squared error of the standardised outputs: epochs passes
+ * over n rows in minibatches of `batch` (a fresh pseudo-random row order per
+ * epoch), learning rate cosine-annealed from lr0 to lr1.  loss_per_epoch
+ * (host double[epochs], may be NULL) receives each epoch's mean loss. */
+int cfk_surrogate_train(cfk_ctx *ctx, const float *X, const float *G, long long n, int epochs, int batch, double lr0,
+                        double lr1, unsigned long long seed, double *loss_per_epoch);
+/* Gradient of the mean loss over the n rows (device float[CFK_SG_NPARAM]),
+ * and the loss itself (host, may be NULL); the weights are not changed. */
+int cfk_surrogate_gradients(cfk_ctx *ctx, const float *X, const float *G, long long n, float *grad_out,
+                            double *loss_out);
+/* Standardised network outputs for n rows of raw features: Y (device
+ * float[n][16], columns 11..15 are padding). */
+int cfk_surrogate_forward(cfk_ctx *ctx, const float *X, long long n, float *Y);
+/* Host copies of the FP32 weights (float[CFK_SG_NPARAM]) and standardisation
+ * (float[CFK_SG_NNORM]); either pointer may be NULL. */
+int cfk_surrogate_get_params(cfk_ctx *ctx, float *weights, float *norm);
+int cfk_surrogate_set_params(cfk_ctx *ctx, const float *weights, const float *norm);
+int cfk_surrogate_default_gate(cfk_surrogate_gate *gate);
+/* Surrogate reaction step over dt at every node (constant volume; a bound Cn
+ * is added after the reaction change).  Nodes outside the training range,
+ * that the plain integrator would finish in fewer than min_substeps
+ * substeps, with |dT| > dT_max, with an inconsistent network dT, whose
+ * energy Newton iteration fails, or that failed the judge within
+ * revert_steps, are integrated by the plain FP64 work-queue kernel instead;
+ * a rotating
+ * 1/judge_stride of the remaining nodes is integrated by it as well and
+ * compared with the surrogate's prediction.  stats (may be NULL) makes the
+ * call synchronise the stream and report the counts. */
+int cfk_surrogate_reaction_step(cfk_ctx *ctx, double dt, const cfk_surrogate_gate *gate, int step_index,
+                                cfk_surrogate_stats *stats, void *stream);
+
 /* ---- measurement ------------------------------------------------------ */
 /* Phases of a step timed with CUDA events when profiling is on (plain steps
  * only; graph replays are not instrumented). */
