@@ -202,6 +202,156 @@ def reacting_bench(args, local, world, dist):
     return out
 
 
+def _reactor_ctx(mech, case, local, seed):
+    """A chemistry context holding `case` (constant-volume reactors) with the
+    surrogate initialised."""
+    import corefl_b200 as cfk
+    param = dict(case.param)
+    param["device"] = local
+    ctx = cfk.Context(param, case.faces)
+    zone = ctx.alloc_zone(case.mx, case.my, case.mz)
+    ctx.set_mechanism(mech)
+    for fld, arr in (("bv", case.bv), ("sv", case.sv), ("jac", case.jac), ("metric", case.metric)):
+        a = np.ascontiguousarray(arr)
+        ctx.h2d(getattr(zone, fld), a.ctypes.data, a.nbytes)
+    ctx.cv_from_bv()
+    ctx.surrogate_init(seed, mech.element_mass_fractions())
+    return ctx, zone
+
+
+def surrogate_bench(args, local):
+    """MLP chemistry surrogate against the plain point-implicit integrator on
+    the batched H2/air reactors (T ~ U[1000,1600] K, p log-uniform in
+    [1,10] atm, phi ~ U[0.5,2], Li-2004, dt = 1e-7 s per step).
+
+    1. training data: the plain work-queue step on `train_cells` reactors for
+       `window` steps, one (state, change) row per reactor and step, recorded
+       on the device; Adam on the device (tcgen05 forward/backward kernels).
+    2. accuracy: unseen reactors, `window` steps from the unburnt state, gated
+       surrogate step (default gate, judge every 64th node) vs the plain step:
+       ignition delay (time of max dT/dt) and peak temperature, max relative
+       error over the reactors that ignite.
+    3. throughput: 2^20 unseen reactors advanced `window` steps by the
+       surrogate path (judge off: this only builds the run's state mix) and
+       then, from that same state, K plain work-queue steps and K gated
+       surrogate steps (default gate, judge on), timed with CUDA events.
+       Metric: reacting cell-steps/s of each."""
+    import torch
+    import mechanism
+    import surrogate as sg
+
+    mech = mechanism.load("li2004")
+    dt, window = 1e-7, args.surrogate_window
+    out = {"workload": "constant-volume H2/air reactors, Li-2004 9s/19r, dt 1e-7 s; T~U[1000,1600] K, "
+                       "p~logU[1,10] atm, phi~U[0.5,2]", "dtype": "bf16 network, fp32 accumulate; fp64 rest"}
+    # 1. training
+    n_train = args.surrogate_train_cells
+    ctx, _ = _reactor_ctx(mech, cases.reactor_batch(mech, n_train, seed=11), local, 11)
+    t0 = time.time()
+    X, G = sg.record_trajectories(ctx, n_train, window, dt, torch, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    t_rec = time.time() - t0
+    t0 = time.time()
+    losses = sg.fit(ctx, X, G, epochs=args.surrogate_epochs, batch=8192, lr0=2e-3, lr1=1e-5, seed=3)
+    torch.cuda.synchronize()
+    t_fit = time.time() - t0
+    weights, norm = ctx.surrogate_get_params()
+    rows = X.shape[0]
+    out["training"] = {"cells": n_train, "steps": window, "rows": rows, "record_s": t_rec, "epochs": args.surrogate_epochs,
+                       "train_s": t_fit, "rows_per_s": rows * args.surrogate_epochs / t_fit,
+                       "loss_first": losses[0], "loss_last": losses[-1]}
+    del X, G
+    ctx.close()
+
+    # 2. accuracy on full trajectories
+    n_acc = args.surrogate_accuracy_cells
+    case = cases.reactor_batch(mech, n_acc, seed=12)
+    T0 = case.bv[5, :n_acc].copy()
+    traj = {}
+    for mode in ("plain", "surrogate"):
+        ctx, zone = _reactor_ctx(mech, case, local, 12)
+        ctx.surrogate_set_params(weights, norm)
+        gate = ctx.surrogate_default_gate()
+        stats = []
+        Ts = torch.empty((window, n_acc), dtype=torch.float64, device=f"cuda:{local}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(window):
+            if mode == "plain":
+                ctx.wu_reaction_step(dt, schedule=1)
+            else:
+                st = ctx.surrogate_reaction_step(dt, gate, s, want_stats=(s % 50 == 49))
+                if st:
+                    stats.append(st)
+            # temperature plane bv[5] after the step (ngg = 0: plane length = cells)
+            ctx.d2d(Ts[s].data_ptr(), zone.bv + 5 * case.P * 8, n_acc * 8)
+        e1.record()
+        torch.cuda.synchronize()
+        traj[mode] = (Ts.cpu().numpy(), e0.elapsed_time(e1), stats)
+        ctx.close()
+    Tp, Ts_ = traj["plain"][0], traj["surrogate"][0]
+    tau_p, pk_p, rise_p = sg.ignition_metrics(dt, T0, Tp)
+    tau_s, pk_s, rise_s = sg.ignition_metrics(dt, T0, Ts_)
+    ign = (rise_p > 20.0) & (tau_p < (window - 50) * dt)
+    st = traj["surrogate"][2]
+    out["accuracy"] = {
+        "cells": n_acc, "steps": window, "ignited": int(ign.sum()),
+        "tau_ign_max_rel_err": float((np.abs(tau_s[ign] - tau_p[ign]) / tau_p[ign]).max()) if ign.any() else None,
+        "T_peak_max_rel_err": float((np.abs(pk_s - pk_p) / pk_p).max()),
+        "T_max_abs_err_K": float(np.abs(Ts_ - Tp).max()),
+        "on_network": sum(x["surrogate"] for x in st) / max(sum(x["cells"] for x in st), 1),
+        "plain_ms": traj["plain"][1], "surrogate_ms": traj["surrogate"][1]}
+
+    # 3. throughput on 2^20 reactors at the run's state mix
+    n = args.reacting_cells
+    case = cases.reactor_batch(mech, n, seed=2026)
+    ctx, zone = _reactor_ctx(mech, case, local, 2026)
+    ctx.surrogate_set_params(weights, norm)
+    # the advance only builds the state mix that is timed below (judge off)
+    adv = ctx.surrogate_default_gate(judge_stride=0)
+    t0 = time.time()
+    for s in range(window):
+        ctx.surrogate_reaction_step(dt, adv, s)
+    ctx.sync()
+    t_adv = time.time() - t0
+    P = case.P
+    planes = {"cv": case.param["n_var"], "bv": 6, "sv": case.param["n_scalar"], "reaction_timeScale": 1}
+    saved = {k: torch.empty(c * P, dtype=torch.float64, device=f"cuda:{local}") for k, c in planes.items()}
+    for k, buf in saved.items():
+        ctx.d2d(buf.data_ptr(), getattr(zone, k), buf.numel() * 8)
+    k_steps = max(args.steps // 10, 2)
+    res = {}
+    nsub = torch.zeros(n, dtype=torch.int32, device=f"cuda:{local}")
+    for mode in ("plain", "surrogate"):
+        for kk, buf in saved.items():
+            ctx.d2d(getattr(zone, kk), buf.data_ptr(), buf.numel() * 8)
+        gate = ctx.surrogate_default_gate()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        e0.record()
+        for s in range(k_steps):
+            if mode == "plain":
+                ctx.wu_reaction_step(dt, schedule=1, nsub_ptr=nsub.data_ptr())
+            else:
+                stats.append(ctx.surrogate_reaction_step(dt, gate, window + s, want_stats=True))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[mode] = {"cells_per_s": n * k_steps / (ms * 1e-3), "ms_per_step": ms / k_steps, "steps": k_steps}
+        if mode == "plain":
+            ns_ = nsub.cpu().numpy()
+            res[mode].update({"substeps_mean": float(ns_.mean()), "substeps_max": int(ns_.max())})
+        else:
+            res[mode]["on_network"] = sum(x["surrogate"] for x in stats) / sum(x["cells"] for x in stats)
+            res[mode]["last_step"] = stats[-1]
+    ctx.close()
+    out["throughput"] = {"cells": n, "state": f"after {window} steps ({window * dt * 1e6:.0f} us)",
+                         "advance_s": t_adv, **res,
+                         "speedup": res["surrogate"]["cells_per_s"] / res["plain"]["cells_per_s"]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -214,6 +364,12 @@ def main():
     ap.add_argument("--no-reacting", action="store_true")
     ap.add_argument("--reacting-only", action="store_true", help="only the batched-reactor measurement")
     ap.add_argument("--reacting-cells", type=int, default=1 << 20)
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--surrogate-only", action="store_true", help="only the MLP surrogate measurement")
+    ap.add_argument("--surrogate-window", type=int, default=600, help="steps of the training/accuracy window")
+    ap.add_argument("--surrogate-train-cells", type=int, default=16384)
+    ap.add_argument("--surrogate-accuracy-cells", type=int, default=2048)
+    ap.add_argument("--surrogate-epochs", type=int, default=200)
     args = ap.parse_args()
     rank, world, local = _env_rank()
     args.warmup = max(args.warmup, 3)
@@ -228,6 +384,10 @@ def main():
     if args.reacting_only:
         torch.cuda.set_device(local)
         print(json.dumps({"reacting": reacting_bench(args, local, 1, None)}), flush=True)
+        return
+    if args.surrogate_only:
+        torch.cuda.set_device(local)
+        print(json.dumps({"surrogate": surrogate_bench(args, local)}), flush=True)
         return
 
     dist = None
@@ -337,6 +497,8 @@ def main():
     ctx.close()
 
     reacting = None if args.no_reacting else reacting_bench(args, local, world, dist)
+    # the surrogate measurement runs on rank 0 only (its window is one GPU's work)
+    surrogate = None if (args.no_surrogate or args.no_reacting or rank != 0) else surrogate_bench(args, local)
 
     if rank == 0:
         cpu = None
@@ -359,6 +521,7 @@ def main():
             "e2e": e2e,
             "clocks": clk.summary(),
             "reacting": reacting,
+            "surrogate": surrogate,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -149,6 +149,7 @@ def lib() -> ctypes.CDLL:
             "cfk_rk3_step_graph": (i, [vp, _DP, vp]),
             "cfk_memcpy_h2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
             "cfk_memcpy_d2h": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
+            "cfk_memcpy_d2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
             "cfk_stream_sync": (i, [vp, vp]),
             "cfk_host_alloc": (i, [ctypes.c_size_t, ctypes.POINTER(vp)]),
             "cfk_host_free": (i, [vp]),
@@ -339,6 +340,9 @@ class Context:
 
     def d2h(self, dst, src, nbytes, stream=None):
         self._ck(self.L.cfk_memcpy_d2h(self.h, dst, src, nbytes, stream), "d2h")
+
+    def d2d(self, dst, src, nbytes, stream=None):
+        self._ck(self.L.cfk_memcpy_d2d(self.h, dst, src, nbytes, stream), "d2d")
 
     @property
     def kernel_launches(self) -> int:

@@ -21,8 +21,9 @@ cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, uns
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
                                        int n_face, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
-cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, double dt, int schedule, int *nsub_out,
-                               int *err, unsigned int *counter, int n_sm, cudaStream_t st);
+cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
+                               int schedule, int *nsub_out, int *err, unsigned int *counter, int n_sm,
+                               cudaStream_t st);
 }  // namespace cfk
 
 using namespace cfk;
@@ -268,6 +269,7 @@ int cfk_set_mechanism(cfk_ctx *c, const cfk_mechanism *m) {
   }
   CFK_CHECK(c, cudaSetDevice(c->hp.device), "cudaSetDevice");
   CFK_CHECK(c, cudaMemcpy(c->d_mech, &h, sizeof(Mech), cudaMemcpyHostToDevice), "mechanism upload");
+  c->h_mech = h;
   c->have_mech = true;
   return CFK_OK;
 }
@@ -288,8 +290,8 @@ int cfk_wu_reaction_step(cfk_ctx *c, double dt, int schedule, int *nsub_out, voi
   if (c->hp.chem_advance_method != 0 && c->hp.chem_advance_method != 1)
     return fail(c, CFK_ERR_ARG, "chem_advance_method must be 0 (explicit) or 1 (point implicit)");
   unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
-  CFK_CHECK(c, launch_wu_reaction(c->z, c->p, c->d_mech, dt, schedule, nsub_out, c->d_err, counter, c->n_sm,
-                                  S(stream)),
+  CFK_CHECK(c, launch_wu_reaction(c->z, c->p, c->d_mech, c->h_mech, dt, schedule, nsub_out, c->d_err, counter,
+                                  c->n_sm, S(stream)),
             "wu_reaction_step");
   c->launches += 1;
   return CFK_OK;
@@ -456,6 +458,10 @@ int cfk_memcpy_d2h(cfk_ctx *c, void *dst, const void *src, size_t bytes, void *s
   CFK_CHECK(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S(stream)), "d2h");
   return CFK_OK;
 }
+int cfk_memcpy_d2d(cfk_ctx *c, void *dst, const void *src, size_t bytes, void *stream) {
+  CFK_CHECK(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, S(stream)), "d2d");
+  return CFK_OK;
+}
 int cfk_stream_sync(cfk_ctx *c, void *stream) {
   CFK_CHECK(c, cudaStreamSynchronize(S(stream)), "stream sync");
   int h_err = 0;
@@ -465,6 +471,7 @@ int cfk_stream_sync(cfk_ctx *c, void *stream) {
       cudaMemset(c->d_err, 0, sizeof(int));
       std::string msg;
       if (h_err & 1) msg += "temperature Newton iteration reached its 1000-iteration cap; ";
+      if (h_err & 4) msg += "surrogate kernel: tensor-core completion wait timed out; ";
       if (h_err & 2) msg += "a node needed more than 100000 reaction substeps (capped); ";
       return fail(c, CFK_ERR_NUMERIC, msg);
     }

@@ -282,8 +282,10 @@ template <int NS>
 __host__ __device__ constexpr int fast_smem_bytes() { return (NS * NS + NS) * kFastBlock * (int)sizeof(double); }
 
 template <int NS>
-__global__ void __launch_bounds__(kFastBlock) wu_reaction_plain_ns_kernel(Zone z, Param p, const Mech *mc, double dt,
+__global__ void __launch_bounds__(kFastBlock) wu_reaction_plain_ns_kernel(Zone z, Param p,
+                                                                         const __grid_constant__ Mech mech, double dt,
                                                                          int *nsub_out, int *err) {
+  const Mech *mc = &mech;
   extern __shared__ double sys[];
   const LaneSlot L{sys + threadIdx.x, kFastBlock}, R{sys + NS * NS * kFastBlock + threadIdx.x, kFastBlock};
   const Dims d = z.d;
@@ -313,11 +315,13 @@ __global__ void __launch_bounds__(kFastBlock) wu_reaction_plain_ns_kernel(Zone z
 
 // Work-queue schedule (see wu_reaction_queue_kernel), optionally over a node list.
 template <int NS>
-__global__ void __launch_bounds__(kFastBlock) wu_reaction_queue_ns_kernel(Zone z, Param p, const Mech *mc, double dt,
+__global__ void __launch_bounds__(kFastBlock) wu_reaction_queue_ns_kernel(Zone z, Param p,
+                                                                         const __grid_constant__ Mech mech, double dt,
                                                                          int *nsub_out, int *err,
                                                                          unsigned int *counter,
                                                                          const unsigned int *list,
                                                                          const unsigned int *list_count) {
+  const Mech *mc = &mech;
   extern __shared__ double sys[];
   const LaneSlot L{sys + threadIdx.x, kFastBlock}, R{sys + NS * NS * kFastBlock + threadIdx.x, kFastBlock};
   const Dims d = z.d;
@@ -392,20 +396,21 @@ cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, double dt, int schedule, int *nsub_out,
-                               int *err, unsigned int *counter, int n_sm, cudaStream_t st) {
+cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
+                               int schedule, int *nsub_out, int *err, unsigned int *counter, int n_sm,
+                               cudaStream_t st) {
   const long long total = (long long)z.d.mx * z.d.my * z.d.mz;
   if (p.n_spec == kMaxSpec) {
     constexpr int smem = fast_smem_bytes<kMaxSpec>();
     if (schedule == 0) {
       wu_reaction_plain_ns_kernel<kMaxSpec><<<(unsigned)((total + kFastBlock - 1) / kFastBlock), kFastBlock, smem, st>>>(
-          z, p, mc, dt, nsub_out, err);
+          z, p, mc_host, dt, nsub_out, err);
     } else {
       cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
       if (e != cudaSuccess) return e;
       const long long blocks = queue_blocks(wu_reaction_queue_ns_kernel<kMaxSpec>, kFastBlock, smem, n_sm, total);
-      wu_reaction_queue_ns_kernel<kMaxSpec><<<(unsigned)blocks, kFastBlock, smem, st>>>(z, p, mc, dt, nsub_out, err,
-                                                                                      counter, nullptr, nullptr);
+      wu_reaction_queue_ns_kernel<kMaxSpec><<<(unsigned)blocks, kFastBlock, smem, st>>>(
+          z, p, mc_host, dt, nsub_out, err, counter, nullptr, nullptr);
     }
     return cudaGetLastError();
   }
@@ -424,15 +429,15 @@ cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, do
 
 // Work-queue reaction step over the nodes list[0 .. *list_count); the count
 // lives on the device, so the grid covers max_nodes.
-cudaError_t launch_wu_reaction_list(const Zone &z, const Param &p, const Mech *mc, double dt, const unsigned int *list,
-                                    const unsigned int *list_count, long long max_nodes, int *err,
-                                    unsigned int *counter, int n_sm, cudaStream_t st) {
+cudaError_t launch_wu_reaction_list(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
+                                    const unsigned int *list, const unsigned int *list_count, long long max_nodes,
+                                    int *err, unsigned int *counter, int n_sm, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess) return e;
   if (p.n_spec == kMaxSpec) {
     constexpr int smem = fast_smem_bytes<kMaxSpec>();
     const long long blocks = queue_blocks(wu_reaction_queue_ns_kernel<kMaxSpec>, kFastBlock, smem, n_sm, max_nodes);
-    wu_reaction_queue_ns_kernel<kMaxSpec><<<(unsigned)blocks, kFastBlock, smem, st>>>(z, p, mc, dt, nullptr, err,
+    wu_reaction_queue_ns_kernel<kMaxSpec><<<(unsigned)blocks, kFastBlock, smem, st>>>(z, p, mc_host, dt, nullptr, err,
                                                                                     counter, list, list_count);
     return cudaGetLastError();
   }

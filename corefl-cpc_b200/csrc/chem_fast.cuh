@@ -11,8 +11,13 @@
 //    destruction rates and the Jacobian are accumulated reaction by reaction
 //    (each accumulator still sums the reactions in mechanism order);
 //  * the NS x NS system matrix and right-hand side live in shared memory,
-//    entry e of lane t at base[e * stride + t], so the pivoted LU's runtime
-//    row indices address shared memory rather than local memory.
+//    entry e of lane t at base[e * stride + t], so the Jacobian's sparse
+//    accumulation and the pivoted LU's runtime row indices address shared
+//    memory rather than local memory;
+//  * the mechanism tables are a __grid_constant__ kernel parameter: uniform
+//    reads through the constant cache;
+//  * divisions by the same value are one reciprocal and products, so results
+//    match the runtime-count path to rounding, not bit for bit.
 #pragma once
 
 #include "chem.cuh"
@@ -99,10 +104,12 @@ struct LaneSlot {
 };
 
 // Column-pivoted LU solve of L x = R in the elimination order of
-// solve_chem_system; L and R are overwritten, x returned in registers.
+// solve_chem_system (divisions by a pivot as one reciprocal each); L and R
+// are overwritten, x returned in registers.
 template <int NS>
 __device__ __forceinline__ void lu_solve_ns(const LaneSlot &L, const LaneSlot &R, double *x) {
   int ipiv[NS];
+  double rdiag[NS];
 #pragma unroll
   for (int n = 0; n < NS; ++n) {
     int ik = n;
@@ -130,9 +137,9 @@ __device__ __forceinline__ void lu_solve_ns(const LaneSlot &L, const LaneSlot &R
       for (int t = 0; t < n; ++t) v -= L(n * NS + t) * L(t * NS + p);
       L(n * NS + p) = v;
     }
-    const double piv = L(n * NS + n);
+    rdiag[n] = 1.0 / L(n * NS + n);
 #pragma unroll
-    for (int m = n + 1; m < NS; ++m) L(m * NS + n) /= piv;
+    for (int m = n + 1; m < NS; ++m) L(m * NS + n) *= rdiag[n];
   }
 #pragma unroll
   for (int m = 0; m < NS; ++m) {
@@ -149,12 +156,12 @@ __device__ __forceinline__ void lu_solve_ns(const LaneSlot &L, const LaneSlot &R
   for (int m = 1; m < NS; ++m)
 #pragma unroll
     for (int t = 0; t < m; ++t) x[m] -= L(m * NS + t) * x[t];
-  x[NS - 1] /= L(NS * NS - 1);
+  x[NS - 1] *= rdiag[NS - 1];
 #pragma unroll
   for (int m = NS - 2; m >= 0; --m) {
 #pragma unroll
     for (int t = m + 1; t < NS; ++t) x[m] -= L(m * NS + t) * x[t];
-    x[m] /= L(m * NS + m);
+    x[m] *= rdiag[m];
   }
 }
 
@@ -301,15 +308,15 @@ __device__ __forceinline__ bool zero_d_substep_ns(const Mech *mc, int method, do
         omega_d[l] += q1 * f + q2 * bq;
       }
     if (method == 1) {
-      const unsigned netm = kn.net_mask[r];
-#pragma unroll
-      for (int m = 0; m < NS; ++m)
-        if (netm >> m & 1u) {
-          const double net = kn.stb[r][m] - kn.stf[r][m];
-#pragma unroll
-          for (int n = 0; n < NS; ++n)
-            if (inv >> n & 1u) L(m * NS + n) += net * (kn.stf[r][n] * q1 - kn.stb[r][n] * q2);
-        }
+      // the matrix is in shared memory: its runtime row/column indices are free
+      const int ni = kn.n_inv[r];
+      for (int qa = 0; qa < ni; ++qa) {
+        const double net = kn.inv_b[r][qa] - kn.inv_f[r][qa];
+        if (net == 0) continue;
+        const int m = kn.inv_sp[r][qa];
+        for (int qb = 0; qb < ni; ++qb)
+          L(m * NS + kn.inv_sp[r][qb]) += net * (kn.inv_f[r][qb] * q1 - kn.inv_b[r][qb] * q2);
+      }
     }
   }
   double omega[NS];
@@ -323,14 +330,17 @@ __device__ __forceinline__ bool zero_d_substep_ns(const Mech *mc, int method, do
 #pragma unroll
   for (int l = 0; l < NS; ++l) c[l] *= 1e+3 / th->imw[l];
   if (method == 1) {
+    // (I - dt J): J_mn / rhoY_n * 1e3 / imw_m, with the 2 NS divisions hoisted
+    double rc[NS], wm[NS];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      rc[n] = c[n] > 1e-25 ? 1.0 / c[n] : 0.0;
+      wm[n] = 1e+3 / th->imw[n];
+    }
 #pragma unroll
     for (int m = 0; m < NS; ++m)
 #pragma unroll
-      for (int n = 0; n < NS; ++n) {
-        const double rhoY = c[n];
-        const double zz = rhoY > 1e-25 ? L(m * NS + n) / rhoY : 0.0;
-        L(m * NS + n) = (m == n ? 1 : 0) - dt * (zz * 1e+3 / th->imw[m]);
-      }
+      for (int n = 0; n < NS; ++n) L(m * NS + n) = (m == n ? 1 : 0) - dt * (L(m * NS + n) * rc[n] * wm[m]);
 #pragma unroll
     for (int l = 0; l < NS; ++l) R(l) = omega[l];
     lu_solve_ns<NS>(L, R, omega);

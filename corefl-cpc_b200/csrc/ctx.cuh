@@ -23,6 +23,7 @@ struct cfk_ctx {
   bool bound = false;
   std::vector<void *> owned;  // device arrays owned by the context
   Mech *d_mech = nullptr;
+  Mech h_mech{};  // host copy, passed by value to the kernels that read it from the constant bank
   bool have_mech = false;
   int n_sm = 148;
   // device scratch: [0] dt bits (u64), [1] error flags (int)

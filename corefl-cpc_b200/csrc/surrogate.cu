@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
         Z0[e] = s;
       }
       for (int l = 0; l < ns; ++l) Yn[l] = sg_boxcox_inv(sg_boxcox(Y0[l]) + rr[l]);
-      sg_project(a.proj, ns, Z0, Yn);
+      const bool projected = sg_project(a.proj, ns, Z0, Yn);
       double qv[5], rY[kMaxSpec];
 #pragma unroll
       for (int l = 0; l < 5; ++l) qv[l] = a.z.cv[id + l * szp];
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
       guess = fmin(fmax(guess, fmax(T0 - 500.0, 200.0)), T0 + 3000.0);
       Tn = guess;
       double pn = 0;
-      const bool ok = temperature_newton(th, ns, Yn, qv[4], qv[0], u * u + v * v + w * w, Tn, pn);
+      const bool ok = projected && temperature_newton(th, ns, Yn, qv[4], qv[0], u * u + v * v + w * w, Tn, pn);
       if (!ok) reason = SG_NEWTON_FAILED;
       else if (fabs(Tn - T0) > a.gate.dT_max) reason = SG_IGNITION;
       else if (fabs(T0 + rr[9] - Tn) > a.gate.dT_consistency) reason = SG_CONSISTENCY;

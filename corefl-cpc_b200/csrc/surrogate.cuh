@@ -110,52 +110,73 @@ __host__ __device__ inline void sg_raw_features(double T, double p, const double
   f[11] = log(dt);
 }
 
-// Weighted least-squares projection of Y onto {mu Y = Z0}: the correction of
-// species k is proportional to (Y_k + 1e-12), so trace species move least.
-// Negative results are clipped and the fractions renormalised to sum 1.
-__device__ inline void sg_project(const SgProj &pj, int ns, const double *Z0, double *Y) {
+// Weighted least-squares projection of Y onto {mu Y = Z0, Y >= 0}: the
+// correction of species k is proportional to (Y_k + 1e-12), so trace species
+// move least; species driven negative are clipped to 0 and frozen, and the
+// projection is repeated over the rest (at most ns passes).  Returns false
+// if the element residual max_e |mu Y - Z0| stays above 1e-10 (the caller
+// then leaves the node to the plain integrator).  Y sums to 1 on success.
+__device__ inline bool sg_project(const SgProj &pj, int ns, const double *Z0, double *Y) {
   const int ne = pj.n_elem;
-  double w[kMaxSpec], A[4][5];
-  for (int k = 0; k < ns; ++k) w[k] = Y[k] + 1e-12;
+  unsigned active = (1u << ns) - 1u;
+  for (int pass = 0; pass < ns; ++pass) {
+    double w[kMaxSpec], A[4][5];
+    for (int k = 0; k < ns; ++k) w[k] = (active >> k & 1u) ? Y[k] + 1e-12 : 0.0;
+    for (int e = 0; e < ne; ++e) {
+      double r = Z0[e];
+      for (int k = 0; k < ns; ++k) r -= pj.mu[e][k] * Y[k];
+      A[e][ne] = r;
+      for (int f = 0; f < ne; ++f) {
+        double acc = 0;
+        for (int k = 0; k < ns; ++k) acc += pj.mu[e][k] * w[k] * pj.mu[f][k];
+        A[e][f] = acc;
+      }
+    }
+    // Gaussian elimination with partial pivoting on the ne x ne system
+    for (int c = 0; c < ne; ++c) {
+      int piv = c;
+      for (int r = c + 1; r < ne; ++r)
+        if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+      if (piv != c)
+        for (int q = 0; q <= ne; ++q) { const double t = A[c][q]; A[c][q] = A[piv][q]; A[piv][q] = t; }
+      if (!(fabs(A[c][c]) > 1e-300)) return false;
+      const double inv = 1.0 / A[c][c];
+      for (int r = c + 1; r < ne; ++r) {
+        const double f = A[r][c] * inv;
+        for (int q = c; q <= ne; ++q) A[r][q] -= f * A[c][q];
+      }
+    }
+    double lam[4];
+    for (int c = ne - 1; c >= 0; --c) {
+      double acc = A[c][ne];
+      for (int q = c + 1; q < ne; ++q) acc -= A[c][q] * lam[q];
+      lam[c] = acc / A[c][c];
+    }
+    bool clipped = false;
+    for (int k = 0; k < ns; ++k) {
+      if (!(active >> k & 1u)) continue;
+      double d = 0;
+      for (int e = 0; e < ne; ++e) d += pj.mu[e][k] * lam[e];
+      Y[k] += w[k] * d;
+      if (Y[k] < 0) {
+        Y[k] = 0;
+        active &= ~(1u << k);
+        clipped = true;
+      }
+    }
+    if (!clipped) break;
+  }
+  double res = 0, sum = 0;
   for (int e = 0; e < ne; ++e) {
     double r = Z0[e];
     for (int k = 0; k < ns; ++k) r -= pj.mu[e][k] * Y[k];
-    A[e][ne] = r;
-    for (int f = 0; f < ne; ++f) {
-      double s = 0;
-      for (int k = 0; k < ns; ++k) s += pj.mu[e][k] * w[k] * pj.mu[f][k];
-      A[e][f] = s;
-    }
+    res = fmax(res, fabs(r));
   }
-  // Gaussian elimination with partial pivoting on the ne x ne system
-  for (int c = 0; c < ne; ++c) {
-    int piv = c;
-    for (int r = c + 1; r < ne; ++r)
-      if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
-    if (piv != c)
-      for (int q = 0; q <= ne; ++q) { const double t = A[c][q]; A[c][q] = A[piv][q]; A[piv][q] = t; }
-    const double inv = 1.0 / A[c][c];
-    for (int r = c + 1; r < ne; ++r) {
-      const double f = A[r][c] * inv;
-      for (int q = c; q <= ne; ++q) A[r][q] -= f * A[c][q];
-    }
-  }
-  double lam[4];
-  for (int c = ne - 1; c >= 0; --c) {
-    double s = A[c][ne];
-    for (int q = c + 1; q < ne; ++q) s -= A[c][q] * lam[q];
-    lam[c] = s / A[c][c];
-  }
-  double sum = 0;
-  for (int k = 0; k < ns; ++k) {
-    double d = 0;
-    for (int e = 0; e < ne; ++e) d += pj.mu[e][k] * lam[e];
-    Y[k] += w[k] * d;
-    if (Y[k] < 0) Y[k] = 0;
-    sum += Y[k];
-  }
+  for (int k = 0; k < ns; ++k) sum += Y[k];
+  if (!(res <= 1e-10) || !(sum > 0)) return false;
   const double inv = 1.0 / sum;
   for (int k = 0; k < ns; ++k) Y[k] *= inv;
+  return true;
 }
 
 }  // namespace cfk

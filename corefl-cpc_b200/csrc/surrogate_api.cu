@@ -33,9 +33,9 @@ cudaError_t launch_sg_adam(float *master, float *m, float *v, const float *parti
                            cudaStream_t st);
 cudaError_t launch_sg_publish(const float *master, uint8_t *w16, cudaStream_t st);
 cudaError_t launch_sg_init(float *master, float *m, float *v, unsigned long long seed, cudaStream_t st);
-cudaError_t launch_wu_reaction_list(const Zone &z, const Param &p, const Mech *mc, double dt, const unsigned int *list,
-                                    const unsigned int *list_count, long long max_nodes, int *err,
-                                    unsigned int *counter, int n_sm, cudaStream_t st);
+cudaError_t launch_wu_reaction_list(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
+                                    const unsigned int *list, const unsigned int *list_count, long long max_nodes,
+                                    int *err, unsigned int *counter, int n_sm, cudaStream_t st);
 
 struct Surrogate {
   uint8_t *w16 = nullptr;
@@ -398,8 +398,8 @@ int cfk_surrogate_reaction_step(cfk_ctx *c, double dt, const cfk_surrogate_gate 
   CFK_CHECK(c, launch_sg_step(c->z, c->d_mech, s->w16, s->norm, g, s->proj, dt, s->list, s->counts, s->judge,
                               s->counts + 1, s->revert, s->cnt, c->d_err, c->n_sm, st),
             "surrogate step");
-  CFK_CHECK(c, launch_wu_reaction_list(c->z, c->p, c->d_mech, dt, s->list, s->counts, n, c->d_err, s->counts + 2,
-                                       c->n_sm, st),
+  CFK_CHECK(c, launch_wu_reaction_list(c->z, c->p, c->d_mech, c->h_mech, dt, s->list, s->counts, n, c->d_err,
+                                       s->counts + 2, c->n_sm, st),
             "fallback reaction step");
   c->launches += 2;
   if (g.judge_stride > 0) {

@@ -179,6 +179,8 @@ int cfk_rk3_step_graph(cfk_ctx *ctx, double *dt_used, void *stream);
 /* ---- host <-> device helpers for callers without a CUDA runtime -------- */
 int cfk_memcpy_h2d(cfk_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes, void *stream);
 int cfk_memcpy_d2h(cfk_ctx *ctx, void *dst_host, const void *src_dev, size_t bytes, void *stream);
+/* device to device (snapshot / restore of zone arrays) */
+int cfk_memcpy_d2d(cfk_ctx *ctx, void *dst_dev, const void *src_dev, size_t bytes, void *stream);
 int cfk_stream_sync(cfk_ctx *ctx, void *stream);
 /* pinned host buffers */
 int cfk_host_alloc(size_t bytes, void **out);
@@ -277,7 +279,8 @@ int cfk_surrogate_default_gate(cfk_surrogate_gate *gate);
  * is added after the reaction change).  Nodes outside the training range,
  * that the plain integrator would finish in fewer than min_substeps
  * substeps, with |dT| > dT_max, with an inconsistent network dT, whose
- * energy Newton iteration fails, or that failed the judge within
+ * element-conservation projection or energy Newton iteration fails
+ * (counted as fallback_newton), or that failed the judge within
  * revert_steps, are integrated by the plain FP64 work-queue kernel instead;
  * a rotating
  * 1/judge_stride of the remaining nodes is integrated by it as well and
