@@ -129,6 +129,15 @@ def _air_param(**kw) -> dict:
     return p
 
 
+def ghost_layers(scheme: int) -> int:
+    """Ghost layers of an inviscid scheme (reference src/Parameter.cpp:196-252)."""
+    if scheme in (71, 72):
+        return 4
+    if scheme in (51, 52):
+        return 3
+    return 2
+
+
 def _reference_scale(rho: float, u: float, p: float) -> tuple[float, float]:
     """rho_ref and v_ref of the reference state (reference src/BoundCond.cpp:274-283):
     v_ref = |u|, or the speed of sound when |u| < 1."""
@@ -138,12 +147,14 @@ def _reference_scale(rho: float, u: float, p: float) -> tuple[float, float]:
     return rho, v
 
 
-def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5) -> Case:
+def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5, reconstruction: int = 2) -> Case:
     """Sod shock tube on x in [0,1] as an nx-by-ny 2-D block (the reference
     runs 1-D problems with 7 nodes in y), outflow on all four faces,
     left (1,0,1) / right (0.125,0,0.1) split at x = 0.5 (the right state is
-    applied to x in [0.5, 1.5] inclusive, reference src/Field.cu:290)."""
-    ngg = 4 if scheme in (71, 72) else 3
+    applied to x in [0.5, 1.5] inclusive, reference src/Field.cu:290).
+    scheme: 52/72 WENO5/7 characteristic, 1 LF, 2 Roe, 3 AUSM+, 4 HLLC with
+    `reconstruction` 1 first order, 2 MUSCL, 3 NND2."""
+    ngg = ghost_layers(scheme)
     xs = np.linspace(0.0, 1.0, nx)
     ys = np.arange(ny) * 0.01
     x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
@@ -159,14 +170,15 @@ def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5) -> Case:
     bv[4] = p
     bv[5] = p * MW_AIR / (rho * R_U)
     rho_ref, v_ref = _reference_scale(1.0, 0.0, 1.0)
-    param = _air_param(dim=2, inviscid_scheme=scheme, cfl=cfl, weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref,
-                       rho_ref=rho_ref)
+    param = _air_param(dim=2, inviscid_scheme=scheme, reconstruction=reconstruction, cfl=cfl,
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref)
     faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
     return Case("sod", nx, ny, 1, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg)
 
 
 def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float = 0.05, reynolds: float = 1000.0,
-              dt: float | None = None, cfl: float = 0.5, ny: int | None = None, nz: int | None = None) -> Case:
+              dt: float | None = None, cfl: float = 0.5, ny: int | None = None, nz: int | None = None,
+              reconstruction: int = 2) -> Case:
     """3-D viscous single-species wave on a curvilinear periodic block:
     x = xi + amp*sin(2 pi eta) sin(2 pi zeta), y = eta, z = zeta on [0,1]^3
     with n nodes per direction (node-based periodicity: node 0 and node n-1
@@ -176,7 +188,7 @@ def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float =
     to give rho U L / mu = Re.  dt: fixed step; None means CFL-controlled."""
     ny = n if ny is None else ny
     nz = n if nz is None else nz
-    ngg = 4 if scheme in (71, 72) else 3
+    ngg = ghost_layers(scheme)
     p0 = 1.0 / GAMMA_AIR
     T0 = p0 * MW_AIR / (1.0 * R_U)
     mu0 = 1.7894e-5 * (T0 / 288.16) ** 1.5 * (288.16 + 110) / (T0 + 110)
@@ -197,7 +209,8 @@ def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float =
     bv[4] = p0
     bv[5] = p0 * MW_AIR / (bv[0] * R_U)
     rho_ref, v_ref = _reference_scale(1.0, 1.0, p0)
-    param = _air_param(dim=3, inviscid_scheme=scheme, viscous_order=2 if viscous else 0, cfl=cfl,
+    param = _air_param(dim=3, inviscid_scheme=scheme, reconstruction=reconstruction,
+                       viscous_order=2 if viscous else 0, cfl=cfl,
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref,
                        fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
     faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]

@@ -11,6 +11,8 @@
 namespace cfk {
 cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t weno_air_init_attributes();
+cudaError_t launch_pv_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t pv_air_init_attributes();
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
                              int rk, int *err, cudaStream_t st);
@@ -52,16 +54,37 @@ struct PhaseScope {
 
 namespace {
 
+// Ghost layers the inviscid scheme reads (reference src/Parameter.cpp:196-252):
+// 4 for WENO7, 3 for WENO5, 2 for the primitive-variable schemes; none for
+// chemistry-only contexts.
+int ghost_layers(int scheme) {
+  if (scheme == 71 || scheme == 72) return 4;
+  if (scheme == 51 || scheme == 52) return 3;
+  return scheme == 0 ? 0 : 2;
+}
+
+// compute_inviscid_flux dispatch (reference src/InviscidScheme.cu:12-26).
+cudaError_t launch_inviscid(const Zone &z, const Param &p, cudaStream_t st, int *n) {
+  if (p.inviscid_scheme == 52 || p.inviscid_scheme == 72) return launch_weno_air(z, p, st, n);
+  return launch_pv_air(z, p, st, n);
+}
+
 int validate(const cfk_param *p, std::string &why) {
   if (p->dim != 2 && p->dim != 3) { why = "dim must be 2 or 3"; return -1; }
   if (p->n_spec < 0 || p->n_spec > kMaxSpec) { why = "n_spec out of range (0..9)"; return -1; }
   if (p->n_var != 5 + p->n_scalar) { why = "n_var must equal 5 + n_scalar"; return -1; }
   if (p->n_scalar < p->n_spec) { why = "n_scalar must be >= n_spec"; return -1; }
   const int s = p->inviscid_scheme;
-  if (!(s == 52 || s == 72 || s == 0)) {
+  if (!(s == 52 || s == 72 || s == 0 || (s >= 1 && s <= 4))) {
     why = "inviscid_scheme " + std::to_string(s) + " is not supported by this build";
     return -1;
   }
+  if (s >= 1 && s <= 4 && !(p->reconstruction >= 1 && p->reconstruction <= 3)) {
+    why = "reconstruction must be 1 (first order), 2 (MUSCL) or 3 (NND2) for inviscid_scheme 1-4";
+    return -1;
+  }
+  if (s >= 1 && s <= 4 && !(p->limiter == 0 || p->limiter == 1)) { why = "limiter must be 0 or 1"; return -1; }
+  if (s == 2 && !(p->entropy_fix_factor >= 0)) { why = "entropy_fix_factor must be >= 0"; return -1; }
   if (p->viscous_order != 0 && p->viscous_order != 2) { why = "viscous_order must be 0 or 2"; return -1; }
   if (p->sensor_threshold > 1e-10) { why = "hybrid shock-sensor schemes are not supported (shockSensor_threshold must be 0)"; return -1; }
   if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
@@ -74,7 +97,10 @@ int validate(const cfk_param *p, std::string &why) {
   // The WENO weights are normalised through products of two (eps + beta)^2
   // terms; eps = 1e-40 * weno_eps_scale must stay above 1e-70 so that those
   // products (>= eps^4) remain normal numbers.
-  if (s != 0 && !(p->weno_eps_scale >= 1e-30)) { why = "weno_eps_scale must be >= 1e-30 ((rho_ref*v_ref)^2)"; return -1; }
+  if ((s == 52 || s == 72) && !(p->weno_eps_scale >= 1e-30)) {
+    why = "weno_eps_scale must be >= 1e-30 ((rho_ref*v_ref)^2)";
+    return -1;
+  }
   for (int n = 0; n < p->n_face; ++n) {
     const cfk_face &f = p->faces[n];
     if (f.face < 0 || f.face > 2 || (f.direction != -1 && f.direction != 1) ||
@@ -111,6 +137,7 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   e = cudaSetDevice(param->device);
   if (e != cudaSuccess) return CFK_ERR_CUDA;
   e = weno_air_init_attributes();
+  if (e == cudaSuccess) e = pv_air_init_attributes();
   if (e != cudaSuccess) {
     fprintf(stderr, "cfk_create: kernel attribute setup failed (%s)\n", cudaGetErrorString(e));
     return CFK_ERR_CUDA;
@@ -156,7 +183,7 @@ const char *cfk_last_error(const cfk_ctx *c) { return c ? c->err.c_str() : "null
 int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   if (!c || !zn) return CFK_ERR_ARG;
   if (zn->mx < 1 || zn->my < 1 || zn->mz < 1) return fail(c, CFK_ERR_ARG, "zone extents must be positive");
-  const int need_g = c->hp.inviscid_scheme == 72 ? 4 : (c->hp.inviscid_scheme == 0 ? 0 : 3);
+  const int need_g = ghost_layers(c->hp.inviscid_scheme);
   if (zn->ngg < need_g) return fail(c, CFK_ERR_ARG, "ngg too small for the inviscid scheme");
   if ((c->hp.dim == 2) != (zn->mz == 1)) return fail(c, CFK_ERR_ARG, "dim does not match mz");
   if (c->hp.inviscid_scheme != 0 && (!zn->cv || !zn->bv || !zn->qn || !zn->dq || !zn->metric || !zn->jac))
@@ -182,7 +209,7 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
 int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
   if (!c || !out) return CFK_ERR_ARG;
   CFK_CHECK(c, cudaSetDevice(c->hp.device), "cudaSetDevice");
-  const int g = c->hp.inviscid_scheme == 72 ? 4 : (c->hp.inviscid_scheme == 0 ? 0 : 3);
+  const int g = ghost_layers(c->hp.inviscid_scheme);
   cfk_zone zn{};
   zn.mx = mx; zn.my = my; zn.mz = mz; zn.ngg = g;
   const size_t P = (size_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g), N = (size_t)mx * my * mz;
@@ -309,7 +336,7 @@ int cfk_compute_viscous_flux(cfk_ctx *c, void *stream) {
 int cfk_compute_inviscid_flux(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
   int n = 0;
-  CFK_CHECK(c, launch_weno_air(c->z, c->p, S(stream), &n), "inviscid flux");
+  CFK_CHECK(c, launch_inviscid(c->z, c->p, S(stream), &n), "inviscid flux");
   c->launches += n;
   return CFK_OK;
 }
@@ -379,7 +406,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
-      CFK_CHECK(c, launch_weno_air(z, p, st, &n), "inviscid flux");
+      CFK_CHECK(c, launch_inviscid(z, p, st, &n), "inviscid flux");
     }
     {
       PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
