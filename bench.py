@@ -118,7 +118,7 @@ def cpu_baseline_sample(target_s: float = 15.0, n: int = 49):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle  # test/baseline infrastructure only
 
-    case = cases.sine_wave(n=n, scheme=72, viscous=True, cfl=0.5)
+    case = cases.sine_wave(n=n, scheme=args.scheme, viscous=True, cfl=0.5, reconstruction=args.reconstruction)
     z = pyoracle.OracleZone(case)
     z.initialize()
     z.step()  # warm
@@ -359,6 +359,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_NODES, help="nodes per direction (default 257)")
+    ap.add_argument("--scheme", type=int, default=72,
+                    help="inviscid_scheme: 72/52 WENO7/5 characteristic (default 72), 1 LF, 2 Roe, 3 AUSM+, 4 HLLC")
+    ap.add_argument("--reconstruction", type=int, default=2, help="for schemes 1-4: 1 first order, 2 MUSCL, 3 NND2")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reacting", action="store_true")
@@ -401,7 +404,7 @@ def main():
         torch.cuda.set_device(0)
 
     n = args.n
-    case = cases.sine_wave(n=n, scheme=72, viscous=True, cfl=0.5)
+    case = cases.sine_wave(n=n, scheme=args.scheme, viscous=True, cfl=0.5, reconstruction=args.reconstruction)
     param = dict(case.param)
     param["device"] = local
     ctx = cfk.Context(param, case.faces)
@@ -443,27 +446,40 @@ def main():
     nodes = case.N
     value = nodes * args.steps * world / (ms * 1e-3)
 
-    # ---- roofline of the dominant kernel (the three WENO sweeps)
+    # ---- roofline of the dominant kernel (the three inviscid sweeps)
     inv_ms, inv_k = phases["inviscid"]
     faces_per_launch = ((case.mx + 1) * case.my * case.mz + case.mx * (case.my + 1) * case.mz +
                         case.mx * case.my * (case.mz + 1)) / 3.0
     avg_launch_ms = inv_ms / max(inv_k, 1)
-    achieved = FLOPS_PER_FACE_WENO7_CH * faces_per_launch / (avg_launch_ms * 1e-3) / 1e12
-    peak = cfk.measure_fp64_peak()
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "weno_air_traffic.json")
-    if os.path.exists(tf):
-        with open(tf) as f:
-            traffic = json.load(f).get("bytes_per_launch_257")
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "weno_air_flux_diff<dir,7> (x/y/z sweeps)",
-                "peak_source": "measured live: cfk_measure_fp64_peak FMA-chain kernel",
-                "avg_launch_ms": avg_launch_ms, "flops_per_launch": FLOPS_PER_FACE_WENO7_CH * faces_per_launch}
     hbm_peak = None
     mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(mp):
         with open(mp) as f:
             hbm_peak = json.load(f).get("hbm_gbs")
+    if args.scheme == 72:
+        achieved = FLOPS_PER_FACE_WENO7_CH * faces_per_launch / (avg_launch_ms * 1e-3) / 1e12
+        peak = cfk.measure_fp64_peak()
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "weno_air_traffic.json")
+        if os.path.exists(tf):
+            with open(tf) as f:
+                traffic = json.load(f).get("bytes_per_launch_257")
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": traffic, "kernel": "weno_air_flux_diff<dir,7> (x/y/z sweeps)",
+                    "peak_source": "measured live: cfk_measure_fp64_peak FMA-chain kernel",
+                    "avg_launch_ms": avg_launch_ms, "flops_per_launch": FLOPS_PER_FACE_WENO7_CH * faces_per_launch}
+    else:
+        # primitive-variable schemes are HBM-bound: algorithmic bytes per node
+        # and direction = bv[5] + metric[3] + jac + dq[5] read-modify-write
+        # (Roe: + the six other metric terms of the entropy-fix width)
+        per_node = 8 * (5 + 3 + 1 + 10 + (6 if args.scheme == 2 else 0))
+        achieved = per_node * case.N / (avg_launch_ms * 1e-3) / 1e9
+        peak = hbm_peak
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak if peak else None, "traffic": None,
+                    "kernel": f"pv_air_flux_diff<dir,{args.scheme},{args.reconstruction}> (x/y/z sweeps)",
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs", "avg_launch_ms": avg_launch_ms,
+                    "bytes_per_launch": per_node * case.N}
 
     # ---- end to end through the C ABI with pinned host buffers
     P = case.P
@@ -509,8 +525,11 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "3-D viscous sine wave, curvilinear periodic block, WENO7-ch + 2nd-order "
-                                   "viscous, SSP-RK3 CFL 0.5 (device dt)", "nodes": f"{n}^3", "global_nodes": nodes * world,
+            "config": {"workload": "3-D viscous sine wave, curvilinear periodic block, "
+                                   + ("WENO7-ch" if args.scheme == 72 else f"inviscid_scheme {args.scheme} "
+                                      f"reconstruction {args.reconstruction}") +
+                                   " + 2nd-order viscous, SSP-RK3 CFL 0.5 (device dt)",
+                       "nodes": f"{n}^3", "global_nodes": nodes * world,
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cv alone "
                        f"{5 * P * 8 / 1e6:.0f} MB)"},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
