@@ -227,8 +227,15 @@ def perturbed(case: Case, seed: int = 0, amp: float = 1e-3) -> Case:
         bv[l] = bv[l] + amp * scale * rng.standard_normal(bv[l].shape)
     bv[0] = np.abs(bv[0])
     bv[4] = np.abs(bv[4])
-    bv[5] = bv[4] * MW_AIR / (bv[0] * R_U)
+    bv[5] = bv[4] / (bv[0] * _gas_constant(case))
     return dataclasses.replace(case, bv=bv)
+
+
+def _gas_constant(case: Case) -> np.ndarray:
+    """Specific gas constant per padded node: air, or R_u sum Y_k / W_k."""
+    if case.mech is None:
+        return np.full(case.P, R_AIR)
+    return R_U * (case.sv[:case.mech.n_spec] / case.mech.mw[:, None]).sum(axis=0)
 
 
 def _mix_param(mech, **kw) -> dict:
@@ -291,3 +298,110 @@ def reactor_batch(mech, n: int, seed: int = 0) -> Case:
     X[:, mech.index("N2")] = 3.76
     X /= X.sum(axis=1, keepdims=True)
     return reactor(mech, T, p, X)
+
+
+def without_reactions(mech):
+    """Copy of a mechanism with its reaction list emptied (non-reacting
+    mixture flow: species, thermo and transport only)."""
+    d = {f.name: getattr(mech, f.name) for f in dataclasses.fields(mech)}
+    for name, v in d.items():
+        if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == mech.n_reac and name not in (
+                "mw", "t_low", "t_mid", "t_high", "low", "high", "geometry", "LJ_potent_inv", "vis_coeff",
+                "ZRotF298", "WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8", "binary_diffusivity_coeff",
+                "kb_over_eps_jk", "elem_comp") and mech.n_reac != mech.n_spec:
+            d[name] = v[:0]
+    return type(mech)(**d)
+
+
+def _mix_reference(rho, u, p, gamma_est=1.4):
+    """rho_ref and v_ref of a mixture reference state: v_ref = |u|, or an
+    estimate of the sound speed when |u| < 1 (reference src/BoundCond.cpp:274-283
+    uses the mixture's own sound speed; only the WENO epsilon depends on it)."""
+    v = abs(u) if abs(u) >= 1 else math.sqrt(gamma_est * p / rho)
+    return rho, v
+
+
+def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool = False, left=None, right=None,
+             length: float = 0.1) -> Case:
+    """Shock tube of a mixture as an nx-by-ny 2-D block on x in [0, length],
+    outflow on all faces, split at the middle.  States are dicts with
+    rho [kg/m^3], p [Pa] and Y (mass fractions by species name).  Default:
+    the high-pressure state of the reference's reactive shock-tube example
+    (rho 0.18075, p 35594, H2/O2/Ar 0.0128/0.1014/0.8859 by mass) on the
+    left, its low-pressure one (rho 0.072, p 7173) with 20 % O2 / 80 % Ar on
+    the right: a shock, a contact carrying a composition jump and an
+    expansion.  `reacting` keeps the mechanism's reactions."""
+    m = mech if reacting else without_reactions(mech)
+    if left is None:
+        left = dict(rho=0.18075, p=35594.0, Y={"H2": 0.012772428, "O2": 0.101362139, "AR": 0.885865433})
+    if right is None:
+        right = dict(rho=0.072, p=7173.0, Y={"O2": 0.2, "AR": 0.8})
+    ngg = ghost_layers(scheme)
+    xs = np.linspace(0.0, length, nx)
+    ys = np.arange(ny) * length / 100.0
+    x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
+    y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
+    z = np.zeros_like(x)
+    jac, metric, xg = metrics(x, y, z, ngg)
+    P = jac.size
+    ns = m.n_spec
+    yl, yr = np.zeros(ns), np.zeros(ns)
+    for k, v in left["Y"].items():
+        yl[m.index(k)] = v
+    for k, v in right["Y"].items():
+        yr[m.index(k)] = v
+    rside = xg > 0.5 * length
+    sv = np.where(rside[None, :], yr[:, None], yl[:, None])
+    bv = np.zeros((6, P))
+    bv[0] = np.where(rside, right["rho"], left["rho"])
+    bv[4] = np.where(rside, right["p"], left["p"])
+    Rm = R_U * (sv / m.mw[:, None]).sum(axis=0)
+    bv[5] = bv[4] / (bv[0] * Rm)
+    rho_ref, v_ref = _mix_reference(left["rho"], 0.0, left["p"])
+    param = _mix_param(m, dim=2, inviscid_scheme=scheme, cfl=0.5, weno_eps_scale=(rho_ref * v_ref) ** 2,
+                       v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac)
+    faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
+    return Case("mix_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m)
+
+
+def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int | None = None,
+             nz: int | None = None, length: float = 2e-3, reacting: bool = False, T0: float = 600.0,
+             dt: float | None = None) -> Case:
+    """Curvilinear periodic 3-D block of a non-uniform H2/N2 - air mixture:
+    x = xi + 0.05 sin(2 pi eta) sin(2 pi zeta) on [0, length]^3 (node-based
+    periodicity), mixture fraction Z = 0.5 + 0.4 sin(2 pi x / length) between
+    a fuel stream (H2 : N2 = 1 : 1 by mole) and air, T = T0 + 50 sin(2 pi y),
+    p = 1 atm, u = 50 m/s: viscous stress, heat conduction and
+    mixture-averaged species diffusion are all active."""
+    m = mech if reacting else without_reactions(mech)
+    ny = n if ny is None else ny
+    nz = n if nz is None else nz
+    ngg = ghost_layers(scheme)
+    xi, eta, zeta = np.linspace(0, 1, n), np.linspace(0, 1, ny), np.linspace(0, 1, nz)
+    Z3, Y3, X3 = np.meshgrid(zeta, eta, xi, indexing="ij")
+    x = (X3 + 0.05 * np.sin(2 * np.pi * Y3) * np.sin(2 * np.pi * Z3)) * length
+    jac, metric, xg = metrics(x, Y3 * length, Z3 * length, ngg)
+    P = jac.size
+    ns = m.n_spec
+    Xf, Xa = np.zeros(ns), np.zeros(ns)
+    Xf[m.index("H2")], Xf[m.index("N2")] = 0.5, 0.5
+    Xa[m.index("O2")], Xa[m.index("N2")] = 0.21, 0.79
+    Yf, Ya = mole_to_mass(m, Xf), mole_to_mass(m, Xa)
+    Zm = 0.5 + 0.4 * np.sin(2 * np.pi * xg / length)
+    sv = Zm[None, :] * Yf[:, None] + (1 - Zm[None, :]) * Ya[:, None]
+    # ghost nodes take the same analytic fields (periodic block)
+    Rm = R_U * (sv / m.mw[:, None]).sum(axis=0)
+    shape = (nz + 2 * ngg, ny + 2 * ngg, n + 2 * ngg)
+    jj = np.broadcast_to(np.arange(-ngg, ny + ngg)[None, :, None], shape).reshape(-1)
+    T = T0 + 50.0 * np.sin(2 * np.pi * jj / (ny - 1))
+    bv = np.zeros((6, P))
+    bv[4] = 101325.0
+    bv[5] = T
+    bv[0] = bv[4] / (Rm * T)
+    bv[1] = 50.0
+    rho_ref, v_ref = _mix_reference(float(bv[0].mean()), 50.0, 101325.0)
+    param = _mix_param(m, dim=3, inviscid_scheme=scheme, viscous_order=2 if viscous else 0, cfl=0.5,
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
+                       fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
+    faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]
+    return Case("mix_wave", n, ny, nz, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m)

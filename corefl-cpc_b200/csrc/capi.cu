@@ -13,6 +13,10 @@ cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int 
 cudaError_t weno_air_init_attributes();
 cudaError_t launch_pv_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t pv_air_init_attributes();
+cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
+cudaError_t weno_mix_init_attributes();
+cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
+cudaError_t viscous_mix_init_attributes();
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
                              int rk, int *err, cudaStream_t st);
@@ -63,10 +67,17 @@ int ghost_layers(int scheme) {
   return scheme == 0 ? 0 : 2;
 }
 
-// compute_inviscid_flux dispatch (reference src/InviscidScheme.cu:12-26).
-cudaError_t launch_inviscid(const Zone &z, const Param &p, cudaStream_t st, int *n) {
-  if (p.inviscid_scheme == 52 || p.inviscid_scheme == 72) return launch_weno_air(z, p, st, n);
+// compute_inviscid_flux dispatch (reference src/InviscidScheme.cu:12-26);
+// th: host copy of the mixture tables, nullptr for air.
+cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, int *n) {
+  if (p.inviscid_scheme == 52 || p.inviscid_scheme == 72)
+    return th ? launch_weno_mix(z, p, *th, st, n) : launch_weno_air(z, p, st, n);
   return launch_pv_air(z, p, st, n);
+}
+
+// compute_viscous_flux dispatch (reference src/ViscousScheme.cu:7-73).
+cudaError_t launch_viscous(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, int *n) {
+  return th ? launch_viscous_mix(z, p, *th, st, n) : launch_viscous_air(z, p, st, n);
 }
 
 int validate(const cfk_param *p, std::string &why) {
@@ -88,8 +99,20 @@ int validate(const cfk_param *p, std::string &why) {
   if (p->viscous_order != 0 && p->viscous_order != 2) { why = "viscous_order must be 0 or 2"; return -1; }
   if (p->sensor_threshold > 1e-10) { why = "hybrid shock-sensor schemes are not supported (shockSensor_threshold must be 0)"; return -1; }
   if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
-  if (p->n_spec > 0 && s != 0) {
-    why = "the mixture model is supported for chemistry-only contexts (inviscid_scheme 0) in this build";
+  if (p->n_spec > 0 && s != 0 && !(s == 52 || s == 72)) {
+    why = "the mixture model is supported with WENO5/7 characteristic fluxes (52, 72) in this build";
+    return -1;
+  }
+  if (p->n_spec > 0 && s != 0 && p->n_spec != kMaxSpec) {
+    why = "the mixture flux kernels are built for 9 species";
+    return -1;
+  }
+  if (p->n_spec > 0 && p->n_scalar != p->n_spec) {
+    why = "passive scalars beside the species are not supported (n_scalar must equal n_spec)";
+    return -1;
+  }
+  if (p->n_spec > 0 && p->viscous_order == 2 && p->gradPInDiffusionFlux) {
+    why = "gradPInDiffusionFlux is not supported";
     return -1;
   }
   if (s == 0 && p->n_spec == 0) { why = "inviscid_scheme 0 (no flux) is for reacting mixtures only"; return -1; }
@@ -138,6 +161,8 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   if (e != cudaSuccess) return CFK_ERR_CUDA;
   e = weno_air_init_attributes();
   if (e == cudaSuccess) e = pv_air_init_attributes();
+  if (e == cudaSuccess) e = weno_mix_init_attributes();
+  if (e == cudaSuccess) e = viscous_mix_init_attributes();
   if (e != cudaSuccess) {
     fprintf(stderr, "cfk_create: kernel attribute setup failed (%s)\n", cudaGetErrorString(e));
     return CFK_ERR_CUDA;
@@ -190,6 +215,10 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
     return fail(c, CFK_ERR_ARG, "cv, bv, qn, dq, metric and jac are required");
   if (c->hp.n_spec > 0 && (!zn->cv || !zn->bv || !zn->sv || !zn->jac || !zn->reaction_timeScale))
     return fail(c, CFK_ERR_ARG, "cv, bv, sv, jac and reaction_timeScale are required for reacting mixtures");
+  if (c->hp.n_spec > 0 && c->hp.inviscid_scheme != 0 &&
+      (!zn->acoustic_speed || !zn->gamma || !zn->mul || !zn->thermal_conductivity || !zn->rho_D))
+    return fail(c, CFK_ERR_ARG,
+                "acoustic_speed, gamma, mul, thermal_conductivity and rho_D are required for the mixture flow path");
   if (c->hp.viscous_order > 0 && !zn->mul) return fail(c, CFK_ERR_ARG, "mul is required for viscous runs");
   if (c->hp.n_scalar > 0 && !zn->sv) return fail(c, CFK_ERR_ARG, "sv is required when n_scalar > 0");
   // 32-bit plane extents, as in the reference's int indexing
@@ -235,6 +264,12 @@ int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
 }
 
 static const Thermo *thermo_of(cfk_ctx *c) { return c->have_mech ? &c->d_mech->th : nullptr; }
+// host copy of the mixture tables for kernels that take them by value
+static const Thermo *thermo_host(cfk_ctx *c) { return c->have_mech ? &c->h_mech.th : nullptr; }
+static int need_mech_for_mixture(cfk_ctx *c) {
+  if (c->hp.n_spec > 0 && !c->have_mech) return fail(c, CFK_ERR_STATE, "mixture context without a mechanism");
+  return CFK_OK;
+}
 
 int cfk_set_mechanism(cfk_ctx *c, const cfk_mechanism *m) {
   if (!c || !m) return CFK_ERR_ARG;
@@ -327,16 +362,19 @@ int cfk_wu_reaction_step(cfk_ctx *c, double dt, int schedule, int *nsub_out, voi
 int cfk_compute_viscous_flux(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
   if (c->hp.viscous_order == 0) return CFK_OK;
+  if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
-  CFK_CHECK(c, launch_viscous_air(c->z, c->p, S(stream), &n), "viscous flux");
+  CFK_CHECK(c, launch_viscous(c->z, c->p, thermo_host(c), S(stream), &n), "viscous flux");
   c->launches += n;
   return CFK_OK;
 }
 
 int cfk_compute_inviscid_flux(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
+  if (c->hp.inviscid_scheme == 0) return fail(c, CFK_ERR_STATE, "inviscid_scheme 0 has no flux");
+  if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
-  CFK_CHECK(c, launch_inviscid(c->z, c->p, S(stream), &n), "inviscid flux");
+  CFK_CHECK(c, launch_inviscid(c->z, c->p, thermo_host(c), S(stream), &n), "inviscid flux");
   c->launches += n;
   return CFK_OK;
 }
@@ -385,6 +423,8 @@ int cfk_local_time_step(cfk_ctx *c, double *dt_out, void *stream) {
 
 // The body of one RK3 step, issued on one stream with no host synchronisation.
 static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
+  if (c->hp.inviscid_scheme == 0) return fail(c, CFK_ERR_STATE, "inviscid_scheme 0 contexts have no RK3 step");
+  if (int r = need_mech_for_mixture(c)) return r;
   const Zone &z = c->z;
   const Param &p = c->p;
   const Thermo *th = thermo_of(c);
@@ -402,11 +442,16 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order == 2) {
       PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
-      CFK_CHECK(c, launch_viscous_air(z, p, st, &n), "viscous flux");
+      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
+    }
+    if (c->have_mech && p.n_reac > 0) {
+      // explicit chemical source of a reacting mixture (reference src/RK.cuh:147-149)
+      CFK_CHECK(c, launch_finite_rate_chemistry(z, c->d_mech, st), "finite_rate_chemistry");
+      ++n;
     }
     {
       PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
-      CFK_CHECK(c, launch_inviscid(z, p, st, &n), "inviscid flux");
+      CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");
     }
     {
       PhaseScope ps(c, CFK_PH_UPDATE, st, &n);

@@ -1,0 +1,336 @@
+// Fused characteristic WENO flux + flux difference for a reacting mixture
+// (NS species, thermally perfect, NASA-7 thermo).
+//
+// Restates compute_convective_term_weno_{x,y,z} with the mixture branch of
+// the characteristic reconstruction (reference src/WENO.cu:1096-1469) and
+// compute_derivative_{x,y,z} (:1544, 2219, 2885) in the stage / faces / diff
+// structure of weno_air.cu:
+//   stage — Q[5], the species densities rho*Y_k, the face-normal flux
+//           G = (rho U, rho u U + p k_x, ..., (rho E + p) U), U, p, J and the
+//           spectral radius |U| + c|grad k| (c from the acoustic-speed array)
+//           of every stencil point, in shared memory;
+//   faces — Roe average of u, v, w, Y_k and T, mixture gamma and c from the
+//           NASA-7 cp at the averaged temperature, the five characteristic
+//           fields with the species coupling terms (beta_k = (gamma R_k T -
+//           (gamma-1) h_k) / c^2), NS species fields (rho Y_k - Y~_k rho),
+//           LLF split, WENO5-JS / WENO7-Z, back projection;
+//   diff  — dq -= F(n+1/2) - F(n-1/2) for all 5 + NS variables.
+// The mixture tables are a __grid_constant__ parameter (constant bank).
+#include "cfk_common.cuh"
+#include "chem_fast.cuh"
+#include "thermo.cuh"
+#include "weno.cuh"
+
+namespace cfk {
+
+namespace {
+
+// staged values per point: Q0..4, G0..4, U, p, J, lambda, rhoY[NS]
+template <int NS>
+struct MixVals {
+  static constexpr int U = 10, P = 11, J = 12, LAM = 13, Y0 = 14, N = 14 + NS;
+};
+
+template <int DIR, int ORD, int NS>
+struct MixTile {
+  static constexpr int R = ORD == 7 ? 3 : 2;
+  static constexpr int NPF = 2 * R + 2;
+  static constexpr int TN = DIR == 0 ? 63 : 15;
+  static constexpr int C = DIR == 0 ? 4 : 16;
+  static constexpr int NF = TN + 1;
+  static constexpr int NPT = TN + 2 * R + 2;
+  static constexpr int NT = 256;
+  static constexpr int NQ = MixVals<NS>::N;
+  static constexpr int NV = 5 + NS;
+  __device__ static int spt(int q, int c, int t) {
+    return DIR == 0 ? (q * C + c) * NPT + t : (q * NPT + t) * C + c;
+  }
+  __device__ static int sfl(int v, int c, int t) {
+    return DIR == 0 ? (v * C + c) * NF + t : (v * NF + t) * C + c;
+  }
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(NQ * C * NPT + NV * C * NF); }
+};
+
+}  // namespace
+
+template <int DIR, int ORD, int NS>
+__global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref, const __grid_constant__ Thermo thermo) {
+  using T = MixTile<DIR, ORD, NS>;
+  using V = MixVals<NS>;
+  constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
+  const Thermo *th = &thermo;
+  extern __shared__ double sm[];
+  double *spts = sm;
+  double *sflx = sm + T::NQ * C * NPT;
+
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), szq = d.plane(0);
+  const int m = d.ext(DIR);
+  int n0, cbase, cfix;
+  if (DIR == 0) { n0 = blockIdx.x * TN; cbase = blockIdx.y * C; cfix = blockIdx.z; }
+  else { n0 = blockIdx.y * TN; cbase = blockIdx.x * C; cfix = blockIdx.z; }
+  const int ncol_max = DIR == 0 ? d.my : d.mx;
+  auto node_idx = [&](int g_, int c, int a) -> int64_t {
+    const int cc = cbase + c;
+    if (DIR == 0) return d.idx(g_, a, cc, cfix);
+    if (DIR == 1) return d.idx(g_, cc, a, cfix);
+    return d.idx(g_, cc, cfix, a);
+  };
+  auto split = [&](int item, int n_t, int &c, int &t) {
+    if (DIR == 0) { c = item / n_t; t = item - c * n_t; }
+    else { t = item / C; c = item - t * C; }
+  };
+  const int mmo = 3 * DIR;
+
+  // ---- stage ------------------------------------------------------------
+  for (int item = threadIdx.x; item < NPT * C; item += T::NT) {
+    int c, t;
+    split(item, NPT, c, t);
+    const int a = n0 - 1 - R + t;
+    if (cbase + c >= ncol_max || a > m + R) continue;
+    const int64_t id = node_idx(g, c, a);
+    const double q0 = z.cv[id], q1 = z.cv[id + sz], q2 = z.cv[id + 2 * sz], q3 = z.cv[id + 3 * sz],
+                 q4 = z.cv[id + 4 * sz];
+    const double m0 = z.metric[id + mmo * sz], m1 = z.metric[id + (mmo + 1) * sz], m2 = z.metric[id + (mmo + 2) * sz];
+    const double Uk = (q1 * m0 + q2 * m1 + q3 * m2) / q0;
+    const double pk = z.bv[id + 4 * sz];
+    double *s = spts;
+    s[T::spt(0, c, t)] = q0;
+    s[T::spt(1, c, t)] = q1;
+    s[T::spt(2, c, t)] = q2;
+    s[T::spt(3, c, t)] = q3;
+    s[T::spt(4, c, t)] = q4;
+    s[T::spt(5, c, t)] = q0 * Uk;
+    s[T::spt(6, c, t)] = fma(q1, Uk, pk * m0);
+    s[T::spt(7, c, t)] = fma(q2, Uk, pk * m1);
+    s[T::spt(8, c, t)] = fma(q3, Uk, pk * m2);
+    s[T::spt(9, c, t)] = (q4 + pk) * Uk;
+    s[T::spt(V::U, c, t)] = Uk;
+    s[T::spt(V::P, c, t)] = pk;
+    s[T::spt(V::J, c, t)] = z.jac[id];
+    s[T::spt(V::LAM, c, t)] = abs(Uk) + sqrt(m0 * m0 + m1 * m1 + m2 * m2) * z.acoustic_speed[id];
+#pragma unroll
+    for (int l = 0; l < NS; ++l) s[T::spt(V::Y0 + l, c, t)] = z.cv[id + (5 + l) * sz];
+  }
+  __syncthreads();
+
+  // ---- face fluxes ------------------------------------------------------
+  for (int item = threadIdx.x; item < NF * C; item += T::NT) {
+    int c, t;
+    split(item, NF, c, t);
+    const int f = n0 - 1 + t;
+    if (cbase + c >= ncol_max || f > m - 1) continue;
+    const double *s = spts;
+    const int pc = t + R;
+    // face normal averaged with the (i+1) node, as the reference does
+    const int64_t idf = node_idx(g, c, f);
+    double kx = 0.5 * (z.metric[idf + mmo * sz] + z.metric[idf + 1 + mmo * sz]);
+    double ky = 0.5 * (z.metric[idf + (mmo + 1) * sz] + z.metric[idf + 1 + (mmo + 1) * sz]);
+    double kz = 0.5 * (z.metric[idf + (mmo + 2) * sz] + z.metric[idf + 1 + (mmo + 2) * sz]);
+
+    const double rho_l = s[T::spt(0, c, pc)], rho_r = s[T::spt(0, c, pc + 1)];
+    double temp1 = sqrt(rho_l * rho_r);
+    const double rlc = 1 / (rho_l + temp1);
+    const double rrc = 1 / (temp1 + rho_r);
+    const double um = rlc * s[T::spt(1, c, pc)] + rrc * s[T::spt(1, c, pc + 1)];
+    const double vm = rlc * s[T::spt(2, c, pc)] + rrc * s[T::spt(2, c, pc + 1)];
+    const double wm = rlc * s[T::spt(3, c, pc)] + rrc * s[T::spt(3, c, pc + 1)];
+    double svm[NS];
+#pragma unroll
+    for (int l = 0; l < NS; ++l)
+      svm[l] = rlc * s[T::spt(V::Y0 + l, c, pc)] + rrc * s[T::spt(V::Y0 + l, c, pc + 1)];
+    temp1 = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) temp1 += svm[l] * th->gas_const[l];
+    double temp3 = (rlc * s[T::spt(V::P, c, pc)] + rrc * s[T::spt(V::P, c, pc + 1)]) / temp1;
+    double hb[NS], cpb[NS];
+    enthalpy_cp_ns<NS>(th, temp3, hb, cpb);  // compute_enthalpy_and_cp at the averaged T
+    double temp2 = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) temp2 += svm[l] * cpb[l];
+    const double gamma = temp2 / (temp2 - temp1);
+    const double cm = sqrt(gamma * temp1 * temp3);
+    const double gm1 = gamma - 1;
+    temp1 = 1.0 / sqrt(kx * kx + ky * ky + kz * kz);
+    kx *= temp1; ky *= temp1; kz *= temp1;
+    const double Uk_bar = kx * um + ky * vm + kz * wm;
+    double nx = 0, ny = 0, nz = 0;
+    if (abs(kx) > 0.8) { nx = -kz; nz = kx; }
+    else { ny = kz; nz = -ky; }
+    temp1 = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+    nx *= temp1; ny *= temp1; nz *= temp1;
+    double qx = ky * nz - kz * ny, qy = kz * nx - kx * nz, qz = kx * ny - ky * nx;
+    temp1 = 1.0 / sqrt(qx * qx + qy * qy + qz * qz);
+    qx *= temp1; qy *= temp1; qz *= temp1;
+    const double Un = nx * um + ny * vm + nz * wm;
+    const double Uq = qx * um + qy * vm + qz * wm;
+    temp2 = 1.0 / (cm * cm);
+    double beta[NS];
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      beta[l] = gamma * th->gas_const[l] * temp3 - gm1 * hb[l];
+      beta[l] *= temp2;
+    }
+    const double alpha = 0.5 * gm1 * (um * um + vm * vm + wm * wm);
+    double lam = 0;
+#pragma unroll
+    for (int q = 0; q < NPF; ++q) lam = max(lam, s[T::spt(V::LAM, c, t + q)]);
+    double sbq[NPF], sbf[NPF];
+#pragma unroll
+    for (int q = 0; q < NPF; ++q) {
+      const int tq = t + q;
+      const double uq = s[T::spt(V::U, c, tq)];
+      double sp = 0, sn = 0;
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        const double ry = s[T::spt(V::Y0 + n, c, tq)];
+        sp = fma(beta[n], ry, sp);
+        sn = fma(beta[n], ry * uq, sn);
+      }
+      sbq[q] = sp;
+      sbf[q] = sn;
+    }
+
+    double fChar[5 + NS];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      asm volatile("" ::: "memory");
+      double L0, L1, L2, L3, L4, tb = 0.5;
+      if (l == 0) {
+        L0 = (alpha + Uk_bar * cm) * temp2 * 0.5;
+        L1 = -(gm1 * um + kx * cm) * temp2 * 0.5;
+        L2 = -(gm1 * vm + ky * cm) * temp2 * 0.5;
+        L3 = -(gm1 * wm + kz * cm) * temp2 * 0.5;
+        L4 = gm1 * temp2 * 0.5;
+      } else if (l == 1) {
+        tb = 0; L0 = -Un; L1 = nx; L2 = ny; L3 = nz; L4 = 0;
+      } else if (l == 2) {
+        tb = 0; L0 = -Uq; L1 = qx; L2 = qy; L3 = qz; L4 = 0;
+      } else if (l == 3) {
+        tb = -1;
+        L0 = 1 - alpha * temp2;
+        L1 = gm1 * um * temp2;
+        L2 = gm1 * vm * temp2;
+        L3 = gm1 * wm * temp2;
+        L4 = -gm1 * temp2;
+      } else {
+        L0 = (alpha - Uk_bar * cm) * temp2 * 0.5;
+        L1 = -(gm1 * um - kx * cm) * temp2 * 0.5;
+        L2 = -(gm1 * vm - ky * cm) * temp2 * 0.5;
+        L3 = -(gm1 * wm - kz * cm) * temp2 * 0.5;
+        L4 = gm1 * temp2 * 0.5;
+      }
+      double vp[NPF - 1], vmn[NPF - 1];
+#pragma unroll
+      for (int q = 0; q < NPF; ++q) {
+        const int tq = t + q;
+        const double LF = L0 * s[T::spt(5, c, tq)] + L1 * s[T::spt(6, c, tq)] + L2 * s[T::spt(7, c, tq)] +
+                          L3 * s[T::spt(8, c, tq)] + L4 * s[T::spt(9, c, tq)] + tb * sbf[q];
+        const double LQ = L0 * s[T::spt(0, c, tq)] + L1 * s[T::spt(1, c, tq)] + L2 * s[T::spt(2, c, tq)] +
+                          L3 * s[T::spt(3, c, tq)] + L4 * s[T::spt(4, c, tq)] + tb * sbq[q];
+        const double jq = s[T::spt(V::J, c, tq)];
+        if (q < NPF - 1) vp[q] = 0.5 * jq * (LF + lam * LQ);
+        if (q > 0) vmn[q - 1] = 0.5 * jq * (LF - lam * LQ);
+      }
+      if constexpr (ORD == 7) fChar[l] = weno7_z(vp, vmn, eps_ref);
+      else fChar[l] = weno5_js(vp, vmn, eps_ref);
+    }
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      asm volatile("" ::: "memory");
+      double vp[NPF - 1], vmn[NPF - 1];
+#pragma unroll
+      for (int q = 0; q < NPF; ++q) {
+        const int tq = t + q;
+        const double LQ = s[T::spt(V::Y0 + l, c, tq)] - svm[l] * s[T::spt(0, c, tq)];
+        const double LF = s[T::spt(V::U, c, tq)] * LQ;
+        const double jq = s[T::spt(V::J, c, tq)];
+        if (q < NPF - 1) vp[q] = 0.5 * jq * (LF + lam * LQ);
+        if (q > 0) vmn[q - 1] = 0.5 * jq * (LF - lam * LQ);
+      }
+      if constexpr (ORD == 7) fChar[5 + l] = weno7_z(vp, vmn, eps_ref);
+      else fChar[5 + l] = weno5_js(vp, vmn, eps_ref);
+    }
+    const double f034 = fChar[0] + fChar[3] + fChar[4];
+    const double f04 = fChar[0] - fChar[4];
+    const double H = rlc * (s[T::spt(4, c, pc)] + s[T::spt(V::P, c, pc)]) +
+                     rrc * (s[T::spt(4, c, pc + 1)] + s[T::spt(V::P, c, pc + 1)]);
+    sflx[T::sfl(0, c, t)] = f034;
+    sflx[T::sfl(1, c, t)] = um * f034 - kx * cm * f04 + nx * fChar[1] + qx * fChar[2];
+    sflx[T::sfl(2, c, t)] = vm * f034 - ky * cm * f04 + ny * fChar[1] + qy * fChar[2];
+    sflx[T::sfl(3, c, t)] = wm * f034 - kz * cm * f04 + nz * fChar[1] + qz * fChar[2];
+    double f4 = H * f034 - Uk_bar * cm * f04 + Un * fChar[1] + Uq * fChar[2] - cm * cm / gm1 * fChar[3];
+    double bsum = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      sflx[T::sfl(5 + l, c, t)] = svm[l] * f034 + fChar[5 + l];
+      bsum += beta[l] * fChar[5 + l];
+    }
+    f4 -= bsum * cm * cm / gm1;
+    sflx[T::sfl(4, c, t)] = f4;
+  }
+  __syncthreads();
+
+  // ---- flux difference into dq -----------------------------------------
+  for (int item = threadIdx.x; item < TN * C; item += T::NT) {
+    int c, t;
+    split(item, TN, c, t);
+    const int a = n0 + t;
+    if (cbase + c >= ncol_max || a > m - 1) continue;
+    const int64_t iq = node_idx(0, c, a);
+#pragma unroll
+    for (int v = 0; v < T::NV; ++v) z.dq[iq + v * szq] -= sflx[T::sfl(v, c, t + 1)] - sflx[T::sfl(v, c, t)];
+  }
+}
+
+namespace {
+
+template <int DIR, int ORD>
+cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, cudaStream_t st) {
+  using T = MixTile<DIR, ORD, kMaxSpec>;
+  const Dims &d = z.d;
+  dim3 grid;
+  if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
+  else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
+  else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
+  weno_mix_flux_diff<DIR, ORD, kMaxSpec><<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th);
+  return cudaGetLastError();
+}
+
+template <int DIR, int ORD>
+cudaError_t set_mix_attr() {
+  return cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)MixTile<DIR, ORD, kMaxSpec>::smem_bytes());
+}
+
+}  // namespace
+
+cudaError_t weno_mix_init_attributes() {
+  cudaError_t e;
+  if ((e = set_mix_attr<0, 5>()) != cudaSuccess) return e;
+  if ((e = set_mix_attr<1, 5>()) != cudaSuccess) return e;
+  if ((e = set_mix_attr<2, 5>()) != cudaSuccess) return e;
+  if ((e = set_mix_attr<0, 7>()) != cudaSuccess) return e;
+  if ((e = set_mix_attr<1, 7>()) != cudaSuccess) return e;
+  return set_mix_attr<2, 7>();
+}
+
+// x, y and (3-D) z sweeps; the species count is fixed at 9 (kMaxSpec).
+cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch) {
+  const double eps_ref = kEpsWeno * p.weno_eps_scale;
+  const bool w7 = p.inviscid_scheme == 72;
+  cudaError_t e = w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, st) : launch_mix_dir<0, 5>(z, eps_ref, th, st);
+  if (e != cudaSuccess) return e;
+  e = w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, st) : launch_mix_dir<1, 5>(z, eps_ref, th, st);
+  if (e != cudaSuccess) return e;
+  *n_launch += 2;
+  if (z.d.mz > 1) {
+    e = w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, st) : launch_mix_dir<2, 5>(z, eps_ref, th, st);
+    if (e != cudaSuccess) return e;
+    *n_launch += 1;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace cfk

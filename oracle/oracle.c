@@ -880,6 +880,8 @@ double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed) {
   for (int rk = 0; rk < 3; ++rk) {
     memset(z->dq, 0, sizeof(double) * szq * p->n_var);
     orc_compute_viscous_flux(z, p);
+    /* explicit chemical source of a reacting mixture (src/RK.cuh:147-149) */
+    if (p->mech && p->n_reac > 0) orc_finite_rate_chemistry(z, p);
     orc_compute_inviscid_flux(z, p);
     orc_update_cv_and_bv_rk(z, p, dt, rk);
     orc_apply_boundary_conditions(z, p);
