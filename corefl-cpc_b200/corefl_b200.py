@@ -147,6 +147,7 @@ def lib() -> ctypes.CDLL:
             "cfk_local_time_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step_graph": (i, [vp, _DP, vp]),
+            "cfk_wu_splitting_step": (i, [vp, i, _DP, vp]),
             "cfk_memcpy_h2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
             "cfk_memcpy_d2h": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
             "cfk_memcpy_d2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
@@ -330,6 +331,11 @@ class Context:
         dt = ctypes.c_double(0.0)
         fn = self.L.cfk_rk3_step_graph if graph else self.L.cfk_rk3_step
         self._ck(fn(self.h, ctypes.byref(dt) if want_dt else None, stream), "rk3_step")
+        return dt.value
+
+    def wu_splitting_step(self, schedule=1, stream=None) -> float:
+        dt = ctypes.c_double(0.0)
+        self._ck(self.L.cfk_wu_splitting_step(self.h, schedule, ctypes.byref(dt), stream), "wu_splitting_step")
         return dt.value
 
     def sync(self, stream=None):

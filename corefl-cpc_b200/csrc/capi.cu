@@ -19,11 +19,11 @@ cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, 
 cudaError_t viscous_mix_init_attributes();
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
-                             int rk, int *err, cudaStream_t st);
+                             int rk, int *err, cudaStream_t st, bool minus_cn = false);
 cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
 cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
-                            cudaStream_t st);
+                            cudaStream_t st, bool with_reaction = true);
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
                                        int n_face, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
@@ -469,6 +469,56 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
   }
   c->launches += n;
+  return CFK_OK;
+}
+
+// One step of Wu's splitting (the loop body of wu_splitting, reference
+// src/StrangSplitting.cu:683-861).  With the CFL step the dt is read back to
+// the host once (the reaction kernels take it by value).
+int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *stream) {
+  NEED_ZONE(c);
+  if (c->hp.inviscid_scheme == 0) return fail(c, CFK_ERR_STATE, "inviscid_scheme 0 contexts have no transport step");
+  if (!c->have_mech || c->hp.n_reac == 0) return fail(c, CFK_ERR_STATE, "no reacting mechanism loaded");
+  if (!c->z.Cn) return fail(c, CFK_ERR_ARG, "Cn is required for Wu's splitting");
+  if (schedule != 0 && schedule != 1) return fail(c, CFK_ERR_ARG, "schedule must be 0 or 1");
+  const Zone &z = c->z;
+  const Param &p = c->p;
+  const Thermo *th = thermo_of(c);
+  cudaStream_t st = S(stream);
+  const size_t P = (size_t)z.d.plane(z.d.ngg), N = (size_t)z.d.plane(0);
+  int n = 0;
+  double dt = c->hp.dt;
+  if (!p.fixed_dt) {
+    CFK_CHECK(c, launch_local_dt(z, p, th, c->d_dt_bits, st, false), "local_time_step_without_reaction");
+    n += 2;
+    CFK_CHECK(c, cudaMemcpyAsync(&dt, c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, st), "dt copy");
+    CFK_CHECK(c, cudaStreamSynchronize(st), "dt sync");
+  }
+  // compute_cn (:15-41): Cn = transport right-hand side
+  CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
+  if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
+  CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");
+  CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "Cn copy");
+  // wu_reaction_subStep (:475-502)
+  unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
+  CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
+            "wu_reaction_step");
+  ++n;
+  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, st, &n), "boundary conditions");
+  CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
+  ++n;
+  // wu_RK_subStep (:564-634): SSP-RK3 over dt/2 on dq - Cn, no property update
+  CFK_CHECK(c, cudaMemcpyAsync(z.qn, z.cv, P * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "qn copy");
+  for (int rk = 0; rk < 3; ++rk) {
+    CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
+    if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
+    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");
+    CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
+    ++n;
+    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, st, &n), "boundary conditions");
+  }
+  c->launches += n;
+  if (dt_used) *dt_used = dt;
   return CFK_OK;
 }
 

@@ -15,9 +15,12 @@ __constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
 // update_cv_and_bv_rk (reference src/RK.cuh:224-281).  dt comes from the
 // device scalar when dt_dev is non-null (CFL step computed on the device).
 // ---------------------------------------------------------------------------
+// With minus_cn the right-hand side is dq - Cn: update_cv_and_bv_rk_wu
+// (reference src/StrangSplitting.cu:504-562).
 template <bool MIX>
 __global__ void __launch_bounds__(256) update_cv_and_bv_rk_kernel(Zone z, Param p, const Thermo *th, double dt_host,
-                                                                  const double *dt_dev, int rk, int *err) {
+                                                                  const double *dt_dev, int rk, int *err,
+                                                                  bool minus_cn) {
   const Dims d = z.d;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
@@ -30,11 +33,11 @@ __global__ void __launch_bounds__(256) update_cv_and_bv_rk_kernel(Zone z, Param 
   const double dt_div_jac = dt / z.jac[id];
   double cvl[kMaxVar];
   const int nv = p.n_var;
+  auto rhs = [&](int l) { return minus_cn ? z.dq[iq + l * szq] - z.Cn[iq + l * szq] : z.dq[iq + l * szq]; };
 #pragma unroll
-  for (int l = 0; l < 5; ++l) cvl[l] = a * z.qn[id + l * sz] + b * z.cv[id + l * sz] + c * dt_div_jac * z.dq[iq + l * szq];
+  for (int l = 0; l < 5; ++l) cvl[l] = a * z.qn[id + l * sz] + b * z.cv[id + l * sz] + c * dt_div_jac * rhs(l);
   if (MIX) {
-    for (int l = 5; l < nv; ++l)
-      cvl[l] = a * z.qn[id + l * sz] + b * z.cv[id + l * sz] + c * dt_div_jac * z.dq[iq + l * szq];
+    for (int l = 5; l < nv; ++l) cvl[l] = a * z.qn[id + l * sz] + b * z.cv[id + l * sz] + c * dt_div_jac * rhs(l);
   }
   if (d.mz == 1) cvl[3] = 0;
   const double rho = cvl[0];
@@ -142,9 +145,11 @@ __global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo 
 // a warp/CTA min reduction and one atomicMin on the bit pattern (dt > 0, so
 // the unsigned order of the bits is the order of the values).
 // ---------------------------------------------------------------------------
+// with_reaction = false: local_time_step_without_reaction (reference
+// src/TimeAdvanceFunc.cu:21-100), the step of Wu's splitting.
 template <bool MIX>
 __global__ void __launch_bounds__(256) local_time_step_kernel(Zone z, Param p, const Thermo *th,
-                                                              unsigned long long *dt_min_bits) {
+                                                              unsigned long long *dt_min_bits, bool with_reaction) {
   const Dims d = z.d;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(256) local_time_step_kernel(Zone z, Param p, c
       msr = max(msr, max_length * max_length * mdv);
     }
     dt = p.cfl / msr;
-    if (MIX && p.n_reac > 0) {
+    if (MIX && with_reaction && p.n_reac > 0) {
       const double reaction_dt = p.cfl * z.reaction_timeScale[id];
       if (reaction_dt > 1e-20 && reaction_dt < 1e-5) dt = min(dt, reaction_dt);
     }
@@ -330,9 +335,11 @@ static dim3 padded_grid(const Dims &d, int tpb) {
 }
 
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
-                             int rk, int *err, cudaStream_t st) {
-  if (p.n_spec > 0) update_cv_and_bv_rk_kernel<true><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err);
-  else update_cv_and_bv_rk_kernel<false><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err);
+                             int rk, int *err, cudaStream_t st, bool minus_cn) {
+  if (p.n_spec > 0)
+    update_cv_and_bv_rk_kernel<true><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
+  else
+    update_cv_and_bv_rk_kernel<false><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
   return cudaGetLastError();
 }
 
@@ -349,10 +356,12 @@ cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo
 }
 
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
-                            cudaStream_t st) {
+                            cudaStream_t st, bool with_reaction) {
   reset_dt_kernel<<<1, 1, 0, st>>>(dt_bits);
-  if (p.n_spec > 0) local_time_step_kernel<true><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits);
-  else local_time_step_kernel<false><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits);
+  if (p.n_spec > 0)
+    local_time_step_kernel<true><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits, with_reaction);
+  else
+    local_time_step_kernel<false><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits, with_reaction);
   return cudaGetLastError();
 }
 

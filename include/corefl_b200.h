@@ -175,6 +175,15 @@ int cfk_rk3_step(cfk_ctx *ctx, double *dt_used, void *stream);
 /* Same step replayed from a CUDA graph captured on first use (the graph is
  * rebuilt if the zone is re-bound). */
 int cfk_rk3_step_graph(cfk_ctx *ctx, double *dt_used, void *stream);
+/* One step of Wu's splitting for a reacting mixture (the loop body of
+ * wu_splitting, reference src/StrangSplitting.cu:683-861): dt fixed or from
+ * local_time_step_without_reaction; Cn = viscous + inviscid right-hand side
+ * (compute_cn, :15-41); the reaction step over dt with the frozen Cn
+ * (schedule 0 one thread per node, 1 work queue), BCs, property update
+ * (wu_reaction_subStep, :475-502); SSP-RK3 over dt/2 on dq - Cn with BCs and
+ * no property update (wu_RK_subStep, :564-634).  *dt_used (may be NULL)
+ * receives the dt; the CFL dt costs one host synchronisation. */
+int cfk_wu_splitting_step(cfk_ctx *ctx, int schedule, double *dt_used, void *stream);
 
 /* ---- host <-> device helpers for callers without a CUDA runtime -------- */
 int cfk_memcpy_h2d(cfk_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes, void *stream);

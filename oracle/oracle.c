@@ -548,7 +548,17 @@ static const double RK_C[3] = {1.0, 0.25, 2.0 / 3.0};
 
 void orc_temperature_and_pressure(orc_zone *z, const orc_param *p, long id, double total_energy);
 
-void orc_update_cv_and_bv_rk(orc_zone *z, const orc_param *p, double dt, int rk) {
+static void update_cv_and_bv(orc_zone *z, const orc_param *p, double dt, int rk, int minus_cn);
+
+void orc_update_cv_and_bv_rk(orc_zone *z, const orc_param *p, double dt, int rk) { update_cv_and_bv(z, p, dt, rk, 0); }
+
+/* update_cv_and_bv_rk_wu (src/StrangSplitting.cu:504-562): the same update
+ * with dq - Cn, the transport part frozen at the start of the step. */
+void orc_update_cv_and_bv_rk_wu(orc_zone *z, const orc_param *p, double dt, int rk) {
+  update_cv_and_bv(z, p, dt, rk, 1);
+}
+
+static void update_cv_and_bv(orc_zone *z, const orc_param *p, double dt, int rk, int minus_cn) {
   const int ngg = z->ngg, nv = p->n_var, mx = z->mx, my = z->my, mz = z->mz;
   const long sz = psz(z, ngg), szq = psz(z, 0);
   const int ns = p->n_spec;
@@ -559,9 +569,10 @@ void orc_update_cv_and_bv_rk(orc_zone *z, const orc_param *p, double dt, int rk)
         const long id = pidx(z, ngg, i, j, k), iq = pidx(z, 0, i, j, k);
         double *cv = z->cv, *bv = z->bv, *sv = z->sv;
         const double dt_div_jac = dt / z->jac[id];
-        for (int l = 0; l < nv; ++l)
-          cv[id + l * sz] = RK_A[rk] * z->qn[id + l * sz] + RK_B[rk] * cv[id + l * sz] +
-                            RK_C[rk] * dt_div_jac * z->dq[iq + l * szq];
+        for (int l = 0; l < nv; ++l) {
+          const double r = minus_cn ? z->dq[iq + l * szq] - z->Cn[iq + l * szq] : z->dq[iq + l * szq];
+          cv[id + l * sz] = RK_A[rk] * z->qn[id + l * sz] + RK_B[rk] * cv[id + l * sz] + RK_C[rk] * dt_div_jac * r;
+        }
         if (mz == 1) cv[id + 3 * sz] = 0;
         bv[id] = cv[id];
         const double density_inv = 1.0 / cv[id];
@@ -657,7 +668,14 @@ void orc_update_physical_properties(orc_zone *z, const orc_param *p) {
 /* ------------------------------------------------------------------------ */
 double orc_mixture_max_diffuse_vel(const orc_zone *z, const orc_param *p, long id);
 
-void orc_local_time_step(orc_zone *z, const orc_param *p) {
+static void local_time_step(orc_zone *z, const orc_param *p, int with_reaction);
+
+void orc_local_time_step(orc_zone *z, const orc_param *p) { local_time_step(z, p, 1); }
+
+/* local_time_step_without_reaction (src/TimeAdvanceFunc.cu:21-100) */
+void orc_local_time_step_without_reaction(orc_zone *z, const orc_param *p) { local_time_step(z, p, 0); }
+
+static void local_time_step(orc_zone *z, const orc_param *p, int with_reaction) {
   const int g = z->ngg, mx = z->mx, my = z->my, mz = z->mz;
   const long sz = psz(z, g);
   const int dim = mz == 1 ? 2 : 3;
@@ -702,7 +720,7 @@ void orc_local_time_step(orc_zone *z, const orc_param *p) {
           max_sr = max_sr > vr ? max_sr : vr;
         }
         double dt = p->cfl / max_sr;
-        if (p->mech && p->n_reac > 0) {
+        if (with_reaction && p->mech && p->n_reac > 0) {
           const double reaction_dt = p->cfl * z->reaction_timeScale[id];
           if (reaction_dt > 1e-20 && reaction_dt < 1e-5) dt = dt < reaction_dt ? dt : reaction_dt;
         }
@@ -869,6 +887,39 @@ void orc_eliminate_k_gradient(orc_zone *z, const orc_param *p) {
 /* ------------------------------------------------------------------------ */
 /* One SSP-RK3 step: src/RK.cuh:84-212 (single block, no MPI).               */
 /* ------------------------------------------------------------------------ */
+/* One step of Wu's splitting, the loop body of wu_splitting
+ * (src/StrangSplitting.cu:683-861): dt without the reaction limit;
+ * compute_cn (:15-41): Cn = viscous + inviscid right-hand side;
+ * wu_reaction_subStep (:475-502): the reaction step over dt with the frozen
+ * Cn, BCs, 2-D k-ghost copy, properties; wu_RK_subStep (:564-634): SSP-RK3
+ * over dt/2 on dq - Cn with BCs (no property update inside). */
+double orc_wu_splitting_step(orc_zone *z, const orc_param *p, double dt_fixed) {
+  const long sz = psz(z, z->ngg), szq = psz(z, 0);
+  double dt = dt_fixed;
+  if (!p->fixed_dt) {
+    orc_local_time_step_without_reaction(z, p);
+    dt = orc_global_time_step(z);
+  }
+  memset(z->dq, 0, sizeof(double) * szq * p->n_var);
+  orc_compute_viscous_flux(z, p);
+  orc_compute_inviscid_flux(z, p);
+  memcpy(z->Cn, z->dq, sizeof(double) * szq * p->n_var);
+  orc_wu_reaction_step(z, p, dt, NULL);
+  orc_apply_boundary_conditions(z, p);
+  if (z->mz == 1) orc_eliminate_k_gradient(z, p);
+  orc_update_physical_properties(z, p);
+  memcpy(z->qn, z->cv, sizeof(double) * sz * p->n_var);
+  for (int rk = 0; rk < 3; ++rk) {
+    memset(z->dq, 0, sizeof(double) * szq * p->n_var);
+    orc_compute_viscous_flux(z, p);
+    orc_compute_inviscid_flux(z, p);
+    orc_update_cv_and_bv_rk_wu(z, p, 0.5 * dt, rk);
+    orc_apply_boundary_conditions(z, p);
+    if (z->mz == 1) orc_eliminate_k_gradient(z, p);
+  }
+  return dt;
+}
+
 double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed) {
   const long sz = psz(z, z->ngg), szq = psz(z, 0);
   memcpy(z->qn, z->cv, sizeof(double) * sz * p->n_var);

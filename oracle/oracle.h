@@ -101,6 +101,11 @@ void orc_apply_boundary_conditions(orc_zone *z, const orc_param *p);
 void orc_eliminate_k_gradient(orc_zone *z, const orc_param *p);
 /* One SSP-RK3 step (reference src/RK.cuh:84-212); returns the dt used. */
 double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed);
+/* Stage update with dq - Cn (reference src/StrangSplitting.cu:504-562). */
+void orc_update_cv_and_bv_rk_wu(orc_zone *z, const orc_param *p, double dt, int rk);
+void orc_local_time_step_without_reaction(orc_zone *z, const orc_param *p);
+/* One step of Wu's splitting (reference src/StrangSplitting.cu:683-861); returns the dt used. */
+double orc_wu_splitting_step(orc_zone *z, const orc_param *p, double dt_fixed);
 
 /* scalar WENO reconstructions (reference src/WENO.cu:3059-3222) */
 double orc_weno5(const double *vp, const double *vm, double eps, int if_shock);

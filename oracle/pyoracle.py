@@ -128,6 +128,12 @@ def lib() -> ctypes.CDLL:
         L.orc_update_cv_and_bv_rk.restype = None
         L.orc_rk3_step.argtypes = [zp, pp, ctypes.c_double]
         L.orc_rk3_step.restype = ctypes.c_double
+        L.orc_wu_splitting_step.argtypes = [zp, pp, ctypes.c_double]
+        L.orc_wu_splitting_step.restype = ctypes.c_double
+        L.orc_update_cv_and_bv_rk_wu.argtypes = [zp, pp, ctypes.c_double, ctypes.c_int]
+        L.orc_update_cv_and_bv_rk_wu.restype = None
+        L.orc_local_time_step_without_reaction.argtypes = [zp, pp]
+        L.orc_local_time_step_without_reaction.restype = None
         L.orc_global_time_step.argtypes = [zp]
         L.orc_global_time_step.restype = ctypes.c_double
         L.orc_weno5.argtypes = [_DP, _DP, ctypes.c_double, ctypes.c_int]
@@ -203,6 +209,9 @@ class OracleZone:
 
     def step(self) -> float:
         return self.L.orc_rk3_step(ctypes.byref(self.z), ctypes.byref(self.p), self.p.dt)
+
+    def wu_splitting_step(self) -> float:
+        return self.L.orc_wu_splitting_step(ctypes.byref(self.z), ctypes.byref(self.p), self.p.dt)
 
     def reaction_step(self, dt: float, want_nsub: bool = False):
         """Wu-splitting reaction step over the zone (point implicit when

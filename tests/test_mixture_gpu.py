@@ -93,3 +93,38 @@ def test_mixture_flux_single_calls(scheme):
     gz.ctx.viscous()
     oz.call("orc_compute_viscous_flux")
     assert rel_err(gz.get("dq")[1:], oz["dq"][1:], momentum=(0, 1, 2)) <= 1e-11
+
+
+def _lockstep_wu(case, n_steps, tol=1e-12):
+    oz = pyoracle.OracleZone(case)
+    oz.initialize()
+    gz = GpuZone(case)
+    gz.initialize()
+    for s in range(n_steps):
+        gz.load_from(oz, keys=MIX_KEYS)
+        dt_o = oz.wu_splitting_step()
+        dt_g = gz.ctx.wu_splitting_step(schedule=1)
+        assert dt_g == pytest.approx(dt_o, rel=1e-12), f"dt differs at step {s}"
+        e = rel_err(interior_planes(case, gz.get("cv")), interior_planes(case, oz["cv"]))
+        assert e <= tol, f"step {s}: conserved-variable relative difference {e:.3e}"
+        assert rel_err(gz.get("Cn"), oz["Cn"]) <= 1e-11
+    assert rel_err(gz.get("sv"), oz["sv"], momentum=()) <= tol
+
+
+def test_wu_splitting_reacting_3d_viscous_cfl_step():
+    """Wu's splitting on the reacting 3-D block (1100 K, Li-2004): CFL step
+    without the reaction limit, Cn from the viscous + WENO5 right-hand side,
+    point-implicit reaction step with the frozen Cn, half-step RK3 on dq - Cn."""
+    case = cases.mix_wave(mechanism.load("li2004"), 11, ny=13, nz=9, scheme=52, reacting=True, T0=1100.0)
+    _lockstep_wu(case, 3)
+
+
+def test_wu_splitting_reacting_tube_fixed_step():
+    """Reacting H2/O2/Ar tube (WENO7, 2-D), fixed step of 1e-8 s."""
+    mech = mechanism.load("premix_h2_ar")
+    left = dict(rho=0.18075, p=35594.0 * 4, Y={"H2": 0.012772428, "O2": 0.101362139, "AR": 0.885865433})
+    right = dict(rho=0.072, p=7173.0 * 4, Y={"H2": 0.012772428, "O2": 0.101362139, "AR": 0.885865433})
+    case = cases.mix_tube(mech, 96, 7, scheme=72, reacting=True, left=left, right=right)
+    case.param["fixed_dt"] = 1
+    case.param["dt"] = 1e-8
+    _lockstep_wu(case, 3)
