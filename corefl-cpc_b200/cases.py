@@ -124,7 +124,7 @@ def _air_param(**kw) -> dict:
     p = dict(dim=3, n_var=5, n_spec=0, n_scalar=0, n_reac=0, inviscid_scheme=72, reconstruction=2, limiter=0,
              viscous_order=0, positive_preserving=0, gradPInDiffusionFlux=0, fixed_dt=0, chem_advance_method=0,
              entropy_fix_factor=0.125, Pr=0.72, Sc=0.5, cfl=0.5, dt=0.0, weno_eps_scale=1.0, v_ref=1.0, rho_ref=1.0,
-             sensor_threshold=0.0)
+             sensor_threshold=0.0, shock_sensor=0, sensor_eps=-1.0)
     p.update(kw)
     return p
 

@@ -27,7 +27,7 @@ class cfk_param(ctypes.Structure):
         ("entropy_fix_factor", ctypes.c_double), ("Pr", ctypes.c_double), ("Sc", ctypes.c_double),
         ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("weno_eps_scale", ctypes.c_double),
         ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double), ("sensor_threshold", ctypes.c_double),
-        ("device", ctypes.c_int),
+        ("device", ctypes.c_int), ("shock_sensor", ctypes.c_int), ("sensor_eps", ctypes.c_double),
     ]
 
 
@@ -97,7 +97,7 @@ class cfk_zone(ctypes.Structure):
     _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
         (n, ctypes.c_void_p) for n in ("jac", "metric", "cv", "bv", "sv", "qn", "mul", "mach", "acoustic_speed",
                                        "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
-                                       "dt_local", "Cn")
+                                       "dt_local", "Cn", "shock_sensor")
     ]
 
 
@@ -140,6 +140,7 @@ def lib() -> ctypes.CDLL:
             "cfk_alloc_zone": (i, [vp, i, i, i, ctypes.POINTER(cfk_zone)]),
             "cfk_compute_viscous_flux": (i, [vp, vp]),
             "cfk_compute_inviscid_flux": (i, [vp, vp]),
+            "cfk_compute_shock_sensor": (i, [vp, vp]),
             "cfk_update_cv_and_bv_rk": (i, [vp, d, i, vp]),
             "cfk_update_physical_properties": (i, [vp, vp]),
             "cfk_compute_cv_from_bv": (i, [vp, vp]),
@@ -309,6 +310,9 @@ class Context:
 
     def inviscid(self, stream=None):
         self._ck(self.L.cfk_compute_inviscid_flux(self.h, stream), "inviscid")
+
+    def shock_sensor(self, stream=None):
+        self._ck(self.L.cfk_compute_shock_sensor(self.h, stream), "shock sensor")
 
     def update_rk(self, dt, rk, stream=None):
         self._ck(self.L.cfk_update_cv_and_bv_rk(self.h, dt, rk, stream), "update")

@@ -27,6 +27,7 @@ cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, uns
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
                                        int n_face, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
+cudaError_t launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t st);
 cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
                                int schedule, int *nsub_out, int *err, unsigned int *counter, int n_sm,
                                cudaStream_t st);
@@ -97,7 +98,14 @@ int validate(const cfk_param *p, std::string &why) {
   if (s >= 1 && s <= 4 && !(p->limiter == 0 || p->limiter == 1)) { why = "limiter must be 0 or 1"; return -1; }
   if (s == 2 && !(p->entropy_fix_factor >= 0)) { why = "entropy_fix_factor must be >= 0"; return -1; }
   if (p->viscous_order != 0 && p->viscous_order != 2) { why = "viscous_order must be 0 or 2"; return -1; }
-  if (p->sensor_threshold > 1e-10) { why = "hybrid shock-sensor schemes are not supported (shockSensor_threshold must be 0)"; return -1; }
+  if (p->sensor_threshold > 1e-10 && !(s == 52 || s == 72)) {
+    why = "shockSensor_threshold > 0 (hybrid scheme) needs inviscid_scheme 52 or 72";
+    return -1;
+  }
+  if (p->sensor_threshold > 1e-10 && !(p->shock_sensor >= 0 && p->shock_sensor <= 2)) {
+    why = "shock_sensor must be 0 (Ducros), 1 (Jameson) or 2 (density/pressure jump)";
+    return -1;
+  }
   if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
   if (p->n_spec > 0 && s != 0 && !(s == 52 || s == 72)) {
     why = "the mixture model is supported with WENO5/7 characteristic fluxes (52, 72) in this build";
@@ -178,6 +186,8 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   p.Sc = param->Sc; p.cfl = param->cfl; p.weno_eps_scale = param->weno_eps_scale; p.v_ref = param->v_ref;
   p.rho_ref = param->rho_ref;
   p.chem_advance_method = param->chem_advance_method;
+  p.shock_sensor = param->shock_sensor; p.sensor_eps = param->sensor_eps;
+  p.sensor_threshold = param->sensor_threshold;
   e = cudaMalloc(&c->d_dt_bits, 64);
   if (e != cudaSuccess) { delete c; return CFK_ERR_CUDA; }
   c->d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(c->d_dt_bits) + 8);
@@ -197,6 +207,7 @@ int cfk_destroy(cfk_ctx *c) {
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : c->pool) cudaEventDestroy(e);
   for (void *ptr : c->owned) cudaFree(ptr);
+  if (c->own_sensor) cudaFree(c->own_sensor);
   cudaFree(c->d_dt_bits);
   cudaFree(c->d_mech);
   delete c;
@@ -230,6 +241,21 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   z.mul = zn->mul; z.mach = zn->mach; z.acoustic_speed = zn->acoustic_speed; z.gamma = zn->gamma;
   z.thermal_conductivity = zn->thermal_conductivity; z.rho_D = zn->rho_D;
   z.reaction_timeScale = zn->reaction_timeScale; z.dq = zn->dq; z.dt_local = zn->dt_local; z.Cn = zn->Cn;
+  z.shock_sensor = zn->shock_sensor;
+  if (c->p.sensor_threshold > 1e-10 && !z.shock_sensor) {
+    // the hybrid scheme needs a sensor array whose ghost layers are zero
+    // (reference src/Field.cu:526, allocated with cudaMemset 0)
+    const size_t P = (size_t)z.d.plane(z.d.ngg);
+    if (c->own_sensor_n < P) {
+      if (c->own_sensor) cudaFree(c->own_sensor);
+      c->own_sensor = nullptr;
+      c->own_sensor_n = 0;
+      CFK_CHECK(c, cudaMalloc(&c->own_sensor, P * sizeof(double)), "shock sensor allocation");
+      c->own_sensor_n = P;
+    }
+    CFK_CHECK(c, cudaMemset(c->own_sensor, 0, P * sizeof(double)), "shock sensor reset");
+    z.shock_sensor = c->own_sensor;
+  }
   c->bound = true;
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
   return CFK_OK;
@@ -255,6 +281,7 @@ int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
   bool ok = al(&zn.jac, P) && al(&zn.metric, 9 * P) && al(&zn.cv, nv * P) && al(&zn.bv, 6 * P) &&
             al(&zn.sv, nsc * P) && al(&zn.qn, nv * P) && al(&zn.mul, P) && al(&zn.mach, P) &&
             al(&zn.dq, nv * N) && al(&zn.dt_local, N);
+  if (ok && c->hp.sensor_threshold > 1e-10) ok = al(&zn.shock_sensor, P);
   if (ok && ns > 0)
     ok = al(&zn.acoustic_speed, P) && al(&zn.gamma, P) && al(&zn.thermal_conductivity, P) && al(&zn.rho_D, ns * P) &&
          al(&zn.reaction_timeScale, P) && al(&zn.Cn, nv * N);
@@ -379,6 +406,14 @@ int cfk_compute_inviscid_flux(cfk_ctx *c, void *stream) {
   return CFK_OK;
 }
 
+int cfk_compute_shock_sensor(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  if (!(c->p.sensor_threshold > 1e-10)) return CFK_OK;
+  CFK_CHECK(c, launch_shock_sensor(c->z, c->p, S(stream)), "compute_shock_sensor");
+  c->launches += 1;
+  return CFK_OK;
+}
+
 int cfk_update_cv_and_bv_rk(cfk_ctx *c, double dt, int rk, void *stream) {
   NEED_ZONE(c);
   if (rk < 0 || rk > 2) return fail(c, CFK_ERR_ARG, "rk must be 0, 1 or 2");
@@ -431,6 +466,12 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
   const size_t P = (size_t)z.d.plane(z.d.ngg), N = (size_t)z.d.plane(0);
   int n = 0;
   CFK_CHECK(c, cudaMemcpyAsync(z.qn, z.cv, P * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "qn copy");
+  if (p.sensor_threshold > 1e-10) {
+    // once per step, before the stages (reference src/RK.cuh:112-117)
+    PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
+    CFK_CHECK(c, launch_shock_sensor(z, p, st), "compute_shock_sensor");
+    ++n;
+  }
   const double *dt_dev = nullptr;
   if (!p.fixed_dt) {
     PhaseScope ps(c, CFK_PH_DT, st, &n);
@@ -494,7 +535,11 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
     CFK_CHECK(c, cudaMemcpyAsync(&dt, c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, st), "dt copy");
     CFK_CHECK(c, cudaStreamSynchronize(st), "dt sync");
   }
-  // compute_cn (:15-41): Cn = transport right-hand side
+  // compute_cn (:15-41): shock sensor, then Cn = transport right-hand side
+  if (p.sensor_threshold > 1e-10) {
+    CFK_CHECK(c, launch_shock_sensor(z, p, st), "compute_shock_sensor");
+    ++n;
+  }
   CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
   if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
   CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");

@@ -42,6 +42,7 @@ struct Zone {
   double *jac, *metric, *cv, *bv, *sv, *qn, *mul, *mach;
   double *acoustic_speed, *gamma, *thermal_conductivity, *rho_D, *reaction_timeScale;
   double *dq, *dt_local, *Cn;
+  double *shock_sensor;  // ngg ghosts, zero outside the interior; hybrid WENO only
 };
 
 // Kernel-side scalar settings.
@@ -51,6 +52,8 @@ struct Param {
   int positive_preserving, gradPInDiffusionFlux, fixed_dt, chem_advance_method;
   double entropy_fix_factor, Pr, Sc, cfl;
   double weno_eps_scale, v_ref, rho_ref;
+  int shock_sensor;                 // 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump
+  double sensor_eps, sensor_threshold;
 };
 
 }  // namespace cfk

@@ -22,6 +22,8 @@ struct cfk_ctx {
   Zone z{};
   bool bound = false;
   std::vector<void *> owned;  // device arrays owned by the context
+  double *own_sensor = nullptr;  // context-allocated shock sensor (zone without one)
+  size_t own_sensor_n = 0;
   Mech *d_mech = nullptr;
   Mech h_mech{};  // host copy, passed by value to the kernels that read it from the constant bank
   bool have_mech = false;

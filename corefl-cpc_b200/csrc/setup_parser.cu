@@ -141,6 +141,8 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
   p.cfl = get(s.reals, "cfl", 0.8);
   p.dt = get(s.reals, "dt", 1e-8);
   p.sensor_threshold = get(s.reals, "shockSensor_threshold", 0.0);
+  p.shock_sensor = get(s.ints, "shock_sensor", 0);
+  p.sensor_eps = get(s.reals, "shockSensor_epsilon", -1.0);
   const int species = get(s.ints, "species", 0);
   if (species != 0) return report("species != 0 needs a mechanism; pass n_spec/n_scalar explicitly");
   p.n_spec = 0;

@@ -95,4 +95,42 @@ __device__ __forceinline__ double weno7_z(const double *vp, const double *vm, do
   return one12th * ((np * dm + nm * dp) / (dp * dm));
 }
 
+// Linear branches of WENO5 / WENO7 used by the hybrid scheme away from
+// shocks (reference src/WENO.cu:3100-3113 and 3204-3221): the substencil
+// values combined with the optimal weights, which collapse to the 5- and
+// 7-point upwind-biased stencils (UD5: (2, -13, 47, 27, -3) / 60;
+// UD7: (-3, 25, -101, 319, 214, -38, 4) / 420).  The minus side is the plus
+// side read right to left.
+__device__ __forceinline__ double ud5_side(double u0, double u1, double u2, double u3, double u4) {
+  constexpr double r60{1.0 / 60};
+  return r60 * (2 * u0 - 13 * u1 + 47 * u2 + 27 * u3 - 3 * u4);
+}
+
+__device__ __forceinline__ double weno5_linear(const double *vp, const double *vm) {
+  return ud5_side(vp[0], vp[1], vp[2], vp[3], vp[4]) + ud5_side(vm[4], vm[3], vm[2], vm[1], vm[0]);
+}
+
+__device__ __forceinline__ double ud7_side(double u0, double u1, double u2, double u3, double u4, double u5,
+                                           double u6) {
+  constexpr double r420{1.0 / 420};
+  return r420 * (-3 * u0 + 25 * u1 - 101 * u2 + 319 * u3 + 214 * u4 - 38 * u5 + 4 * u6);
+}
+
+__device__ __forceinline__ double weno7_linear(const double *vp, const double *vm) {
+  return ud7_side(vp[0], vp[1], vp[2], vp[3], vp[4], vp[5], vp[6]) +
+         ud7_side(vm[6], vm[5], vm[4], vm[3], vm[2], vm[1], vm[0]);
+}
+
+// Hybrid switch of the WENO sweeps (reference src/WENO.cu:839-849, 1580-1590
+// and the z sweep): the face between node idf and idf + sd takes the
+// nonlinear weights when the sensor of any node idf + ii*sd, ii in
+// [-g+1, g], exceeds the threshold.  sensor == nullptr: WENO everywhere.
+__device__ __forceinline__ bool face_shocked(const double *sensor, int64_t idf, int64_t sd, int g,
+                                             double threshold) {
+  if (sensor == nullptr) return true;
+  for (int ii = -g + 1; ii <= g; ++ii)
+    if (__ldg(sensor + idf + ii * sd) > threshold) return true;
+  return false;
+}
+
 }  // namespace cfk

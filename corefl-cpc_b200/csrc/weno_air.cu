@@ -11,8 +11,10 @@
 //             normal, p, J/2 and the spectral radius |U_k| + c|grad k|;
 //   faces   — each thread projects the 2R+2 stencil points of one face onto
 //             the Roe-averaged left eigenvectors, splits them with the local
-//             Lax-Friedrichs bound, reconstructs with WENO5-JS / WENO7-Z and
-//             projects back; the face fluxes stay in shared memory;
+//             Lax-Friedrichs bound, reconstructs with WENO5-JS / WENO7-Z (or,
+//             for the hybrid scheme, with the linear UD5 / UD7 weights where no
+//             stencil node is shocked) and projects back; the face fluxes stay
+//             in shared memory;
 //   diff    — dq(n) -= F(n+1/2) - F(n-1/2) for the tile's nodes.
 //
 // The face flux never goes to HBM and dq is read-modified-written once per
@@ -50,8 +52,10 @@ struct AirTile {
 
 }  // namespace
 
-template <int DIR, int ORD>
-__global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_ref) {
+// HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
+template <int DIR, int ORD, bool HYB>
+__global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_ref, const double *sensor,
+                                                              double threshold) {
   using T = AirTile<DIR, ORD>;
   constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
   extern __shared__ double sm[];
@@ -158,6 +162,7 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
     double lam = 0;
 #pragma unroll
     for (int q = 0; q < NPF; ++q) lam = max(lam, s[T::spt(12, c, t + q)]);
+    const bool shock = !HYB || face_shocked(sensor, idf, d.stride(g, DIR), g, threshold);
 
     double fChar[5];
 #pragma unroll
@@ -201,8 +206,8 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
         if (q < NPF - 1) vp[q] = hj * (LF + lam * LQ);
         if (q > 0) vmn[q - 1] = hj * (LF - lam * LQ);
       }
-      if constexpr (ORD == 7) fChar[l] = weno7_z(vp, vmn, eps_ref);
-      else fChar[l] = weno5_js(vp, vmn, eps_ref);
+      if constexpr (ORD == 7) fChar[l] = shock ? weno7_z(vp, vmn, eps_ref) : weno7_linear(vp, vmn);
+      else fChar[l] = shock ? weno5_js(vp, vmn, eps_ref) : weno5_linear(vp, vmn);
     }
     // project back (right eigenvectors written out, reference src/WENO.cu:229-243)
     const double f034 = fChar[0] + fChar[3] + fChar[4];
@@ -230,7 +235,8 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
 }
 
 template <int DIR, int ORD>
-static cudaError_t launch_dir(const Zone &z, double eps_ref, cudaStream_t st) {
+static cudaError_t launch_dir(const Zone &z, double eps_ref, const double *sensor, double threshold,
+                              cudaStream_t st) {
   using T = AirTile<DIR, ORD>;
   const Dims &d = z.d;
   dim3 grid;
@@ -238,14 +244,18 @@ static cudaError_t launch_dir(const Zone &z, double eps_ref, cudaStream_t st) {
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
   const size_t smem = T::smem_bytes();
-  weno_air_flux_diff<DIR, ORD><<<grid, T::NT, smem, st>>>(z, eps_ref);
+  if (sensor) weno_air_flux_diff<DIR, ORD, true><<<grid, T::NT, smem, st>>>(z, eps_ref, sensor, threshold);
+  else weno_air_flux_diff<DIR, ORD, false><<<grid, T::NT, smem, st>>>(z, eps_ref, nullptr, threshold);
   return cudaGetLastError();
 }
 
 template <int DIR, int ORD>
 static cudaError_t set_smem_attr() {
-  return cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)AirTile<DIR, ORD>::smem_bytes());
+  const int b = (int)AirTile<DIR, ORD>::smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 // Opt every instantiation in to its dynamic shared-memory size (> 48 KB for
@@ -264,15 +274,18 @@ cudaError_t weno_air_init_attributes() {
 // Host launcher: x, y and (3-D) z sweeps in the reference's order.
 cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch) {
   const double eps_ref = kEpsWeno * p.weno_eps_scale;
+  // hybrid UD5/UD7 + WENO when a sensor threshold is set (reference src/Parameter.cpp:236-252)
+  const double th = p.sensor_threshold;
+  const double *sn = th > 1e-10 ? z.shock_sensor : nullptr;
   cudaError_t e;
   const bool w7 = p.inviscid_scheme == 72;
-  e = w7 ? launch_dir<0, 7>(z, eps_ref, st) : launch_dir<0, 5>(z, eps_ref, st);
+  e = w7 ? launch_dir<0, 7>(z, eps_ref, sn, th, st) : launch_dir<0, 5>(z, eps_ref, sn, th, st);
   if (e != cudaSuccess) return e;
-  e = w7 ? launch_dir<1, 7>(z, eps_ref, st) : launch_dir<1, 5>(z, eps_ref, st);
+  e = w7 ? launch_dir<1, 7>(z, eps_ref, sn, th, st) : launch_dir<1, 5>(z, eps_ref, sn, th, st);
   if (e != cudaSuccess) return e;
   *n_launch += 2;
   if (z.d.mz > 1) {
-    e = w7 ? launch_dir<2, 7>(z, eps_ref, st) : launch_dir<2, 5>(z, eps_ref, st);
+    e = w7 ? launch_dir<2, 7>(z, eps_ref, sn, th, st) : launch_dir<2, 5>(z, eps_ref, sn, th, st);
     if (e != cudaSuccess) return e;
     *n_launch += 1;
   }

@@ -53,8 +53,10 @@ struct MixTile {
 
 }  // namespace
 
-template <int DIR, int ORD, int NS>
-__global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref, const __grid_constant__ Thermo thermo) {
+// HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
+template <int DIR, int ORD, int NS, bool HYB>
+__global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref, const __grid_constant__ Thermo thermo,
+                                                          const double *sensor, double threshold) {
   using T = MixTile<DIR, ORD, NS>;
   using V = MixVals<NS>;
   constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
@@ -176,6 +178,7 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
     double lam = 0;
 #pragma unroll
     for (int q = 0; q < NPF; ++q) lam = max(lam, s[T::spt(V::LAM, c, t + q)]);
+    const bool shock = !HYB || face_shocked(sensor, idf, d.stride(g, DIR), g, threshold);
     double sbq[NPF], sbf[NPF];
 #pragma unroll
     for (int q = 0; q < NPF; ++q) {
@@ -233,8 +236,8 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
         if (q < NPF - 1) vp[q] = 0.5 * jq * (LF + lam * LQ);
         if (q > 0) vmn[q - 1] = 0.5 * jq * (LF - lam * LQ);
       }
-      if constexpr (ORD == 7) fChar[l] = weno7_z(vp, vmn, eps_ref);
-      else fChar[l] = weno5_js(vp, vmn, eps_ref);
+      if constexpr (ORD == 7) fChar[l] = shock ? weno7_z(vp, vmn, eps_ref) : weno7_linear(vp, vmn);
+      else fChar[l] = shock ? weno5_js(vp, vmn, eps_ref) : weno5_linear(vp, vmn);
     }
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
@@ -249,8 +252,8 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
         if (q < NPF - 1) vp[q] = 0.5 * jq * (LF + lam * LQ);
         if (q > 0) vmn[q - 1] = 0.5 * jq * (LF - lam * LQ);
       }
-      if constexpr (ORD == 7) fChar[5 + l] = weno7_z(vp, vmn, eps_ref);
-      else fChar[5 + l] = weno5_js(vp, vmn, eps_ref);
+      if constexpr (ORD == 7) fChar[5 + l] = shock ? weno7_z(vp, vmn, eps_ref) : weno7_linear(vp, vmn);
+      else fChar[5 + l] = shock ? weno5_js(vp, vmn, eps_ref) : weno5_linear(vp, vmn);
     }
     const double f034 = fChar[0] + fChar[3] + fChar[4];
     const double f04 = fChar[0] - fChar[4];
@@ -287,21 +290,29 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
 namespace {
 
 template <int DIR, int ORD>
-cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, cudaStream_t st) {
+cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, const double *sensor, double threshold,
+                           cudaStream_t st) {
   using T = MixTile<DIR, ORD, kMaxSpec>;
   const Dims &d = z.d;
   dim3 grid;
   if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
-  weno_mix_flux_diff<DIR, ORD, kMaxSpec><<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th);
+  if (sensor)
+    weno_mix_flux_diff<DIR, ORD, kMaxSpec, true><<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, sensor, threshold);
+  else
+    weno_mix_flux_diff<DIR, ORD, kMaxSpec, false><<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, nullptr, threshold);
   return cudaGetLastError();
 }
 
 template <int DIR, int ORD>
 cudaError_t set_mix_attr() {
-  return cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)MixTile<DIR, ORD, kMaxSpec>::smem_bytes());
+  const int b = (int)MixTile<DIR, ORD, kMaxSpec>::smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec, true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 }  // namespace
@@ -319,14 +330,16 @@ cudaError_t weno_mix_init_attributes() {
 // x, y and (3-D) z sweeps; the species count is fixed at 9 (kMaxSpec).
 cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch) {
   const double eps_ref = kEpsWeno * p.weno_eps_scale;
+  const double tr = p.sensor_threshold;
+  const double *sn = tr > 1e-10 ? z.shock_sensor : nullptr;  // hybrid UD + WENO
   const bool w7 = p.inviscid_scheme == 72;
-  cudaError_t e = w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, st) : launch_mix_dir<0, 5>(z, eps_ref, th, st);
+  cudaError_t e = w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, sn, tr, st) : launch_mix_dir<0, 5>(z, eps_ref, th, sn, tr, st);
   if (e != cudaSuccess) return e;
-  e = w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, st) : launch_mix_dir<1, 5>(z, eps_ref, th, st);
+  e = w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, sn, tr, st) : launch_mix_dir<1, 5>(z, eps_ref, th, sn, tr, st);
   if (e != cudaSuccess) return e;
   *n_launch += 2;
   if (z.d.mz > 1) {
-    e = w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, st) : launch_mix_dir<2, 5>(z, eps_ref, th, st);
+    e = w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, sn, tr, st) : launch_mix_dir<2, 5>(z, eps_ref, th, sn, tr, st);
     if (e != cudaSuccess) return e;
     *n_launch += 1;
   }

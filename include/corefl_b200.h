@@ -64,8 +64,11 @@ typedef struct cfk_param {
   double Pr, Sc, cfl, dt;
   double weno_eps_scale;   /* (rho_ref * v_ref)^2, reference src/DParameter.cu:25-28 */
   double v_ref, rho_ref;
-  double sensor_threshold; /* <= 1e-10: WENO nonlinear weights everywhere */
+  double sensor_threshold; /* shockSensor_threshold; <= 1e-10: WENO nonlinear weights everywhere,
+                              above: hybrid UD5/UD7 + WENO5/WENO7 (schemes 52/72) */
   int device;              /* CUDA device ordinal the context runs on */
+  int shock_sensor;        /* 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump */
+  double sensor_eps;       /* shockSensor_epsilon (reference default -1) */
 } cfk_param;
 
 /* Device pointers of one block, field for field the arrays of the reference's
@@ -78,6 +81,8 @@ typedef struct cfk_zone {
   double *mul, *mach;            /* ngg ghosts */
   double *acoustic_speed, *gamma, *thermal_conductivity, *rho_D, *reaction_timeScale; /* mixture */
   double *dq, *dt_local, *Cn;    /* n_var, 1, n_var planes, 0 ghosts */
+  double *shock_sensor;          /* 1 plane, ngg ghosts, zero-initialised; hybrid schemes only.  NULL: the
+                                    context allocates its own */
 } cfk_zone;
 
 /* Species, thermo, transport and kinetics tables of a mechanism — the
@@ -131,6 +136,13 @@ int cfk_compute_viscous_flux(cfk_ctx *ctx, void *stream);
  * compute_inviscid_flux<M> (reference src/InviscidScheme.cu:12-26), including
  * compute_convective_term_weno (reference src/WENO.cu:2914-2946). */
 int cfk_compute_inviscid_flux(cfk_ctx *ctx, void *stream);
+/* Shock sensor of the hybrid schemes on the interior nodes (ghost layers
+ * keep 0).  Replaces compute_shock_sensor (reference
+ * src/FieldOperation.cu:158-179), called once per step (reference
+ * src/RK.cuh:112-117, src/StrangSplitting.cu:19-24); cfk_rk3_step and
+ * cfk_wu_splitting_step call it themselves.  No-op unless
+ * sensor_threshold > 1e-10. */
+int cfk_compute_shock_sensor(cfk_ctx *ctx, void *stream);
 /* SSP-RK3 stage update of cv and bv/sv.  Replaces update_cv_and_bv_rk<M>
  * (reference src/RK.cuh:224-281). */
 int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);

@@ -208,10 +208,10 @@ double orc_weno7(const double *vp, const double *vm, double eps, int if_shock) {
 /* (src/WENO.cu:10-244, 414-654).  Mixture branch lives in oracle_mix.c.      */
 /* ------------------------------------------------------------------------ */
 void orc_weno_face_mixture(const orc_zone *z, const orc_param *p, int dir, long idx, double kx, double ky,
-                           double kz, double eps_ref, double *fc);
+                           double kz, double eps_ref, int if_shock, double *fc);
 
 static void weno_face_air_or_cp(const orc_zone *z, const orc_param *p, int dir, long idx, double kx, double ky,
-                                double kz, double eps_ref, double *fc) {
+                                double kz, double eps_ref, int if_shock, double *fc) {
   const int ngg = z->ngg, nv = p->n_var, sch = p->inviscid_scheme;
   const long sz = psz(z, ngg), s = pstride(z, ngg, dir);
   const int mm = 3 * dir;
@@ -262,16 +262,16 @@ static void weno_face_air_or_cp(const orc_zone *z, const orc_param *p, int dir, 
       else if (l == 4) eps_here = eps_scaled[2];
       if (order7) {
         /* vp = fp[i-3..i+3], vm = fm[i-2..i+4]; point m corresponds to offset m-3 */
-        fc[l] = orc_weno7(&fp[l][0], &fm[l][1], eps_here, 1);
+        fc[l] = orc_weno7(&fp[l][0], &fm[l][1], eps_here, if_shock);
       } else {
-        fc[l] = orc_weno5(&fp[l][0], &fm[l][1], eps_here, 1);
+        fc[l] = orc_weno5(&fp[l][0], &fm[l][1], eps_here, if_shock);
       }
     }
     return;
   }
 
   if (p->mech) {
-    orc_weno_face_mixture(z, p, dir, idx, kx, ky, kz, eps_ref, fc);
+    orc_weno_face_mixture(z, p, dir, idx, kx, ky, kz, eps_ref, if_shock, fc);
     return;
   }
 
@@ -368,7 +368,7 @@ static void weno_face_air_or_cp(const orc_zone *z, const orc_param *p, int dir, 
       if (m < np - 1) vPlus[m] = 0.5 * F[6][m] * (LFm + max_lambda * LQm);
       if (m > 0) vMinus[m - 1] = 0.5 * F[6][m] * (LFm - max_lambda * LQm);
     }
-    fChar[l] = order7 ? orc_weno7(vPlus, vMinus, eps_ref, 1) : orc_weno5(vPlus, vMinus, eps_ref, 1);
+    fChar[l] = order7 ? orc_weno7(vPlus, vMinus, eps_ref, if_shock) : orc_weno5(vPlus, vMinus, eps_ref, if_shock);
   }
   temp1 = fChar[0] + fChar[3] + fChar[4];
   temp3 = fChar[0] - fChar[4];
@@ -402,14 +402,21 @@ static void weno_direction(orc_zone *z, const orc_param *p, int dir) {
         const double kx = 0.5 * (z->metric[id + mm * sz] + z->metric[idn + mm * sz]);
         const double ky = 0.5 * (z->metric[id + (mm + 1) * sz] + z->metric[idn + (mm + 1) * sz]);
         const double kz = 0.5 * (z->metric[id + (mm + 2) * sz] + z->metric[idn + (mm + 2) * sz]);
+        /* hybrid scheme: linear weights unless a node of the stencil is
+         * shocked (src/WENO.cu:839-849, 1580-1590 and the z analogue) */
+        int if_shock = 1;
+        if (p->sensor_threshold > 1e-10) {
+          if_shock = 0;
+          for (int ii = -ngg + 1; ii <= ngg; ++ii)
+            if (z->shock_sensor[id + ii * s] > p->sensor_threshold) { if_shock = 1; break; }
+        }
         double fc[ORC_MAX_SPEC + 5];
-        weno_face_air_or_cp(z, p, dir, id, kx, ky, kz, eps_ref, fc);
+        weno_face_air_or_cp(z, p, dir, id, kx, ky, kz, eps_ref, if_shock, fc);
         if (p->positive_preserving && nv > 5) orc_positive_preserving_face(z, p, dir, id, fc);
         for (int l = 0; l < nv; ++l) flux[id + l * sz] = fc[l];
       }
     }
   }
-  (void)s;
   /* derivative: dq -= F(i) - F(i-1) */
   const long szq = psz(z, 0);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -728,6 +735,77 @@ static void local_time_step(orc_zone *z, const orc_param *p, int with_reaction) 
       }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Shock sensors (src/FieldOperation.cu:74-179)                               */
+/* ------------------------------------------------------------------------ */
+static double ducros_sensor(const orc_zone *z, double eps, long id) {
+  const long sz = psz(z, z->ngg);
+  const long si = 1, sj = pstride(z, z->ngg, 1), sk = pstride(z, z->ngg, 2);
+  const double *mt = z->metric, *bv = z->bv;
+  const double xi_x = mt[id], xi_y = mt[id + sz], xi_z = mt[id + 2 * sz];
+  const double eta_x = mt[id + 3 * sz], eta_y = mt[id + 4 * sz], eta_z = mt[id + 5 * sz];
+  const double zeta_x = mt[id + 6 * sz], zeta_y = mt[id + 7 * sz], zeta_z = mt[id + 8 * sz];
+  const double oneD12 = 1.0 / 12.0, twoD3 = 2.0 / 3.0;
+  double d[3][3];
+  for (int v = 0; v < 3; ++v) {
+    const double *f = bv + (v + 1) * sz;
+    const long st[3] = {si, sj, sk};
+    for (int a = 0; a < 3; ++a)
+      d[v][a] = oneD12 * f[id - 2 * st[a]] - twoD3 * f[id - st[a]] + twoD3 * f[id + st[a]] - oneD12 * f[id + 2 * st[a]];
+  }
+  const double duDx = d[0][0] * xi_x + d[0][1] * eta_x + d[0][2] * zeta_x;
+  const double dvDy = d[1][0] * xi_y + d[1][1] * eta_y + d[1][2] * zeta_y;
+  const double dwDz = d[2][0] * xi_z + d[2][1] * eta_z + d[2][2] * zeta_z;
+  double divV2 = duDx + dvDy + dwDz;
+  if (divV2 > 0) return 0;
+  const double duDy = d[0][0] * xi_y + d[0][1] * eta_y + d[0][2] * zeta_y;
+  const double duDz = d[0][0] * xi_z + d[0][1] * eta_z + d[0][2] * zeta_z;
+  const double dvDx = d[1][0] * xi_x + d[1][1] * eta_x + d[1][2] * zeta_x;
+  const double dvDz = d[1][0] * xi_z + d[1][1] * eta_z + d[1][2] * zeta_z;
+  const double dwDx = d[2][0] * xi_x + d[2][1] * eta_x + d[2][2] * zeta_x;
+  const double dwDy = d[2][0] * xi_y + d[2][1] * eta_y + d[2][2] * zeta_y;
+  divV2 *= divV2;
+  const double curl2 = (dwDy - dvDz) * (dwDy - dvDz) + (duDz - dwDx) * (duDz - dwDx) + (dvDx - duDy) * (dvDx - duDy);
+  return divV2 / (divV2 + curl2 + eps);
+}
+
+static double jameson_sensor(const orc_zone *z, long id) {
+  const long sz = psz(z, z->ngg), sj = pstride(z, z->ngg, 1), sk = pstride(z, z->ngg, 2);
+  const double *p = z->bv + 4 * sz;
+  const double twoP = p[id] * 2;
+  const double pI = p[id + 1] + p[id - 1], pJ = p[id + sj] + p[id - sj], pK = p[id + sk] + p[id - sk];
+  return fabs(pI - twoP) / (pI + twoP) + fabs(pJ - twoP) / (pJ + twoP) + fabs(pK - twoP) / (pK + twoP);
+}
+
+static double jump_sensor(const orc_zone *z, long id) {
+  const long sz = psz(z, z->ngg), sj = pstride(z, z->ngg, 1), sk = pstride(z, z->ngg, 2);
+  const double *bv = z->bv;
+  const double rho = bv[id], rhoI = 1.0 / rho, p = bv[id + 4 * sz], pI = 1.0 / p;
+  double s = 0;
+  s = fmax(s, fabs(bv[id + 1] - rho) * rhoI);
+  s = fmax(s, fabs(bv[id + sj] - rho) * rhoI);
+  s = fmax(s, fabs(bv[id + sk] - rho) * rhoI);
+  s = fmax(s, fabs(bv[id + 1 + 4 * sz] - p) * pI);
+  s = fmax(s, fabs(bv[id + sj + 4 * sz] - p) * pI);
+  s = fmax(s, fabs(bv[id + sk + 4 * sz] - p) * pI);
+  return s;
+}
+
+void orc_compute_shock_sensor(orc_zone *z, const orc_param *p) {
+  const int g = z->ngg;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < z->mz; ++k)
+    for (int j = 0; j < z->my; ++j)
+      for (int i = 0; i < z->mx; ++i) {
+        const long id = pidx(z, g, i, j, k);
+        double sensor;
+        if (p->shock_sensor == 1) sensor = jameson_sensor(z, id);
+        else if (p->shock_sensor == 2) sensor = jump_sensor(z, id);
+        else sensor = ducros_sensor(z, p->sensor_eps, id);
+        z->shock_sensor[id] = sensor;
+      }
+}
+
 double orc_global_time_step(const orc_zone *z) {
   const long n = psz(z, 0);
   double dt = 1e6;
@@ -900,6 +978,7 @@ double orc_wu_splitting_step(orc_zone *z, const orc_param *p, double dt_fixed) {
     orc_local_time_step_without_reaction(z, p);
     dt = orc_global_time_step(z);
   }
+  if (p->sensor_threshold > 1e-10) orc_compute_shock_sensor(z, p); /* src/StrangSplitting.cu:19-24 */
   memset(z->dq, 0, sizeof(double) * szq * p->n_var);
   orc_compute_viscous_flux(z, p);
   orc_compute_inviscid_flux(z, p);
@@ -923,6 +1002,7 @@ double orc_wu_splitting_step(orc_zone *z, const orc_param *p, double dt_fixed) {
 double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed) {
   const long sz = psz(z, z->ngg), szq = psz(z, 0);
   memcpy(z->qn, z->cv, sizeof(double) * sz * p->n_var);
+  if (p->sensor_threshold > 1e-10) orc_compute_shock_sensor(z, p); /* src/RK.cuh:112-116 */
   double dt = dt_fixed;
   if (!p->fixed_dt) {
     orc_local_time_step(z, p);

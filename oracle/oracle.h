@@ -40,6 +40,8 @@ typedef struct {
   double *dq, *dt_local, *Cn;
   /* 1 ghost */
   double *vis_flux;
+  /* ngg ghosts, zero outside the interior (hybrid WENO only; may be NULL) */
+  double *shock_sensor;
 } orc_zone;
 
 /* Species / mechanism tables (reference src/DParameter.cuh:84-130). */
@@ -83,6 +85,8 @@ typedef struct {
   int n_face;
   orc_face faces[6];
   const orc_mech *mech;  /* NULL for the calorically perfect air model */
+  int shock_sensor;      /* 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump */
+  double sensor_eps;     /* shockSensor_epsilon */
 } orc_param;
 
 /* zone memory management (host, zero-filled) */
@@ -99,6 +103,8 @@ void orc_compute_viscous_flux(orc_zone *z, const orc_param *p);
 void orc_update_cv_and_bv_rk(orc_zone *z, const orc_param *p, double dt, int rk);
 void orc_apply_boundary_conditions(orc_zone *z, const orc_param *p);
 void orc_eliminate_k_gradient(orc_zone *z, const orc_param *p);
+/* compute_shock_sensor (src/FieldOperation.cu:74-179) on the interior nodes */
+void orc_compute_shock_sensor(orc_zone *z, const orc_param *p);
 /* One SSP-RK3 step (reference src/RK.cuh:84-212); returns the dt used. */
 double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed);
 /* Stage update with dq - Cn (reference src/StrangSplitting.cu:504-562). */

@@ -254,7 +254,7 @@ double orc_mixture_max_diffuse_vel(const orc_zone *z, const orc_param *p, long i
 /* Characteristic WENO face flux with species (src/WENO.cu:1096-1469)        */
 /* ------------------------------------------------------------------------ */
 void orc_weno_face_mixture(const orc_zone *z, const orc_param *p, int dir, long idx, double kx, double ky,
-                           double kz, double eps_ref, double *fc) {
+                           double kz, double eps_ref, int if_shock, double *fc) {
   const orc_mech *mech = p->mech;
   const int ngg = z->ngg, ns = mech->n_spec, nv = p->n_var;
   const long sz = psz(z, ngg), s = pstride(z, ngg, dir);
@@ -375,7 +375,7 @@ void orc_weno_face_mixture(const orc_zone *z, const orc_param *p, int dir, long 
       if (m < np - 1) vPlus[m] = 0.5 * F[6][m] * (LFm + max_lambda * LQm);
       if (m > 0) vMinus[m - 1] = 0.5 * F[6][m] * (LFm - max_lambda * LQm);
     }
-    fChar[l] = order7 ? orc_weno7(vPlus, vMinus, eps_ref, 1) : orc_weno5(vPlus, vMinus, eps_ref, 1);
+    fChar[l] = order7 ? orc_weno7(vPlus, vMinus, eps_ref, if_shock) : orc_weno5(vPlus, vMinus, eps_ref, if_shock);
   }
   for (int l = 0; l < ns; ++l) {
     double vPlus[8], vMinus[8];
@@ -385,7 +385,7 @@ void orc_weno_face_mixture(const orc_zone *z, const orc_param *p, int dir, long 
       if (m < np - 1) vPlus[m] = 0.5 * F[6][m] * (LFm + max_lambda * LQm);
       if (m > 0) vMinus[m - 1] = 0.5 * F[6][m] * (LFm - max_lambda * LQm);
     }
-    fChar[5 + l] = order7 ? orc_weno7(vPlus, vMinus, eps_ref, 1) : orc_weno5(vPlus, vMinus, eps_ref, 1);
+    fChar[5 + l] = order7 ? orc_weno7(vPlus, vMinus, eps_ref, if_shock) : orc_weno5(vPlus, vMinus, eps_ref, if_shock);
   }
   temp1 = fChar[0] + fChar[3] + fChar[4];
   temp3 = fChar[0] - fChar[4];

@@ -26,7 +26,7 @@ class orc_zone(ctypes.Structure):
     _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
         (n, _DP) for n in ("cv", "bv", "sv", "qn", "metric", "jac", "mul", "mach", "fFlux", "gFlux", "hFlux",
                            "acoustic_speed", "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
-                           "dt_local", "Cn", "vis_flux")
+                           "dt_local", "Cn", "vis_flux", "shock_sensor")
     ]
 
 
@@ -39,7 +39,8 @@ class orc_param(ctypes.Structure):
         ("Sc", ctypes.c_double), ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("fixed_dt", ctypes.c_int),
         ("weno_eps_scale", ctypes.c_double), ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double),
         ("sensor_threshold", ctypes.c_double), ("chem_advance_method", ctypes.c_int), ("n_face", ctypes.c_int),
-        ("faces", orc_face * 6), ("mech", ctypes.c_void_p),
+        ("faces", orc_face * 6), ("mech", ctypes.c_void_p), ("shock_sensor", ctypes.c_int),
+        ("sensor_eps", ctypes.c_double),
     ]
 
 
@@ -121,7 +122,7 @@ def lib() -> ctypes.CDLL:
         zp, pp = ctypes.POINTER(orc_zone), ctypes.POINTER(orc_param)
         for name in ("orc_compute_cv_from_bv", "orc_update_physical_properties", "orc_local_time_step",
                      "orc_compute_inviscid_flux", "orc_compute_viscous_flux", "orc_apply_boundary_conditions",
-                     "orc_eliminate_k_gradient"):
+                     "orc_eliminate_k_gradient", "orc_compute_shock_sensor"):
             getattr(L, name).argtypes = [zp, pp]
             getattr(L, name).restype = None
         L.orc_update_cv_and_bv_rk.argtypes = [zp, pp, ctypes.c_double, ctypes.c_int]
@@ -175,6 +176,7 @@ class OracleZone:
             "acoustic_speed": np.zeros(P), "gamma": np.zeros(P), "thermal_conductivity": np.zeros(P),
             "rho_D": np.zeros((ns, P)), "reaction_timeScale": np.zeros(P), "dq": np.zeros((nv, N)),
             "dt_local": np.zeros(N), "Cn": np.zeros((nv, N)), "vis_flux": np.zeros((nv - 1, P1)),
+            "shock_sensor": np.zeros(P),
         }
         if c.sv.shape[0]:
             self.arrays["sv"][: c.sv.shape[0]] = c.sv

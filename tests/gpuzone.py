@@ -8,7 +8,7 @@ import corefl_b200 as cfk
 
 
 class GpuZone:
-    def __init__(self, case, param_overrides=None):
+    def __init__(self, case, param_overrides=None, sensor_array=True):
         import torch
 
         self.torch = torch
@@ -36,6 +36,8 @@ class GpuZone:
                 self.t[k] = z(P)
             self.t["rho_D"] = z(ns, P)
             self.t["Cn"] = z(nv, N)
+        if sensor_array and p.get("sensor_threshold", 0.0) > 1e-10:
+            self.t["shock_sensor"] = z(P)  # else the context allocates its own
         self.ctx.bind(c.mx, c.my, c.mz, c.ngg, {k: v.data_ptr() for k, v in self.t.items()})
         if ns:
             self.ctx.set_mechanism(c.mech)

@@ -122,6 +122,9 @@ def test_param_from_setup_reads_reference_keys(tmp_path):
         "real cfl = 0.5\n"
         "bool fixed_time_step = 0\n"
         "int viscous_order = 0\n"
+        "int shock_sensor = 1\n"
+        "real shockSensor_threshold = 0.02\n"
+        "real shockSensor_epsilon = 1e-6\n"
         "array string boundary_conditions {\n  outflow\n}\n"
         "string reference_state = left\n"
         "struct  left {\n    string type = inflow\n    int label = 5\n    real velocity = 0\n"
@@ -132,6 +135,7 @@ def test_param_from_setup_reads_reference_keys(tmp_path):
     assert rc == 0, err.value
     assert p.inviscid_scheme == 52 and p.viscous_order == 0 and p.cfl == 0.5 and p.fixed_dt == 0
     assert p.n_var == 5 and p.Pr == 0.72
+    assert p.shock_sensor == 1 and p.sensor_threshold == 0.02 and p.sensor_eps == 1e-6
     # |u| < 1, so v_ref is the speed of sound sqrt(gamma p / rho)
     assert p.v_ref == pytest.approx(np.sqrt(1.4), rel=1e-12)
     assert p.weno_eps_scale == pytest.approx(1.4, rel=1e-12)
@@ -147,4 +151,10 @@ def test_create_rejects_unsupported_settings():
     h = ctypes.c_void_p()
     assert corefl_b200.lib().cfk_create(ctypes.byref(p), ctypes.byref(h)) == -1
     p = corefl_b200.make_param(dict(dim=3, n_var=6, inviscid_scheme=72), [])
+    assert corefl_b200.lib().cfk_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    # the hybrid scheme exists for WENO5/7 only, with sensors 0..2
+    p = corefl_b200.make_param(dict(dim=3, n_var=5, inviscid_scheme=4, reconstruction=2, sensor_threshold=0.1), [])
+    assert corefl_b200.lib().cfk_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    p = corefl_b200.make_param(dict(dim=3, n_var=5, inviscid_scheme=72, weno_eps_scale=1.0, sensor_threshold=0.1,
+                                    shock_sensor=3), [])
     assert corefl_b200.lib().cfk_create(ctypes.byref(p), ctypes.byref(h)) == -1
