@@ -13,7 +13,8 @@ cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int 
 cudaError_t weno_air_init_attributes();
 cudaError_t launch_pv_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t pv_air_init_attributes();
-cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
+cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev, double dt_host,
+                            cudaStream_t st, int *n_launch);
 cudaError_t weno_mix_init_attributes();
 cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
 cudaError_t viscous_mix_init_attributes();
@@ -69,10 +70,12 @@ int ghost_layers(int scheme) {
 }
 
 // compute_inviscid_flux dispatch (reference src/InviscidScheme.cu:12-26);
-// th: host copy of the mixture tables, nullptr for air.
-cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, int *n) {
+// th: host copy of the mixture tables, nullptr for air.  dt_dev / dt_host:
+// the step's dt (DParameter::dt) for the positive-preserving limiter.
+cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, const double *dt_dev, double dt_host,
+                            cudaStream_t st, int *n) {
   if (p.inviscid_scheme == 52 || p.inviscid_scheme == 72)
-    return th ? launch_weno_mix(z, p, *th, st, n) : launch_weno_air(z, p, st, n);
+    return th ? launch_weno_mix(z, p, *th, dt_dev, dt_host, st, n) : launch_weno_air(z, p, st, n);
   return launch_pv_air(z, p, st, n);
 }
 
@@ -106,7 +109,10 @@ int validate(const cfk_param *p, std::string &why) {
     why = "shock_sensor must be 0 (Ducros), 1 (Jameson) or 2 (density/pressure jump)";
     return -1;
   }
-  if (p->positive_preserving && p->n_spec > 0) { why = "positive_preserving is not supported by this build"; return -1; }
+  if (p->positive_preserving && p->n_spec > 0 && !(s == 52 || s == 72 || s == 0)) {
+    why = "positive_preserving is supported with the WENO schemes (52, 72)";
+    return -1;
+  }
   if (p->n_spec > 0 && s != 0 && !(s == 52 || s == 72)) {
     why = "the mixture model is supported with WENO5/7 characteristic fluxes (52, 72) in this build";
     return -1;
@@ -401,7 +407,9 @@ int cfk_compute_inviscid_flux(cfk_ctx *c, void *stream) {
   if (c->hp.inviscid_scheme == 0) return fail(c, CFK_ERR_STATE, "inviscid_scheme 0 has no flux");
   if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
-  CFK_CHECK(c, launch_inviscid(c->z, c->p, thermo_host(c), S(stream), &n), "inviscid flux");
+  // the limiter's dt: the fixed dt, else the last CFL dt on the device
+  const double *dt_dev = c->p.fixed_dt ? nullptr : reinterpret_cast<const double *>(c->d_dt_bits);
+  CFK_CHECK(c, launch_inviscid(c->z, c->p, thermo_host(c), dt_dev, c->hp.dt, S(stream), &n), "inviscid flux");
   c->launches += n;
   return CFK_OK;
 }
@@ -492,7 +500,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
-      CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");
+      CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), dt_dev, c->hp.dt, st, &n), "inviscid flux");
     }
     {
       PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
@@ -542,7 +550,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   }
   CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
   if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
-  CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");
+  CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, st, &n), "inviscid flux");
   CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "Cn copy");
   // wu_reaction_subStep (:475-502)
   unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
@@ -557,7 +565,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
-    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), st, &n), "inviscid flux");
+    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;
     CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, st, &n), "boundary conditions");

@@ -51,12 +51,80 @@ struct MixTile {
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(NQ * C * NPT + NV * C * NF); }
 };
 
+// Positive-preserving limiter of the species face fluxes (reference
+// src/WENO.cu:1471-1540; the characteristic scheme has it in the x sweep
+// only).  For each species whose one-sided updates alpha/2 J rhoY -/+ dt f
+// would go negative, the face flux is blended towards the first-order flux
+// f1 = 1/2 (fp + U_L J_L rhoY_L) + 1/2 (fm - U_R J_R rhoY_R) with
+// fp/m = 1/2 J (U +/- c|grad k|) rhoY, theta in [0, 1].  Out of line: the
+// branch is rare and must not add registers to the face loop.  s/sf point at
+// the staged values and face fluxes of this tile; the species face fluxes
+// are updated in shared memory.
+template <int ORD, int NS>
+__device__ __noinline__ void pp_limit_x(const double *s, double *sf, int c, int t, const Zone &z, int64_t idl,
+                                        double dt, double alpha_dim, double rho_ref) {
+  using T = MixTile<0, ORD, NS>;
+  using V = MixVals<NS>;
+  const int pc = t + T::R;
+  const double jac_l = s[T::spt(V::J, c, pc)], jac_r = s[T::spt(V::J, c, pc + 1)];
+  const double alphaL = 0.5 * alpha_dim * jac_l, alphaR = 0.5 * alpha_dim * jac_r;
+  int start_l = -1;
+  for (int l = 0; l < NS; ++l) {
+    const double fl = sf[T::sfl(5 + l, c, t)];
+    const double up = alphaL * s[T::spt(V::Y0 + l, c, pc)] - dt * fl;
+    const double um = alphaR * s[T::spt(V::Y0 + l, c, pc + 1)] + dt * fl;
+    if (up < 0 || um < 0) { start_l = l; break; }
+  }
+  if (start_l < 0) return;
+  // c|grad k| of the two nodes, as staged by the reference (F[5])
+  const int64_t sz = z.d.plane(z.d.ngg);
+  double cg[2];
+  for (int n = 0; n < 2; ++n) {
+    const int64_t id = idl + n;
+    const double m0 = z.metric[id], m1 = z.metric[id + sz], m2 = z.metric[id + 2 * sz];
+    cg[n] = sqrt(m0 * m0 + m1 * m1 + m2 * m2) * z.acoustic_speed[id];
+  }
+  const double UkL = s[T::spt(V::U, c, pc)], UkR = s[T::spt(V::U, c, pc + 1)];
+  const double U1 = UkL * jac_l, U2 = UkR * jac_r;
+  for (int l = start_l; l < NS; ++l) {
+    const double fc = sf[T::sfl(5 + l, c, t)];
+    double f1 = 0, theta_p = 1.0, theta_m = 1.0;
+    bool f1_computed = false;
+    const double rhoYL = s[T::spt(V::Y0 + l, c, pc)], rhoYR = s[T::spt(V::Y0 + l, c, pc + 1)];
+    const double fp = 0.5 * jac_l * (UkL + cg[0]) * rhoYL;
+    const double fm = 0.5 * jac_r * (UkR - cg[1]) * rhoYR;
+    const double up = alphaL * rhoYL - dt * fc;
+    if (up < 0) {
+      f1 = 0.5 * (fp + U1 * rhoYL) + 0.5 * (fm - U2 * rhoYR);
+      f1_computed = true;
+      const double up_lf = alphaL * rhoYL - dt * f1;
+      if (abs(up - up_lf) > 1e-20 * rho_ref) theta_p = min(max((0 - up_lf) / (up - up_lf), 0.0), 1.0);
+    }
+    const double um = alphaR * rhoYR + dt * fc;
+    if (um < 0) {
+      if (!f1_computed) f1 = 0.5 * (fp + U1 * rhoYL) + 0.5 * (fm - U2 * rhoYR);
+      const double um_lf = alphaR * rhoYR + dt * f1;
+      if (abs(um - um_lf) > 1e-20 * rho_ref) theta_m = min(max((0 - um_lf) / (um - um_lf), 0.0), 1.0);
+    }
+    sf[T::sfl(5 + l, c, t)] = min(theta_p, theta_m) * (fc - f1) + f1;
+  }
+}
+
+// Settings of the positive-preserving limiter: off unless `on`; the step's
+// dt from the device (CFL runs) or the host (fixed dt); dt <= 0 selects the
+// node's dt_local as the reference does.
+struct PPArgs {
+  int on;
+  const double *dt_dev;
+  double dt_host, alpha_dim, rho_ref;
+};
+
 }  // namespace
 
 // HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
 template <int DIR, int ORD, int NS, bool HYB>
 __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref, const __grid_constant__ Thermo thermo,
-                                                          const double *sensor, double threshold) {
+                                                          const double *sensor, double threshold, PPArgs pp) {
   using T = MixTile<DIR, ORD, NS>;
   using V = MixVals<NS>;
   constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
@@ -84,6 +152,8 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
     else { t = item / C; c = item - t * C; }
   };
   const int mmo = 3 * DIR;
+  double dt_pp = 0;
+  if (DIR == 0 && pp.on) dt_pp = pp.dt_dev ? *pp.dt_dev : pp.dt_host;
 
   // ---- stage ------------------------------------------------------------
   for (int item = threadIdx.x; item < NPT * C; item += T::NT) {
@@ -272,6 +342,12 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
     }
     f4 -= bsum * cm * cm / gm1;
     sflx[T::sfl(4, c, t)] = f4;
+    if constexpr (DIR == 0) {
+      if (pp.on) {
+        const double dt = dt_pp > 0 ? dt_pp : z.dt_local[node_idx(0, c, f < 0 ? 0 : f)];
+        pp_limit_x<ORD, NS>(s, sflx, c, t, z, idf, dt, pp.alpha_dim, pp.rho_ref);
+      }
+    }
   }
   __syncthreads();
 
@@ -291,7 +367,7 @@ namespace {
 
 template <int DIR, int ORD>
 cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, const double *sensor, double threshold,
-                           cudaStream_t st) {
+                           const PPArgs &pp, cudaStream_t st) {
   using T = MixTile<DIR, ORD, kMaxSpec>;
   const Dims &d = z.d;
   dim3 grid;
@@ -299,9 +375,11 @@ cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, cons
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
   if (sensor)
-    weno_mix_flux_diff<DIR, ORD, kMaxSpec, true><<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, sensor, threshold);
+    weno_mix_flux_diff<DIR, ORD, kMaxSpec, true>
+        <<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, sensor, threshold, pp);
   else
-    weno_mix_flux_diff<DIR, ORD, kMaxSpec, false><<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, nullptr, threshold);
+    weno_mix_flux_diff<DIR, ORD, kMaxSpec, false>
+        <<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, nullptr, threshold, pp);
   return cudaGetLastError();
 }
 
@@ -328,18 +406,22 @@ cudaError_t weno_mix_init_attributes() {
 }
 
 // x, y and (3-D) z sweeps; the species count is fixed at 9 (kMaxSpec).
-cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch) {
+// dt_dev / dt_host: the step's dt for the positive-preserving limiter.
+cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev, double dt_host,
+                            cudaStream_t st, int *n_launch) {
   const double eps_ref = kEpsWeno * p.weno_eps_scale;
   const double tr = p.sensor_threshold;
   const double *sn = tr > 1e-10 ? z.shock_sensor : nullptr;  // hybrid UD + WENO
+  const PPArgs pp{p.positive_preserving ? 1 : 0, dt_dev, dt_host, p.dim == 3 ? 1.0 / 3.0 : 0.5, p.rho_ref};
+  const PPArgs off{0, nullptr, 0.0, 0.0, 0.0};
   const bool w7 = p.inviscid_scheme == 72;
-  cudaError_t e = w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, sn, tr, st) : launch_mix_dir<0, 5>(z, eps_ref, th, sn, tr, st);
+  cudaError_t e = w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, sn, tr, pp, st) : launch_mix_dir<0, 5>(z, eps_ref, th, sn, tr, pp, st);
   if (e != cudaSuccess) return e;
-  e = w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, sn, tr, st) : launch_mix_dir<1, 5>(z, eps_ref, th, sn, tr, st);
+  e = w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, sn, tr, off, st) : launch_mix_dir<1, 5>(z, eps_ref, th, sn, tr, off, st);
   if (e != cudaSuccess) return e;
   *n_launch += 2;
   if (z.d.mz > 1) {
-    e = w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, sn, tr, st) : launch_mix_dir<2, 5>(z, eps_ref, th, sn, tr, st);
+    e = w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, sn, tr, off, st) : launch_mix_dir<2, 5>(z, eps_ref, th, sn, tr, off, st);
     if (e != cudaSuccess) return e;
     *n_launch += 1;
   }

@@ -380,7 +380,7 @@ static void weno_face_air_or_cp(const orc_zone *z, const orc_param *p, int dir, 
   fc[4] = temp2 * temp1 - Uk_bar * cm * temp3 + Un * fChar[1] + Uq * fChar[2] - cm * cm / gm1 * fChar[3];
 }
 
-void orc_positive_preserving_face(const orc_zone *z, const orc_param *p, int dir, long idx, double *fc);
+void orc_positive_preserving_face(const orc_zone *z, const orc_param *p, int dir, int i, int j, int k, double *fc);
 
 /* compute_convective_term_weno (src/WENO.cu:2914-2946): x, y, z face fluxes then
  * compute_derivative_{x,y,z} (src/WENO.cu:1544, 2219, 2885). */
@@ -412,7 +412,9 @@ static void weno_direction(orc_zone *z, const orc_param *p, int dir) {
         }
         double fc[ORC_MAX_SPEC + 5];
         weno_face_air_or_cp(z, p, dir, id, kx, ky, kz, eps_ref, if_shock, fc);
-        if (p->positive_preserving && nv > 5) orc_positive_preserving_face(z, p, dir, id, fc);
+        /* characteristic WENO: the limiter exists in the x sweep only
+         * (src/WENO.cu:1471-1540; the y and z sweeps have none) */
+        if (p->positive_preserving && nv > 5 && dir == 0) orc_positive_preserving_face(z, p, dir, i, j, k, fc);
         for (int l = 0; l < nv; ++l) flux[id + l * sz] = fc[l];
       }
     }
@@ -978,6 +980,7 @@ double orc_wu_splitting_step(orc_zone *z, const orc_param *p, double dt_fixed) {
     orc_local_time_step_without_reaction(z, p);
     dt = orc_global_time_step(z);
   }
+  z->dt_step = dt;
   if (p->sensor_threshold > 1e-10) orc_compute_shock_sensor(z, p); /* src/StrangSplitting.cu:19-24 */
   memset(z->dq, 0, sizeof(double) * szq * p->n_var);
   orc_compute_viscous_flux(z, p);
@@ -1008,6 +1011,7 @@ double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed) {
     orc_local_time_step(z, p);
     dt = orc_global_time_step(z);
   }
+  z->dt_step = dt;
   for (int rk = 0; rk < 3; ++rk) {
     memset(z->dq, 0, sizeof(double) * szq * p->n_var);
     orc_compute_viscous_flux(z, p);

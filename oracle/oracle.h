@@ -42,6 +42,9 @@ typedef struct {
   double *vis_flux;
   /* ngg ghosts, zero outside the interior (hybrid WENO only; may be NULL) */
   double *shock_sensor;
+  /* the step's dt as DParameter::dt holds it after update_dt_global
+   * (src/DParameter.cu:396-398); read by the positive-preserving limiter */
+  double dt_step;
 } orc_zone;
 
 /* Species / mechanism tables (reference src/DParameter.cuh:84-130). */

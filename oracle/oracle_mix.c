@@ -404,11 +404,72 @@ void orc_weno_face_mixture(const orc_zone *z, const orc_param *p, int dir, long 
 }
 
 /* Positive-preserving limiter of the species face fluxes, characteristic
- * branch (src/WENO.cu:1471-1540). */
-void orc_positive_preserving_face(const orc_zone *z, const orc_param *p, int dir, long idx, double *fc) {
-  (void)z; (void)p; (void)dir; (void)idx; (void)fc;
-  fprintf(stderr, "oracle: the positive-preserving limiter is not restated\n");
-  abort();
+ * branch of the x sweep (src/WENO.cu:1471-1540).  For each species whose
+ * one-sided updates alpha/2 J rhoY -/+ dt f would go negative, the face flux
+ * is blended towards a first-order flux f1 with theta in [0, 1].  dt is the
+ * step's dt (DParameter::dt); when that is not positive the reference reads
+ * dt_local(i, j, k), which for the i = -1 face lies outside the array — here
+ * that face takes node 0's value. */
+void orc_positive_preserving_face(const orc_zone *z, const orc_param *p, int dir, int i, int j, int k, double *fc) {
+  const int ngg = z->ngg, ns = p->n_var - 5;
+  const long sz = psz(z, ngg), s = pstride(z, ngg, dir);
+  const long il = pidx(z, ngg, i, j, k), ir = il + s;
+  double dt = z->dt_step;
+  if (!(dt > 0)) dt = z->dt_local[pidx(z, 0, i < 0 ? 0 : i, j, k)];
+  const double alpha = p->dim == 3 ? 1.0 / 3.0 : 0.5;
+  const double jac_l = z->jac[il], jac_r = z->jac[ir];
+  const double alphaL = 0.5 * alpha * jac_l, alphaR = 0.5 * alpha * jac_r;
+  int start_l = -1;
+  for (int l = 0; l < ns; ++l) {
+    const double up = alphaL * z->cv[il + (5 + l) * sz] - dt * fc[5 + l];
+    const double um = alphaR * z->cv[ir + (5 + l) * sz] + dt * fc[5 + l];
+    if (up < 0 || um < 0) { start_l = l; break; }
+  }
+  if (start_l < 0) return;
+  /* Uk and c|grad k| of the two nodes (the staged F[0], F[5], F[6] of
+   * src/WENO.cu:1112-1137) */
+  double Uk[2], cg[2], J[2];
+  const long nd[2] = {il, ir};
+  const int mo = 3 * dir;
+  for (int n = 0; n < 2; ++n) {
+    const long id = nd[n];
+    const double q0 = z->cv[id], q1 = z->cv[id + sz], q2 = z->cv[id + 2 * sz], q3 = z->cv[id + 3 * sz];
+    const double m0 = z->metric[id + mo * sz], m1 = z->metric[id + (mo + 1) * sz], m2 = z->metric[id + (mo + 2) * sz];
+    Uk[n] = (q1 * m0 + q2 * m1 + q3 * m2) / q0;
+    cg[n] = sqrt(m0 * m0 + m1 * m1 + m2 * m2) * z->acoustic_speed[id];
+    J[n] = z->jac[id];
+  }
+  const double U1 = Uk[0] * jac_l, U2 = Uk[1] * jac_r;
+  for (int l = start_l; l < ns; ++l) {
+    double f1 = 0;
+    int f1_computed = 0;
+    double theta_p = 1.0, theta_m = 1.0;
+    const double rhoYL = z->cv[il + (5 + l) * sz], rhoYR = z->cv[ir + (5 + l) * sz];
+    const double fp = 0.5 * J[0] * (Uk[0] + cg[0]) * rhoYL;
+    const double fm = 0.5 * J[1] * (Uk[1] - cg[1]) * rhoYR;
+    const double up = alphaL * rhoYL - dt * fc[5 + l];
+    if (up < 0) {
+      f1 = 0.5 * (fp + U1 * rhoYL) + 0.5 * (fm - U2 * rhoYR);
+      f1_computed = 1;
+      const double up_lf = alphaL * rhoYL - dt * f1;
+      if (fabs(up - up_lf) > 1e-20 * p->rho_ref) {
+        theta_p = (0 - up_lf) / (up - up_lf);
+        if (theta_p > 1) theta_p = 1.0;
+        else if (theta_p < 0) theta_p = 0;
+      }
+    }
+    const double um = alphaR * rhoYR + dt * fc[5 + l];
+    if (um < 0) {
+      if (!f1_computed) f1 = 0.5 * (fp + U1 * rhoYL) + 0.5 * (fm - U2 * rhoYR);
+      const double um_lf = alphaR * rhoYR + dt * f1;
+      if (fabs(um - um_lf) > 1e-20 * p->rho_ref) {
+        theta_m = (0 - um_lf) / (um - um_lf);
+        if (theta_m > 1) theta_m = 1.0;
+        else if (theta_m < 0) theta_m = 0;
+      }
+    }
+    fc[5 + l] = fmin(theta_p, theta_m) * (fc[5 + l] - f1) + f1;
+  }
 }
 
 /* ------------------------------------------------------------------------ */

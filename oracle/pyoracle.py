@@ -27,7 +27,7 @@ class orc_zone(ctypes.Structure):
         (n, _DP) for n in ("cv", "bv", "sv", "qn", "metric", "jac", "mul", "mach", "fFlux", "gFlux", "hFlux",
                            "acoustic_speed", "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
                            "dt_local", "Cn", "vis_flux", "shock_sensor")
-    ]
+    ] + [("dt_step", ctypes.c_double)]
 
 
 class orc_param(ctypes.Structure):
