@@ -364,6 +364,7 @@ def main():
     ap.add_argument("--reconstruction", type=int, default=2, help="for schemes 1-4: 1 first order, 2 MUSCL, 3 NND2")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default WENO tile shapes")
     ap.add_argument("--no-reacting", action="store_true")
     ap.add_argument("--reacting-only", action="store_true", help="only the batched-reactor measurement")
     ap.add_argument("--reacting-cells", type=int, default=1 << 20)
@@ -415,6 +416,8 @@ def main():
     ctx.properties()
     ctx.cv_from_bv()
     ctx.sync()
+    # tile shapes of the WENO sweeps, timed on this block (outside the timed region)
+    tiles, tile_ms = ([0, 0, 0], None) if args.no_autotune else ctx.autotune_tiles(reps=3)
 
     for _ in range(args.warmup):
         ctx.rk3_step(want_dt=False)
@@ -531,7 +534,7 @@ def main():
                                    " + 2nd-order viscous, SSP-RK3 CFL 0.5 (device dt)",
                        "nodes": f"{n}^3", "global_nodes": nodes * world,
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cv alone "
-                       f"{5 * P * 8 / 1e6:.0f} MB)"},
+                       f"{5 * P * 8 / 1e6:.0f} MB)", "weno_tile_variants": tiles, "autotune_ms": tile_ms},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "gpu_launches": launches,
             "roofline": roofline,

@@ -34,6 +34,7 @@ class cfk_param(ctypes.Structure):
 _DP = ctypes.POINTER(ctypes.c_double)
 
 MAX_SPEC, MAX_REAC = 9, 24
+TILE_VARIANTS = 3  # CFK_TILE_VARIANTS
 
 
 class cfk_mechanism(ctypes.Structure):
@@ -141,6 +142,8 @@ def lib() -> ctypes.CDLL:
             "cfk_compute_viscous_flux": (i, [vp, vp]),
             "cfk_compute_inviscid_flux": (i, [vp, vp]),
             "cfk_compute_shock_sensor": (i, [vp, vp]),
+            "cfk_autotune_tiles": (i, [vp, i, ctypes.POINTER(d), ctypes.POINTER(i), vp]),
+            "cfk_set_tile_variants": (i, [vp, ctypes.POINTER(i)]),
             "cfk_update_cv_and_bv_rk": (i, [vp, d, i, vp]),
             "cfk_update_physical_properties": (i, [vp, vp]),
             "cfk_compute_cv_from_bv": (i, [vp, vp]),
@@ -313,6 +316,18 @@ class Context:
 
     def shock_sensor(self, stream=None):
         self._ck(self.L.cfk_compute_shock_sensor(self.h, stream), "shock sensor")
+
+    def autotune_tiles(self, reps=5, stream=None):
+        """Time each tile variant of every WENO sweep and keep the fastest;
+        returns (choice[3], ms[3][TILE_VARIANTS])."""
+        ms = (ctypes.c_double * (3 * TILE_VARIANTS))()
+        ch = (ctypes.c_int * 3)()
+        self._ck(self.L.cfk_autotune_tiles(self.h, reps, ms, ch, stream), "autotune_tiles")
+        return list(ch), [list(ms[d * TILE_VARIANTS:(d + 1) * TILE_VARIANTS]) for d in range(3)]
+
+    def set_tile_variants(self, var):
+        v = (ctypes.c_int * 3)(*var)
+        self._ck(self.L.cfk_set_tile_variants(self.h, v), "set_tile_variants")
 
     def update_rk(self, dt, rk, stream=None):
         self._ck(self.L.cfk_update_cv_and_bv_rk(self.h, dt, rk, stream), "update")

@@ -9,12 +9,15 @@
 #include "ctx.cuh"
 
 namespace cfk {
-cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t launch_weno_air(const Zone &z, const Param &p, const int *var, cudaStream_t st, int *n_launch);
+cudaError_t launch_weno_air_dir(const Zone &z, const Param &p, int dir, int var, cudaStream_t st);
 cudaError_t weno_air_init_attributes();
 cudaError_t launch_pv_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
 cudaError_t pv_air_init_attributes();
 cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev, double dt_host,
-                            cudaStream_t st, int *n_launch);
+                            const int *var, cudaStream_t st, int *n_launch);
+cudaError_t launch_weno_mix_dir(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev,
+                                double dt_host, int dir, int var, cudaStream_t st);
 cudaError_t weno_mix_init_attributes();
 cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
 cudaError_t viscous_mix_init_attributes();
@@ -73,9 +76,9 @@ int ghost_layers(int scheme) {
 // th: host copy of the mixture tables, nullptr for air.  dt_dev / dt_host:
 // the step's dt (DParameter::dt) for the positive-preserving limiter.
 cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, const double *dt_dev, double dt_host,
-                            cudaStream_t st, int *n) {
+                            const int *var, cudaStream_t st, int *n) {
   if (p.inviscid_scheme == 52 || p.inviscid_scheme == 72)
-    return th ? launch_weno_mix(z, p, *th, dt_dev, dt_host, st, n) : launch_weno_air(z, p, st, n);
+    return th ? launch_weno_mix(z, p, *th, dt_dev, dt_host, var, st, n) : launch_weno_air(z, p, var, st, n);
   return launch_pv_air(z, p, st, n);
 }
 
@@ -237,6 +240,8 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
     return fail(c, CFK_ERR_ARG,
                 "acoustic_speed, gamma, mul, thermal_conductivity and rho_D are required for the mixture flow path");
   if (c->hp.viscous_order > 0 && !zn->mul) return fail(c, CFK_ERR_ARG, "mul is required for viscous runs");
+  if (c->hp.positive_preserving && c->hp.n_spec > 0 && !zn->dt_local)
+    return fail(c, CFK_ERR_ARG, "dt_local is required with positive_preserving");
   if (c->hp.n_scalar > 0 && !zn->sv) return fail(c, CFK_ERR_ARG, "sv is required when n_scalar > 0");
   // 32-bit plane extents, as in the reference's int indexing
   const double P = (double)(zn->mx + 2 * zn->ngg) * (zn->my + 2 * zn->ngg) * (zn->mz + 2 * zn->ngg);
@@ -409,7 +414,8 @@ int cfk_compute_inviscid_flux(cfk_ctx *c, void *stream) {
   int n = 0;
   // the limiter's dt: the fixed dt, else the last CFL dt on the device
   const double *dt_dev = c->p.fixed_dt ? nullptr : reinterpret_cast<const double *>(c->d_dt_bits);
-  CFK_CHECK(c, launch_inviscid(c->z, c->p, thermo_host(c), dt_dev, c->hp.dt, S(stream), &n), "inviscid flux");
+  CFK_CHECK(c, launch_inviscid(c->z, c->p, thermo_host(c), dt_dev, c->hp.dt, c->tile_var, S(stream), &n),
+            "inviscid flux");
   c->launches += n;
   return CFK_OK;
 }
@@ -419,6 +425,76 @@ int cfk_compute_shock_sensor(cfk_ctx *c, void *stream) {
   if (!(c->p.sensor_threshold > 1e-10)) return CFK_OK;
   CFK_CHECK(c, launch_shock_sensor(c->z, c->p, S(stream)), "compute_shock_sensor");
   c->launches += 1;
+  return CFK_OK;
+}
+
+// Tile autotuner: times every tile variant of each WENO sweep on the bound
+// zone (into a scratch dq, so the caller's arrays are untouched) and keeps
+// the fastest per direction.  The primitive-variable kernels have one tile
+// shape per direction and are left as they are.
+int cfk_autotune_tiles(cfk_ctx *c, int reps, double *ms_out, int *choice_out, void *stream) {
+  NEED_ZONE(c);
+  const int s = c->hp.inviscid_scheme;
+  if (ms_out)
+    for (int n = 0; n < 3 * CFK_TILE_VARIANTS; ++n) ms_out[n] = 0;
+  if (!(s == 52 || s == 72)) {
+    if (choice_out) for (int d = 0; d < 3; ++d) choice_out[d] = c->tile_var[d];
+    return CFK_OK;
+  }
+  if (int r = need_mech_for_mixture(c)) return r;
+  if (reps < 1) reps = 1;
+  cudaStream_t st = S(stream);
+  const Zone &z0 = c->z;
+  const size_t N = (size_t)z0.d.plane(0);
+  double *scratch = nullptr;
+  CFK_CHECK(c, cudaMalloc(&scratch, N * c->p.n_var * sizeof(double)), "autotune scratch");
+  Zone zt = z0;
+  zt.dq = scratch;
+  Param pt = c->p;
+  pt.positive_preserving = 0;  // the limiter is a rare branch; tune the flux itself
+  const Thermo *th = thermo_host(c);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaError_t e = cudaMemsetAsync(scratch, 0, N * c->p.n_var * sizeof(double), st);
+  const int nd = z0.d.mz > 1 ? 3 : 2;
+  int choice[3] = {c->tile_var[0], c->tile_var[1], c->tile_var[2]};
+  auto sweep = [&](int dir, int var) -> cudaError_t {
+    return th ? launch_weno_mix_dir(zt, pt, *th, nullptr, c->hp.dt, dir, var, st)
+              : launch_weno_air_dir(zt, pt, dir, var, st);
+  };
+  for (int dir = 0; dir < nd && e == cudaSuccess; ++dir) {
+    double best = 1e300;
+    for (int var = 0; var < CFK_TILE_VARIANTS && e == cudaSuccess; ++var) {
+      e = sweep(dir, var);  // warm-up
+      if (e == cudaSuccess) e = cudaEventRecord(a, st);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) e = sweep(dir, var);
+      if (e == cudaSuccess) e = cudaEventRecord(b, st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(b);
+      float ms = 0;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+      const double avg = (double)ms / reps;
+      if (ms_out) ms_out[dir * CFK_TILE_VARIANTS + var] = avg;
+      if (e == cudaSuccess && avg < best) { best = avg; choice[dir] = var; }
+      c->launches += reps + 1;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return cuda_fail(c, e, "autotune");
+  for (int d = 0; d < 3; ++d) c->tile_var[d] = choice[d];
+  if (choice_out) for (int d = 0; d < 3; ++d) choice_out[d] = choice[d];
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  return CFK_OK;
+}
+
+int cfk_set_tile_variants(cfk_ctx *c, const int *var) {
+  if (!c || !var) return CFK_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (var[d] < 0 || var[d] >= CFK_TILE_VARIANTS) return fail(c, CFK_ERR_ARG, "tile variant out of range");
+  for (int d = 0; d < 3; ++d) c->tile_var[d] = var[d];
+  if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
   return CFK_OK;
 }
 
@@ -500,7 +576,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
-      CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), dt_dev, c->hp.dt, st, &n), "inviscid flux");
+      CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), dt_dev, c->hp.dt, c->tile_var, st, &n), "inviscid flux");
     }
     {
       PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
@@ -550,7 +626,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   }
   CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
   if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
-  CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, st, &n), "inviscid flux");
+  CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
   CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "Cn copy");
   // wu_reaction_subStep (:475-502)
   unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
@@ -565,7 +641,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
-    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, st, &n), "inviscid flux");
+    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;
     CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, st, &n), "boundary conditions");

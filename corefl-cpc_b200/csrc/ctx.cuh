@@ -36,6 +36,8 @@ struct cfk_ctx {
   // CUDA graph of one RK3 step
   cudaGraphExec_t graph_exec = nullptr;
   long long graph_kernels = 0;
+  // tile variant of each sweep of the WENO flux kernels (tile autotuner)
+  int tile_var[3] = {0, 0, 0};
   // phase timing with CUDA events (plain steps only)
   bool profiling = false;
   struct Rec { int phase; cudaEvent_t a, b; long long kernels; };

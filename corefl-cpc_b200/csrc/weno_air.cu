@@ -30,12 +30,22 @@ namespace {
 
 constexpr int kNQ = 13;  // staged values per point: Q0..4, G0..4, p, J/2, lambda
 
-template <int DIR, int ORD>
+// Tile shapes of a sweep: VAR selects one of the CFK_TILE_VARIANTS shapes
+// (nodes per column TN x columns C), chosen per direction by the tile
+// autotuner.  x tiles run along the lanes, y/z tiles put C consecutive i
+// columns on the lanes.
+template <int DIR, int VAR>
+struct TileShape {
+  static constexpr int TN = DIR == 0 ? (VAR == 0 ? 63 : VAR == 1 ? 127 : 31) : (VAR == 0 ? 15 : VAR == 1 ? 31 : 7);
+  static constexpr int C = DIR == 0 ? (VAR == 0 ? 4 : VAR == 1 ? 2 : 8) : (VAR == 0 ? 32 : VAR == 1 ? 16 : 32);
+};
+
+template <int DIR, int ORD, int VAR = 0>
 struct AirTile {
-  static constexpr int R = ORD == 7 ? 3 : 2;    // stencil reach left of the face node
-  static constexpr int NPF = 2 * R + 2;         // points per face
-  static constexpr int TN = DIR == 0 ? 63 : 15; // nodes per column
-  static constexpr int C = DIR == 0 ? 4 : 32;   // columns per CTA
+  static constexpr int R = ORD == 7 ? 3 : 2;          // stencil reach left of the face node
+  static constexpr int NPF = 2 * R + 2;               // points per face
+  static constexpr int TN = TileShape<DIR, VAR>::TN;  // nodes per column
+  static constexpr int C = TileShape<DIR, VAR>::C;    // columns per CTA
   static constexpr int NF = TN + 1;             // faces per column
   static constexpr int NPT = TN + 2 * R + 2;    // staged points per column
   static constexpr int NT = 256;                // threads
@@ -53,10 +63,11 @@ struct AirTile {
 }  // namespace
 
 // HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
-template <int DIR, int ORD, bool HYB>
+// VAR: tile shape (TileShape).
+template <int DIR, int ORD, bool HYB, int VAR>
 __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_ref, const double *sensor,
                                                               double threshold) {
-  using T = AirTile<DIR, ORD>;
+  using T = AirTile<DIR, ORD, VAR>;
   constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
   extern __shared__ double sm[];
   double *spts = sm;
@@ -234,28 +245,45 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
   }
 }
 
-template <int DIR, int ORD>
-static cudaError_t launch_dir(const Zone &z, double eps_ref, const double *sensor, double threshold,
+template <int DIR, int ORD, int VAR>
+static cudaError_t launch_var(const Zone &z, double eps_ref, const double *sensor, double threshold,
                               cudaStream_t st) {
-  using T = AirTile<DIR, ORD>;
+  using T = AirTile<DIR, ORD, VAR>;
   const Dims &d = z.d;
   dim3 grid;
   if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
   const size_t smem = T::smem_bytes();
-  if (sensor) weno_air_flux_diff<DIR, ORD, true><<<grid, T::NT, smem, st>>>(z, eps_ref, sensor, threshold);
-  else weno_air_flux_diff<DIR, ORD, false><<<grid, T::NT, smem, st>>>(z, eps_ref, nullptr, threshold);
+  if (sensor) weno_air_flux_diff<DIR, ORD, true, VAR><<<grid, T::NT, smem, st>>>(z, eps_ref, sensor, threshold);
+  else weno_air_flux_diff<DIR, ORD, false, VAR><<<grid, T::NT, smem, st>>>(z, eps_ref, nullptr, threshold);
   return cudaGetLastError();
 }
 
 template <int DIR, int ORD>
+static cudaError_t launch_dir(const Zone &z, double eps_ref, const double *sensor, double threshold, int var,
+                              cudaStream_t st) {
+  if (var == 1) return launch_var<DIR, ORD, 1>(z, eps_ref, sensor, threshold, st);
+  if (var == 2) return launch_var<DIR, ORD, 2>(z, eps_ref, sensor, threshold, st);
+  return launch_var<DIR, ORD, 0>(z, eps_ref, sensor, threshold, st);
+}
+
+template <int DIR, int ORD, int VAR>
 static cudaError_t set_smem_attr() {
-  const int b = (int)AirTile<DIR, ORD>::smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD, false>,
+  const int b = (int)AirTile<DIR, ORD, VAR>::smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD, false, VAR>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  return cudaFuncSetAttribute(weno_air_flux_diff<DIR, ORD, true, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              b);
+}
+
+template <int DIR, int ORD>
+static cudaError_t set_smem_attrs() {
+  cudaError_t e;
+  if ((e = set_smem_attr<DIR, ORD, 0>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<DIR, ORD, 1>()) != cudaSuccess) return e;
+  return set_smem_attr<DIR, ORD, 2>();
 }
 
 // Opt every instantiation in to its dynamic shared-memory size (> 48 KB for
@@ -263,29 +291,32 @@ static cudaError_t set_smem_attr() {
 // stream capture.
 cudaError_t weno_air_init_attributes() {
   cudaError_t e;
-  if ((e = set_smem_attr<0, 5>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<1, 5>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<2, 5>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<0, 7>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<1, 7>()) != cudaSuccess) return e;
-  return set_smem_attr<2, 7>();
+  if ((e = set_smem_attrs<0, 5>()) != cudaSuccess) return e;
+  if ((e = set_smem_attrs<1, 5>()) != cudaSuccess) return e;
+  if ((e = set_smem_attrs<2, 5>()) != cudaSuccess) return e;
+  if ((e = set_smem_attrs<0, 7>()) != cudaSuccess) return e;
+  if ((e = set_smem_attrs<1, 7>()) != cudaSuccess) return e;
+  return set_smem_attrs<2, 7>();
 }
 
-// Host launcher: x, y and (3-D) z sweeps in the reference's order.
-cudaError_t launch_weno_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch) {
+// One sweep (dir 0/1/2) with tile variant var.
+cudaError_t launch_weno_air_dir(const Zone &z, const Param &p, int dir, int var, cudaStream_t st) {
   const double eps_ref = kEpsWeno * p.weno_eps_scale;
   // hybrid UD5/UD7 + WENO when a sensor threshold is set (reference src/Parameter.cpp:236-252)
   const double th = p.sensor_threshold;
   const double *sn = th > 1e-10 ? z.shock_sensor : nullptr;
-  cudaError_t e;
   const bool w7 = p.inviscid_scheme == 72;
-  e = w7 ? launch_dir<0, 7>(z, eps_ref, sn, th, st) : launch_dir<0, 5>(z, eps_ref, sn, th, st);
-  if (e != cudaSuccess) return e;
-  e = w7 ? launch_dir<1, 7>(z, eps_ref, sn, th, st) : launch_dir<1, 5>(z, eps_ref, sn, th, st);
-  if (e != cudaSuccess) return e;
-  *n_launch += 2;
-  if (z.d.mz > 1) {
-    e = w7 ? launch_dir<2, 7>(z, eps_ref, sn, th, st) : launch_dir<2, 5>(z, eps_ref, sn, th, st);
+  if (dir == 0) return w7 ? launch_dir<0, 7>(z, eps_ref, sn, th, var, st) : launch_dir<0, 5>(z, eps_ref, sn, th, var, st);
+  if (dir == 1) return w7 ? launch_dir<1, 7>(z, eps_ref, sn, th, var, st) : launch_dir<1, 5>(z, eps_ref, sn, th, var, st);
+  return w7 ? launch_dir<2, 7>(z, eps_ref, sn, th, var, st) : launch_dir<2, 5>(z, eps_ref, sn, th, var, st);
+}
+
+// Host launcher: x, y and (3-D) z sweeps in the reference's order; var[d]
+// is the tile variant of sweep d.
+cudaError_t launch_weno_air(const Zone &z, const Param &p, const int *var, cudaStream_t st, int *n_launch) {
+  const int nd = z.d.mz > 1 ? 3 : 2;
+  for (int dir = 0; dir < nd; ++dir) {
+    cudaError_t e = launch_weno_air_dir(z, p, dir, var[dir], st);
     if (e != cudaSuccess) return e;
     *n_launch += 1;
   }

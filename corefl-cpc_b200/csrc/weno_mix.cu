@@ -31,12 +31,20 @@ struct MixVals {
   static constexpr int U = 10, P = 11, J = 12, LAM = 13, Y0 = 14, N = 14 + NS;
 };
 
-template <int DIR, int ORD, int NS>
+// Tile shapes of a sweep (nodes per column TN x columns C); VAR is chosen per
+// direction by the tile autotuner.
+template <int DIR, int VAR>
+struct MixShape {
+  static constexpr int TN = DIR == 0 ? (VAR == 0 ? 63 : VAR == 1 ? 127 : 31) : (VAR == 0 ? 15 : VAR == 1 ? 31 : 7);
+  static constexpr int C = DIR == 0 ? (VAR == 0 ? 4 : VAR == 1 ? 2 : 8) : (VAR == 0 ? 16 : VAR == 1 ? 8 : 16);
+};
+
+template <int DIR, int ORD, int NS, int VAR = 0>
 struct MixTile {
   static constexpr int R = ORD == 7 ? 3 : 2;
   static constexpr int NPF = 2 * R + 2;
-  static constexpr int TN = DIR == 0 ? 63 : 15;
-  static constexpr int C = DIR == 0 ? 4 : 16;
+  static constexpr int TN = MixShape<DIR, VAR>::TN;
+  static constexpr int C = MixShape<DIR, VAR>::C;
   static constexpr int NF = TN + 1;
   static constexpr int NPT = TN + 2 * R + 2;
   static constexpr int NT = 256;
@@ -60,10 +68,10 @@ struct MixTile {
 // branch is rare and must not add registers to the face loop.  s/sf point at
 // the staged values and face fluxes of this tile; the species face fluxes
 // are updated in shared memory.
-template <int ORD, int NS>
+template <int ORD, int NS, int VAR>
 __device__ __noinline__ void pp_limit_x(const double *s, double *sf, int c, int t, const Zone &z, int64_t idl,
                                         double dt, double alpha_dim, double rho_ref) {
-  using T = MixTile<0, ORD, NS>;
+  using T = MixTile<0, ORD, NS, VAR>;
   using V = MixVals<NS>;
   const int pc = t + T::R;
   const double jac_l = s[T::spt(V::J, c, pc)], jac_r = s[T::spt(V::J, c, pc + 1)];
@@ -122,10 +130,11 @@ struct PPArgs {
 }  // namespace
 
 // HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
-template <int DIR, int ORD, int NS, bool HYB>
+// VAR: tile shape (MixShape).
+template <int DIR, int ORD, int NS, bool HYB, int VAR>
 __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref, const __grid_constant__ Thermo thermo,
                                                           const double *sensor, double threshold, PPArgs pp) {
-  using T = MixTile<DIR, ORD, NS>;
+  using T = MixTile<DIR, ORD, NS, VAR>;
   using V = MixVals<NS>;
   constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
   const Thermo *th = &thermo;
@@ -345,7 +354,7 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
     if constexpr (DIR == 0) {
       if (pp.on) {
         const double dt = dt_pp > 0 ? dt_pp : z.dt_local[node_idx(0, c, f < 0 ? 0 : f)];
-        pp_limit_x<ORD, NS>(s, sflx, c, t, z, idf, dt, pp.alpha_dim, pp.rho_ref);
+        pp_limit_x<ORD, NS, VAR>(s, sflx, c, t, z, idf, dt, pp.alpha_dim, pp.rho_ref);
       }
     }
   }
@@ -365,63 +374,89 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
 
 namespace {
 
-template <int DIR, int ORD>
-cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, const double *sensor, double threshold,
+template <int DIR, int ORD, int VAR>
+cudaError_t launch_mix_var(const Zone &z, double eps_ref, const Thermo &th, const double *sensor, double threshold,
                            const PPArgs &pp, cudaStream_t st) {
-  using T = MixTile<DIR, ORD, kMaxSpec>;
+  using T = MixTile<DIR, ORD, kMaxSpec, VAR>;
   const Dims &d = z.d;
   dim3 grid;
   if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
   if (sensor)
-    weno_mix_flux_diff<DIR, ORD, kMaxSpec, true>
+    weno_mix_flux_diff<DIR, ORD, kMaxSpec, true, VAR>
         <<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, sensor, threshold, pp);
   else
-    weno_mix_flux_diff<DIR, ORD, kMaxSpec, false>
+    weno_mix_flux_diff<DIR, ORD, kMaxSpec, false, VAR>
         <<<grid, T::NT, T::smem_bytes(), st>>>(z, eps_ref, th, nullptr, threshold, pp);
   return cudaGetLastError();
 }
 
 template <int DIR, int ORD>
+cudaError_t launch_mix_dir(const Zone &z, double eps_ref, const Thermo &th, const double *sensor, double threshold,
+                           const PPArgs &pp, int var, cudaStream_t st) {
+  if (var == 1) return launch_mix_var<DIR, ORD, 1>(z, eps_ref, th, sensor, threshold, pp, st);
+  if (var == 2) return launch_mix_var<DIR, ORD, 2>(z, eps_ref, th, sensor, threshold, pp, st);
+  return launch_mix_var<DIR, ORD, 0>(z, eps_ref, th, sensor, threshold, pp, st);
+}
+
+template <int DIR, int ORD, int VAR>
 cudaError_t set_mix_attr() {
-  const int b = (int)MixTile<DIR, ORD, kMaxSpec>::smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec, false>,
+  const int b = (int)MixTile<DIR, ORD, kMaxSpec, VAR>::smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec, false, VAR>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec, true>,
+  return cudaFuncSetAttribute(weno_mix_flux_diff<DIR, ORD, kMaxSpec, true, VAR>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+
+template <int DIR, int ORD>
+cudaError_t set_mix_attrs() {
+  cudaError_t e;
+  if ((e = set_mix_attr<DIR, ORD, 0>()) != cudaSuccess) return e;
+  if ((e = set_mix_attr<DIR, ORD, 1>()) != cudaSuccess) return e;
+  return set_mix_attr<DIR, ORD, 2>();
 }
 
 }  // namespace
 
 cudaError_t weno_mix_init_attributes() {
   cudaError_t e;
-  if ((e = set_mix_attr<0, 5>()) != cudaSuccess) return e;
-  if ((e = set_mix_attr<1, 5>()) != cudaSuccess) return e;
-  if ((e = set_mix_attr<2, 5>()) != cudaSuccess) return e;
-  if ((e = set_mix_attr<0, 7>()) != cudaSuccess) return e;
-  if ((e = set_mix_attr<1, 7>()) != cudaSuccess) return e;
-  return set_mix_attr<2, 7>();
+  if ((e = set_mix_attrs<0, 5>()) != cudaSuccess) return e;
+  if ((e = set_mix_attrs<1, 5>()) != cudaSuccess) return e;
+  if ((e = set_mix_attrs<2, 5>()) != cudaSuccess) return e;
+  if ((e = set_mix_attrs<0, 7>()) != cudaSuccess) return e;
+  if ((e = set_mix_attrs<1, 7>()) != cudaSuccess) return e;
+  return set_mix_attrs<2, 7>();
 }
 
-// x, y and (3-D) z sweeps; the species count is fixed at 9 (kMaxSpec).
-// dt_dev / dt_host: the step's dt for the positive-preserving limiter.
-cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev, double dt_host,
-                            cudaStream_t st, int *n_launch) {
+// One sweep (dir 0/1/2) with tile variant var; the species count is fixed at
+// 9 (kMaxSpec).  dt_dev / dt_host: the step's dt for the positive-preserving
+// limiter (x sweep only, as in the reference).
+cudaError_t launch_weno_mix_dir(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev,
+                                double dt_host, int dir, int var, cudaStream_t st) {
   const double eps_ref = kEpsWeno * p.weno_eps_scale;
   const double tr = p.sensor_threshold;
   const double *sn = tr > 1e-10 ? z.shock_sensor : nullptr;  // hybrid UD + WENO
-  const PPArgs pp{p.positive_preserving ? 1 : 0, dt_dev, dt_host, p.dim == 3 ? 1.0 / 3.0 : 0.5, p.rho_ref};
-  const PPArgs off{0, nullptr, 0.0, 0.0, 0.0};
+  const PPArgs pp{p.positive_preserving && dir == 0 ? 1 : 0, dt_dev, dt_host, p.dim == 3 ? 1.0 / 3.0 : 0.5,
+                  p.rho_ref};
   const bool w7 = p.inviscid_scheme == 72;
-  cudaError_t e = w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, sn, tr, pp, st) : launch_mix_dir<0, 5>(z, eps_ref, th, sn, tr, pp, st);
-  if (e != cudaSuccess) return e;
-  e = w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, sn, tr, off, st) : launch_mix_dir<1, 5>(z, eps_ref, th, sn, tr, off, st);
-  if (e != cudaSuccess) return e;
-  *n_launch += 2;
-  if (z.d.mz > 1) {
-    e = w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, sn, tr, off, st) : launch_mix_dir<2, 5>(z, eps_ref, th, sn, tr, off, st);
+  if (dir == 0)
+    return w7 ? launch_mix_dir<0, 7>(z, eps_ref, th, sn, tr, pp, var, st)
+              : launch_mix_dir<0, 5>(z, eps_ref, th, sn, tr, pp, var, st);
+  if (dir == 1)
+    return w7 ? launch_mix_dir<1, 7>(z, eps_ref, th, sn, tr, pp, var, st)
+              : launch_mix_dir<1, 5>(z, eps_ref, th, sn, tr, pp, var, st);
+  return w7 ? launch_mix_dir<2, 7>(z, eps_ref, th, sn, tr, pp, var, st)
+            : launch_mix_dir<2, 5>(z, eps_ref, th, sn, tr, pp, var, st);
+}
+
+// x, y and (3-D) z sweeps; var[d] is the tile variant of sweep d.
+cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev, double dt_host,
+                            const int *var, cudaStream_t st, int *n_launch) {
+  const int nd = z.d.mz > 1 ? 3 : 2;
+  for (int dir = 0; dir < nd; ++dir) {
+    cudaError_t e = launch_weno_mix_dir(z, p, th, dt_dev, dt_host, dir, var[dir], st);
     if (e != cudaSuccess) return e;
     *n_launch += 1;
   }

@@ -143,6 +143,21 @@ int cfk_compute_inviscid_flux(cfk_ctx *ctx, void *stream);
  * cfk_wu_splitting_step call it themselves.  No-op unless
  * sensor_threshold > 1e-10. */
 int cfk_compute_shock_sensor(cfk_ctx *ctx, void *stream);
+
+/* ---- tile autotuner (no reference counterpart) ---- */
+/* The WENO flux kernels come in CFK_TILE_VARIANTS tile shapes per sweep
+ * (nodes per column x columns per CTA: x 63x4, 127x2, 31x8; y/z 15x32, 31x16,
+ * 7x32 for air and 15x16, 31x8, 7x16 for mixtures).  cfk_autotune_tiles
+ * times each variant of each sweep on the bound zone (reps launches after one
+ * warm-up, into scratch memory: the zone's arrays are not changed), keeps the
+ * fastest per direction for all later calls, and reports
+ * ms_out[dir * CFK_TILE_VARIANTS + var] (average ms per launch) and
+ * choice_out[3]; either may be NULL.  It allocates, so call it outside stream
+ * capture.  A no-op for the primitive-variable schemes (one tile shape). */
+#define CFK_TILE_VARIANTS 3
+int cfk_autotune_tiles(cfk_ctx *ctx, int reps, double *ms_out, int *choice_out, void *stream);
+/* Sets the tile variant of each sweep (var[3], each 0..CFK_TILE_VARIANTS-1). */
+int cfk_set_tile_variants(cfk_ctx *ctx, const int *var);
 /* SSP-RK3 stage update of cv and bv/sv.  Replaces update_cv_and_bv_rk<M>
  * (reference src/RK.cuh:224-281). */
 int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);

@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def _lockstep(case, n_steps, graph=False, tol=TOL, drift_tol=1e-10):
+def _lockstep(case, n_steps, graph=False, tol=TOL, drift_tol=1e-10, tiles=None):
     """Per-step parity: before every step the device state is reset to the
     oracle's, so each comparison covers exactly one RK3 step from identical
     inputs (tolerance `tol`).  A second, free-running pair checks that the
@@ -27,6 +27,8 @@ def _lockstep(case, n_steps, graph=False, tol=TOL, drift_tol=1e-10):
     oz.initialize()
     gz = GpuZone(case)
     gz.initialize()
+    if tiles is not None:
+        gz.ctx.set_tile_variants(tiles)
     worst = 0.0
     for s in range(n_steps):
         gz.load_from(oz)
@@ -44,6 +46,8 @@ def _lockstep(case, n_steps, graph=False, tol=TOL, drift_tol=1e-10):
     oz2.initialize()
     gz2 = GpuZone(case)
     gz2.initialize()
+    if tiles is not None:
+        gz2.ctx.set_tile_variants(tiles)
     for s in range(n_steps):
         oz2.step()
         gz2.ctx.rk3_step(graph=graph)
