@@ -322,7 +322,7 @@ def _mix_reference(rho, u, p, gamma_est=1.4):
 
 
 def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool = False, left=None, right=None,
-             length: float = 0.1) -> Case:
+             length: float = 0.1, reconstruction: int = 2) -> Case:
     """Shock tube of a mixture as an nx-by-ny 2-D block on x in [0, length],
     outflow on all faces, split at the middle.  States are dicts with
     rho [kg/m^3], p [Pa] and Y (mass fractions by species name).  Default:
@@ -358,7 +358,7 @@ def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool 
     Rm = R_U * (sv / m.mw[:, None]).sum(axis=0)
     bv[5] = bv[4] / (bv[0] * Rm)
     rho_ref, v_ref = _mix_reference(left["rho"], 0.0, left["p"])
-    param = _mix_param(m, dim=2, inviscid_scheme=scheme, cfl=0.5, weno_eps_scale=(rho_ref * v_ref) ** 2,
+    param = _mix_param(m, dim=2, inviscid_scheme=scheme, reconstruction=reconstruction, cfl=0.5, weno_eps_scale=(rho_ref * v_ref) ** 2,
                        v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac)
     faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
     return Case("mix_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m)
@@ -366,7 +366,7 @@ def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool 
 
 def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int | None = None,
              nz: int | None = None, length: float = 2e-3, reacting: bool = False, T0: float = 600.0,
-             dt: float | None = None) -> Case:
+             dt: float | None = None, reconstruction: int = 2) -> Case:
     """Curvilinear periodic 3-D block of a non-uniform H2/N2 - air mixture:
     x = xi + 0.05 sin(2 pi eta) sin(2 pi zeta) on [0, length]^3 (node-based
     periodicity), mixture fraction Z = 0.5 + 0.4 sin(2 pi x / length) between
@@ -400,7 +400,8 @@ def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int 
     bv[0] = bv[4] / (Rm * T)
     bv[1] = 50.0
     rho_ref, v_ref = _mix_reference(float(bv[0].mean()), 50.0, 101325.0)
-    param = _mix_param(m, dim=3, inviscid_scheme=scheme, viscous_order=2 if viscous else 0, cfl=0.5,
+    param = _mix_param(m, dim=3, inviscid_scheme=scheme, reconstruction=reconstruction,
+                       viscous_order=2 if viscous else 0, cfl=0.5,
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
                        fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
     faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]

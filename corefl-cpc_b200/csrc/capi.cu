@@ -13,6 +13,8 @@ cudaError_t launch_weno_air(const Zone &z, const Param &p, const int *var, cudaS
 cudaError_t launch_weno_air_dir(const Zone &z, const Param &p, int dir, int var, cudaStream_t st);
 cudaError_t weno_air_init_attributes();
 cudaError_t launch_pv_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t launch_pv_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
+cudaError_t pv_mix_init_attributes();
 cudaError_t pv_air_init_attributes();
 cudaError_t launch_weno_mix(const Zone &z, const Param &p, const Thermo &th, const double *dt_dev, double dt_host,
                             const int *var, cudaStream_t st, int *n_launch);
@@ -79,7 +81,7 @@ cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, con
                             const int *var, cudaStream_t st, int *n) {
   if (p.inviscid_scheme == 52 || p.inviscid_scheme == 72)
     return th ? launch_weno_mix(z, p, *th, dt_dev, dt_host, var, st, n) : launch_weno_air(z, p, var, st, n);
-  return launch_pv_air(z, p, st, n);
+  return th ? launch_pv_mix(z, p, *th, st, n) : launch_pv_air(z, p, st, n);
 }
 
 // compute_viscous_flux dispatch (reference src/ViscousScheme.cu:7-73).
@@ -116,8 +118,8 @@ int validate(const cfk_param *p, std::string &why) {
     why = "positive_preserving is supported with the WENO schemes (52, 72)";
     return -1;
   }
-  if (p->n_spec > 0 && s != 0 && !(s == 52 || s == 72)) {
-    why = "the mixture model is supported with WENO5/7 characteristic fluxes (52, 72) in this build";
+  if (p->n_spec > 0 && s == 1) {
+    why = "the Lax-Friedrichs flux has no mixture form (the reference leaves it unimplemented); use 2, 3 or 4";
     return -1;
   }
   if (p->n_spec > 0 && s != 0 && p->n_spec != kMaxSpec) {
@@ -178,6 +180,7 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   if (e != cudaSuccess) return CFK_ERR_CUDA;
   e = weno_air_init_attributes();
   if (e == cudaSuccess) e = pv_air_init_attributes();
+  if (e == cudaSuccess) e = pv_mix_init_attributes();
   if (e == cudaSuccess) e = weno_mix_init_attributes();
   if (e == cudaSuccess) e = viscous_mix_init_attributes();
   if (e != cudaSuccess) {

@@ -35,8 +35,8 @@ struct MixVals {
 // direction by the tile autotuner.
 template <int DIR, int VAR>
 struct MixShape {
-  static constexpr int TN = DIR == 0 ? (VAR == 0 ? 63 : VAR == 1 ? 127 : 31) : (VAR == 0 ? 15 : VAR == 1 ? 31 : 7);
-  static constexpr int C = DIR == 0 ? (VAR == 0 ? 4 : VAR == 1 ? 2 : 8) : (VAR == 0 ? 16 : VAR == 1 ? 8 : 16);
+  static constexpr int TN = DIR == 0 ? (VAR == 0 ? 63 : VAR == 1 ? 127 : 31) : (VAR == 0 ? 15 : VAR == 1 ? 31 : 63);
+  static constexpr int C = DIR == 0 ? (VAR == 0 ? 4 : VAR == 1 ? 2 : 8) : (VAR == 0 ? 16 : VAR == 1 ? 8 : 4);
 };
 
 template <int DIR, int ORD, int NS, int VAR = 0>

@@ -1,7 +1,10 @@
 /*
  * CPU oracle: primitive-variable reconstruction (first order, MUSCL, NND2
  * with the minmod limiter) and the Lax-Friedrichs, Roe (Harten entropy fix),
- * AUSM+ and HLLC Riemann solvers, calorically perfect air.
+ * AUSM+ and HLLC Riemann solvers, for calorically perfect air and for
+ * thermally perfect mixtures (species mass fractions reconstructed with the
+ * flow variables, side energies and gamma from NASA-7 thermo; the reference
+ * has no Lax-Friedrichs flux for mixtures).
  * TEST INFRASTRUCTURE ONLY (see oracle.h).
  *
  * Restates, in the reference's arithmetic order:
@@ -29,6 +32,9 @@
 #include <stdlib.h>
 
 #define GAMMA_AIR 1.4
+#define R_U 8314.462618
+/* reconstructed state: rho, u, v, w, p, Y_1..Y_ns, then E (slot nv) and gamma (slot nv + 1) */
+#define NRMAX (ORC_MAX_SPEC + 7)
 
 static inline long psz(const orc_zone *z, int g) {
   return (long)(z->mx + 2 * g) * (z->my + 2 * g) * (z->mz + 2 * g);
@@ -46,10 +52,12 @@ static inline long pstride(const orc_zone *z, int g, int dir) {
 static inline int sgn(double a) { return a < 0 ? -1 : 1; }
 static inline double minmod(double a, double b) { return 0.5 * (sgn(a) + sgn(b)) * fmin(fabs(a), fabs(b)); }
 
-/* pv[4][5]: rho,u,v,w,p at nodes i-1, i, i+1, i+2; out: left/right states at
- * i+1/2 with the total energy per volume in slot 5. */
-static void reconstruct_air(const double pv[4][5], int recon, double pl[6], double pr[6]) {
-  for (int l = 0; l < 5; ++l) {
+/* pv[4][*]: the nv primitive variables at nodes i-1, i, i+1, i+2; out: left
+ * and right states at i+1/2 with the total energy per volume in slot nv and,
+ * for mixtures, gamma in slot nv + 1 (src/InviscidScheme.cu:171-219). */
+static void reconstruct(const double pv[4][NRMAX], int nv, int recon, const orc_mech *mech, double *pl,
+                        double *pr) {
+  for (int l = 0; l < nv; ++l) {
     if (recon == 2) {
       const double kappa = 1.0 / 3.0;
       const double delta_i = pv[1][l] - pv[0][l];
@@ -72,14 +80,44 @@ static void reconstruct_air(const double pv[4][5], int recon, double pl[6], doub
       pr[l] = pv[2][l];
     }
   }
-  const double el = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
-  const double er = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
-  pl[5] = el * pl[0] + pl[4] / (GAMMA_AIR - 1);
-  pr[5] = er * pr[0] + pr[4] / (GAMMA_AIR - 1);
+  if (mech) {
+    const int ns = mech->n_spec;
+    double el = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+    double er = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+    double mw_inv_l = 0, mw_inv_r = 0;
+    for (int l = 0; l < ns; ++l) {
+      mw_inv_l += pl[5 + l] * mech->imw[l];
+      mw_inv_r += pr[5 + l] * mech->imw[l];
+    }
+    const double t_l = pl[4] / (pl[0] * R_U * mw_inv_l);
+    const double t_r = pr[4] / (pr[0] * R_U * mw_inv_r);
+    double hl[ORC_MAX_SPEC], hr[ORC_MAX_SPEC], cpl_i[ORC_MAX_SPEC], cpr_i[ORC_MAX_SPEC];
+    orc_enthalpy_and_cp(mech, t_l, hl, cpl_i);
+    orc_enthalpy_and_cp(mech, t_r, hr, cpr_i);
+    double cpl = 0, cpr = 0, cvl = 0, cvr = 0;
+    for (int l = 0; l < ns; ++l) {
+      cpl += cpl_i[l] * pl[l + 5];
+      cpr += cpr_i[l] * pr[l + 5];
+      cvl += pl[l + 5] * (cpl_i[l] - mech->gas_const[l]);
+      cvr += pr[l + 5] * (cpr_i[l] - mech->gas_const[l]);
+      el += hl[l] * pl[l + 5];
+      er += hr[l] * pr[l + 5];
+    }
+    pl[nv] = pl[0] * el - pl[4];
+    pr[nv] = pr[0] * er - pr[4];
+    pl[nv + 1] = cpl / cvl;
+    pr[nv + 1] = cpr / cvr;
+  } else {
+    const double el = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+    const double er = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+    pl[nv] = el * pl[0] + pl[4] / (GAMMA_AIR - 1);
+    pr[nv] = er * pr[0] + pr[4] / (GAMMA_AIR - 1);
+  }
 }
 
 /* m[2][3]: this direction's metric row at nodes i, i+1; jac[2]. */
-static void ausm_plus(const double *pl, const double *pr, const double m[2][3], const double jac[2], double *fc) {
+static void ausm_plus(const double *pl, const double *pr, int nv, const orc_mech *mech, const double m[2][3],
+                      const double jac[2], double *fc) {
   const double k1 = 0.5 * (jac[0] * m[0][0] + jac[1] * m[1][0]);
   const double k2 = 0.5 * (jac[0] * m[0][1] + jac[1] * m[1][1]);
   const double k3 = 0.5 * (jac[0] * m[0][2] + jac[1] * m[1][2]);
@@ -87,7 +125,7 @@ static void ausm_plus(const double *pl, const double *pr, const double m[2][3], 
   const double ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) / grad_k_div_jac;
   const double ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) / grad_k_div_jac;
   const double p_l = pl[4], p_r = pr[4], rho_l = pl[0], rho_r = pr[0];
-  const double gam_l = GAMMA_AIR, gam_r = GAMMA_AIR;
+  const double gam_l = mech ? pl[nv + 1] : GAMMA_AIR, gam_r = mech ? pr[nv + 1] : GAMMA_AIR;
   const double c = 0.5 * (sqrt(gam_l * p_l / rho_l) + sqrt(gam_r * p_r / rho_r));
   const double mach_l = ul / c, mach_r = ur / c;
   double mlp, mrn, plp, prn;
@@ -121,28 +159,49 @@ static void ausm_plus(const double *pl, const double *pr, const double m[2][3], 
   fc[1] = coeff * pv[1] + p_coeff * k1;
   fc[2] = coeff * pv[2] + p_coeff * k2;
   fc[3] = coeff * pv[3] + p_coeff * k3;
-  fc[4] = coeff * (pv[5] + pv[4]) / pv[0];
+  fc[4] = coeff * (pv[nv] + pv[4]) / pv[0];
+  for (int l = 5; l < nv; ++l) fc[l] = coeff * pv[l];
 }
 
-static void hllc(const double *pl, const double *pr, const double m[2][3], const double jac[2], double *fc) {
+static void hllc(const double *pl, const double *pr, int nv, const orc_mech *mech, const double m[2][3],
+                 const double jac[2], double *fc) {
   const double rl_c = sqrt(pl[0]) / (sqrt(pl[0]) + sqrt(pr[0]));
   const double rr_c = sqrt(pr[0]) / (sqrt(pl[0]) + sqrt(pr[0]));
   const double u_tilde = pl[1] * rl_c + pr[1] * rr_c;
   const double v_tilde = pl[2] * rl_c + pr[2] * rr_c;
   const double w_tilde = pl[3] * rl_c + pr[3] * rr_c;
-  const double gamma = GAMMA_AIR;
-  const double hl = (pl[5] + pl[4]) / pl[0];
-  const double hr = (pr[5] + pr[4]) / pr[0];
-  const double h_tilde = hl * rl_c + hr * rr_c;
-  const double ek_tilde = 0.5 * (u_tilde * u_tilde + v_tilde * v_tilde + w_tilde * w_tilde);
-  const double c_tilde = sqrt((gamma - 1) * (h_tilde - ek_tilde));
+  double gamma = GAMMA_AIR, c_tilde;
+  if (!mech) {
+    const double hl = (pl[nv] + pl[4]) / pl[0];
+    const double hr = (pr[nv] + pr[4]) / pr[0];
+    const double h_tilde = hl * rl_c + hr * rr_c;
+    const double ek_tilde = 0.5 * (u_tilde * u_tilde + v_tilde * v_tilde + w_tilde * w_tilde);
+    c_tilde = sqrt((gamma - 1) * (h_tilde - ek_tilde));
+  } else {
+    const int ns = mech->n_spec;
+    double svm[ORC_MAX_SPEC];
+    for (int l = 0; l < nv - 5; ++l) svm[l] = rl_c * pl[l + 5] + rr_c * pr[l + 5];
+    double mw_inv = 0;
+    for (int l = 0; l < ns; ++l) mw_inv += svm[l] * mech->imw[l];
+    const double tl = pl[4] / pl[0], tr = pr[4] / pr[0];
+    const double t = (rl_c * tl + rr_c * tr) / (R_U * mw_inv);
+    double cp_i[ORC_MAX_SPEC], h_i[ORC_MAX_SPEC];
+    orc_enthalpy_and_cp(mech, t, h_i, cp_i);
+    double cv = 0, cp = 0;
+    for (int l = 0; l < ns; ++l) {
+      cp += cp_i[l] * svm[l];
+      cv += svm[l] * (cp_i[l] - mech->gas_const[l]);
+    }
+    gamma = cp / cv;
+    c_tilde = sqrt(gamma * R_U * mw_inv * t);
+  }
   const double kx = 0.5 * (m[0][0] + m[1][0]);
   const double ky = 0.5 * (m[0][1] + m[1][1]);
   const double kz = 0.5 * (m[0][2] + m[1][2]);
   const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
   const double U_tilde_bar = (kx * u_tilde + ky * v_tilde + kz * w_tilde) / gradK;
   const double jac_ave = 0.5 * (jac[0] + jac[1]);
-  const double gamma_l = GAMMA_AIR, gamma_r = GAMMA_AIR;
+  const double gamma_l = mech ? pl[nv + 1] : GAMMA_AIR, gamma_r = mech ? pr[nv + 1] : GAMMA_AIR;
   const double Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];
   const double cl = sqrt(gamma_l * pl[4] / pl[0]);
   const double sl = fmin(Ul / gradK - cl, U_tilde_bar - c_tilde);
@@ -152,7 +211,8 @@ static void hllc(const double *pl, const double *pr, const double m[2][3], const
     fc[1] = jac_ave * (rhoUk * pl[1] + pl[4] * kx);
     fc[2] = jac_ave * (rhoUk * pl[2] + pl[4] * ky);
     fc[3] = jac_ave * (rhoUk * pl[3] + pl[4] * kz);
-    fc[4] = jac_ave * ((pl[5] + pl[4]) * Ul);
+    fc[4] = jac_ave * ((pl[nv] + pl[4]) * Ul);
+    for (int l = 5; l < nv; ++l) fc[l] = jac_ave * rhoUk * pl[l];
     return;
   }
   const double Ur = kx * pr[1] + ky * pr[2] + kz * pr[3];
@@ -164,7 +224,8 @@ static void hllc(const double *pl, const double *pr, const double m[2][3], const
     fc[1] = jac_ave * (rhoUk * pr[1] + pr[4] * kx);
     fc[2] = jac_ave * (rhoUk * pr[2] + pr[4] * ky);
     fc[3] = jac_ave * (rhoUk * pr[3] + pr[4] * kz);
-    fc[4] = jac_ave * ((pr[5] + pr[4]) * Ur);
+    fc[4] = jac_ave * ((pr[nv] + pr[4]) * Ur);
+    for (int l = 5; l < nv; ++l) fc[l] = jac_ave * rhoUk * pr[l];
     return;
   }
   const double sm = ((pr[0] * Ur * (sr - Ur / gradK) - pl[0] * Ul * (sl - Ul / gradK)) / gradK + pl[4] - pr[4]) /
@@ -178,7 +239,8 @@ static void hllc(const double *pl, const double *pr, const double m[2][3], const
     fc[1] = QlCoeff * pl[1] + dP * kx;
     fc[2] = QlCoeff * pl[2] + dP * ky;
     fc[3] = QlCoeff * pl[3] + dP * kz;
-    fc[4] = QlCoeff * pl[5] / pl[0] + pCoeff * jac_ave * (sl * pm * sm * gradK - sm * pl[4] * Ul);
+    fc[4] = QlCoeff * pl[nv] / pl[0] + pCoeff * jac_ave * (sl * pm * sm * gradK - sm * pl[4] * Ul);
+    for (int l = 5; l < nv; ++l) fc[l] = QlCoeff * pl[l];
   } else {
     const double pCoeff = 1.0 / (sr - sm);
     const double QrCoeff = jac_ave * pCoeff * sm * (sr * gradK - Ur) * pr[0];
@@ -187,10 +249,12 @@ static void hllc(const double *pl, const double *pr, const double m[2][3], const
     fc[1] = QrCoeff * pr[1] + dP * kx;
     fc[2] = QrCoeff * pr[2] + dP * ky;
     fc[3] = QrCoeff * pr[3] + dP * kz;
-    fc[4] = QrCoeff * pr[5] / pr[0] + pCoeff * jac_ave * (sr * pm * sm * gradK - sm * pr[4] * Ur);
+    fc[4] = QrCoeff * pr[nv] / pr[0] + pCoeff * jac_ave * (sr * pm * sm * gradK - sm * pr[4] * Ur);
+    for (int l = 5; l < nv; ++l) fc[l] = QrCoeff * pr[l];
   }
 }
 
+/* air only: the reference prints a message and leaves the flux zero for mixtures */
 static void lax_friedrichs(const double *pl, const double *pr, const double m[2][3], const double jac[2],
                            double *fc) {
   const double kx = 0.5 * (m[0][0] + m[1][0]);
@@ -215,7 +279,8 @@ static void lax_friedrichs(const double *pl, const double *pr, const double m[2]
   fc[4] = ((pl[5] + pl[4]) * Ukl + (pr[5] + pr[4]) * Ukr - spectral_radius * (pr[5] - pl[5])) * half_jac_ave;
 }
 
-/* Entropy-fix width at one node (compute_entropy_fix_delta). */
+/* Entropy-fix width at one node (compute_entropy_fix_delta); mixtures take
+ * the node's acoustic speed from the property array. */
 static double entropy_fix_delta(const orc_zone *z, const orc_param *p, long id) {
   const long sz = psz(z, z->ngg);
   const double *bv = z->bv, *mt = z->metric;
@@ -228,13 +293,13 @@ static double entropy_fix_delta(const orc_zone *z, const orc_param *p, long id) 
                          mt[id + 5 * sz] * mt[id + 5 * sz]);
   const double kz = sqrt(mt[id + 6 * sz] * mt[id + 6 * sz] + mt[id + 7 * sz] * mt[id + 7 * sz] +
                          mt[id + 8 * sz] * mt[id + 8 * sz]);
-  const double acoustic_speed = sqrt(GAMMA_AIR * bv[id + 4 * sz] / bv[id]);
+  const double acoustic_speed = p->mech ? z->acoustic_speed[id] : sqrt(GAMMA_AIR * bv[id + 4 * sz] / bv[id]);
   if (p->dim == 2) return p->entropy_fix_factor * (U + V + acoustic_speed * 0.5 * (kx + ky));
   return p->entropy_fix_factor * (U + V + W + acoustic_speed * (kx + ky + kz) / 3.0);
 }
 
-static void roe(const double *pl, const double *pr, const double m[2][3], const double jac[2], const double delta[2],
-                double *fc) {
+static void roe(const double *pl, const double *pr, int nv, const orc_mech *mech, const double m[2][3],
+                const double jac[2], const double delta[2], double *fc) {
   /* half sum of the left and right fluxes with the node metrics */
   double JacKx = jac[0] * m[0][0], JacKy = jac[0] * m[0][1], JacKz = jac[0] * m[0][2];
   double Uk = pl[1] * JacKx + pl[2] * JacKy + pl[3] * JacKz;
@@ -243,7 +308,8 @@ static void roe(const double *pl, const double *pr, const double m[2][3], const 
   fc[1] = 0.5 * (coeff * pl[1] + pl[4] * JacKx);
   fc[2] = 0.5 * (coeff * pl[2] + pl[4] * JacKy);
   fc[3] = 0.5 * (coeff * pl[3] + pl[4] * JacKz);
-  fc[4] = 0.5 * Uk * (pl[4] + pl[5]);
+  fc[4] = 0.5 * Uk * (pl[4] + pl[nv]);
+  for (int l = 5; l < nv; ++l) fc[l] = 0.5 * coeff * pl[l];
   JacKx = jac[1] * m[1][0];
   JacKy = jac[1] * m[1][1];
   JacKz = jac[1] * m[1][2];
@@ -253,7 +319,8 @@ static void roe(const double *pl, const double *pr, const double m[2][3], const 
   fc[1] += 0.5 * (coeff * pr[1] + pr[4] * JacKx);
   fc[2] += 0.5 * (coeff * pr[2] + pr[4] * JacKy);
   fc[3] += 0.5 * (coeff * pr[3] + pr[4] * JacKz);
-  fc[4] += 0.5 * Uk * (pr[4] + pr[5]);
+  fc[4] += 0.5 * Uk * (pr[4] + pr[nv]);
+  for (int l = 5; l < nv; ++l) fc[l] += 0.5 * coeff * pr[l];
 
   /* Roe averages */
   const double dl = sqrt(pl[0]), dr = sqrt(pr[0]);
@@ -262,11 +329,32 @@ static void roe(const double *pl, const double *pr, const double m[2][3], const 
   const double v = (dl * pl[2] + dr * pr[2]) * inv_denominator;
   const double w = (dl * pl[3] + dr * pr[3]) * inv_denominator;
   const double ek = 0.5 * (u * u + v * v + w * w);
-  const double hl = (pl[5] + pl[4]) / pl[0];
-  const double hr = (pr[5] + pr[4]) / pr[0];
+  const double hl = (pl[nv] + pl[4]) / pl[0];
+  const double hr = (pr[nv] + pr[4]) / pr[0];
   const double h = (dl * hl + dr * hr) * inv_denominator;
-  const double gamma = GAMMA_AIR;
-  const double c = sqrt((gamma - 1) * (h - ek));
+  double gamma = GAMMA_AIR;
+  double c = sqrt((gamma - 1) * (h - ek));
+  double mw = 28.9647;
+  double svm[ORC_MAX_SPEC] = {0};
+  for (int l = 0; l < nv - 5; ++l) svm[l] = (dl * pl[l + 5] + dr * pr[l + 5]) * inv_denominator;
+  double h_i[ORC_MAX_SPEC] = {0};
+  const int ns = mech ? mech->n_spec : 0;
+  if (mech) {
+    double mw_inv = 0;
+    for (int l = 0; l < ns; ++l) mw_inv += svm[l] * mech->imw[l];
+    const double tl = pl[4] / pl[0], tr = pr[4] / pr[0];
+    const double t = (dl * tl + dr * tr) * inv_denominator / (R_U * mw_inv);
+    double cp_i[ORC_MAX_SPEC];
+    orc_enthalpy_and_cp(mech, t, h_i, cp_i);
+    double cv = 0, cp = 0;
+    for (int l = 0; l < ns; ++l) {
+      cp += cp_i[l] * svm[l];
+      cv += svm[l] * (cp_i[l] - mech->gas_const[l]);
+    }
+    gamma = cp / cv;
+    c = sqrt(gamma * R_U * mw_inv * t);
+    mw = 1.0 / mw_inv;
+  }
 
   double kx = 0.5 * (m[0][0] + m[1][0]);
   double ky = 0.5 * (m[0][1] + m[1][1]);
@@ -286,69 +374,76 @@ static void roe(const double *pl, const double *pr, const double m[2][3], const 
   Ukk /= gradK;
 
   const double jac_ave = 0.5 * (jac[0] + jac[1]);
-  double dq[5];
+  double dq[NRMAX];
   dq[0] = jac_ave * (pr[0] - pl[0]);
-  for (int l = 1; l < 5; ++l) dq[l] = jac_ave * (pr[0] * pr[l] - pl[0] * pl[l]);
-  dq[4] = jac_ave * (pr[5] - pl[5]);
+  for (int l = 1; l < nv; ++l) dq[l] = jac_ave * (pr[0] * pr[l] - pl[0] * pl[l]);
+  dq[4] = jac_ave * (pr[nv] - pl[nv]);
 
   double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
   double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Ukk * dq[0]) / c;
+  for (int l = 0; l < ns; ++l) c1 += (mw * mech->imw[l] - h_i[l] * (gamma - 1) / (c * c)) * dq[l + 5];
   double c3 = dq[0] - c1;
-  double LDq[5];
+  double LDq[NRMAX];
   LDq[0] = 0.5 * (c1 - c2);
   LDq[1] = kx * c3 - ((kz * v - ky * w) * dq[0] - kz * dq[2] + ky * dq[3]) / c;
   LDq[2] = ky * c3 - ((kx * w - kz * u) * dq[0] - kx * dq[3] + kz * dq[1]) / c;
   LDq[3] = kz * c3 - ((ky * u - kx * v) * dq[0] - ky * dq[1] + kx * dq[2]) / c;
   LDq[4] = 0.5 * (c1 + c2);
+  for (int l = 0; l < nv - 5; ++l) LDq[l + 5] = dq[l + 5] - svm[l] * dq[0];
 
-  double b[5];
+  double b[NRMAX];
   b[0] = -characteristic[0] * LDq[0];
-  for (int l = 1; l < 5; ++l) b[l] = -characteristic[1] * LDq[l];
+  for (int l = 1; l < nv; ++l) b[l] = -characteristic[1] * LDq[l];
   b[4] = -characteristic[2] * LDq[4];
 
   const double c0 = kx * b[1] + ky * b[2] + kz * b[3];
   c1 = c0 + b[0] + b[4];
   c2 = c * (b[4] - b[0]);
   c3 = 0;
+  for (int l = 0; l < ns; ++l) c3 += (h_i[l] - mw * mech->imw[l] * c * c / (gamma - 1)) * b[l + 5];
   fc[0] += 0.5 * c1;
   fc[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
   fc[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
   fc[3] += 0.5 * (w * c1 + kz * c2 - c * (ky * b[1] - kx * b[2]));
   fc[4] += 0.5 * (h * c1 + Ukk * c2 - c * c * c0 / (gamma - 1) +
                   c * ((kz * v - ky * w) * b[1] + (kx * w - kz * u) * b[2] + (ky * u - kx * v) * b[3]) + c3);
+  for (int l = 0; l < nv - 5; ++l) fc[5 + l] += 0.5 * (b[l + 5] + svm[l] * c1);
 }
 
 static void pv_direction(orc_zone *z, const orc_param *p, int dir) {
-  const int ngg = z->ngg, mx = z->mx, my = z->my, mz = z->mz;
+  const int ngg = z->ngg, mx = z->mx, my = z->my, mz = z->mz, nv = p->n_var;
   const long sz = psz(z, ngg), s = pstride(z, ngg, dir);
   double *flux = dir == 0 ? z->fFlux : (dir == 1 ? z->gFlux : z->hFlux);
   const int mm = 3 * dir;
   const int i0 = dir == 0 ? -1 : 0, j0 = dir == 1 ? -1 : 0, k0 = dir == 2 ? -1 : 0;
   const int sch = p->inviscid_scheme;
+  const orc_mech *mech = p->mech;
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = k0; k < mz; ++k) {
     for (int j = j0; j < my; ++j) {
       for (int i = i0; i < mx; ++i) {
         const long id = pidx(z, ngg, i, j, k);
-        double pv[4][5], m[2][3], jac[2], pl[6], pr[6], fc[5];
-        for (int q = 0; q < 4; ++q)
+        double pv[4][NRMAX], m[2][3], jac[2], pl[NRMAX], pr[NRMAX], fc[NRMAX];
+        for (int q = 0; q < 4; ++q) {
           for (int l = 0; l < 5; ++l) pv[q][l] = z->bv[id + (q - 1) * s + l * sz];
+          for (int l = 5; l < nv; ++l) pv[q][l] = z->sv[id + (q - 1) * s + (l - 5) * sz];
+        }
         for (int q = 0; q < 2; ++q) {
           for (int l = 0; l < 3; ++l) m[q][l] = z->metric[id + q * s + (mm + l) * sz];
           jac[q] = z->jac[id + q * s];
         }
-        reconstruct_air(pv, p->reconstruction, pl, pr);
+        reconstruct(pv, nv, p->reconstruction, mech, pl, pr);
         if (sch == 2) {
           const double delta[2] = {entropy_fix_delta(z, p, id), entropy_fix_delta(z, p, id + s)};
-          roe(pl, pr, m, jac, delta, fc);
+          roe(pl, pr, nv, mech, m, jac, delta, fc);
         } else if (sch == 1) {
           lax_friedrichs(pl, pr, m, jac, fc);
         } else if (sch == 4) {
-          hllc(pl, pr, m, jac, fc);
+          hllc(pl, pr, nv, mech, m, jac, fc);
         } else {
-          ausm_plus(pl, pr, m, jac, fc);
+          ausm_plus(pl, pr, nv, mech, m, jac, fc);
         }
-        for (int l = 0; l < 5; ++l) flux[id + l * sz] = fc[l];
+        for (int l = 0; l < nv; ++l) flux[id + l * sz] = fc[l];
       }
     }
   }
@@ -359,15 +454,15 @@ static void pv_direction(orc_zone *z, const orc_param *p, int dir) {
       for (int i = 0; i < mx; ++i) {
         const long iq = pidx(z, 0, i, j, k);
         const long ic = pidx(z, ngg, i, j, k), im = ic - s;
-        for (int l = 0; l < 5; ++l) z->dq[iq + l * szq] -= flux[ic + l * sz] - flux[im + l * sz];
+        for (int l = 0; l < nv; ++l) z->dq[iq + l * szq] -= flux[ic + l * sz] - flux[im + l * sz];
       }
     }
   }
 }
 
 void orc_roe_like_inviscid(orc_zone *z, const orc_param *p) {
-  if (p->mech) {
-    fprintf(stderr, "oracle: primitive-variable Riemann-solver schemes are restated for air only\n");
+  if (p->mech && p->inviscid_scheme == 1) {
+    fprintf(stderr, "oracle: the reference has no Lax-Friedrichs flux for mixtures\n");
     abort();
   }
   pv_direction(z, p, 0);

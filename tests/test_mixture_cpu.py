@@ -5,6 +5,7 @@ so the exact solution of the gamma-law Riemann problem applies."""
 import math
 
 import numpy as np
+import pytest
 
 import cases
 import mechanism
@@ -118,3 +119,49 @@ def test_oracle_argon_tube_against_exact_solution():
     # the species stay pure argon and gamma is 5/3 everywhere
     assert np.allclose(c.interior(z["sv"][k])[0], 1.0, atol=1e-12)
     assert np.allclose(c.interior(z["gamma"])[0], 5.0 / 3.0, rtol=1e-12)
+
+
+@pytest.mark.parametrize("scheme", [2, 3, 4])
+def test_oracle_pv_schemes_argon_tube_against_exact_solution(scheme):
+    """Roe, AUSM+ and HLLC in their mixture form (reference
+    src/InviscidScheme.cu:171-765, mixture branches) on the argon tube: the
+    side energies and gamma from NASA-7 thermo reproduce the exact
+    gamma = 5/3 Riemann solution."""
+    mech = mechanism.load("premix_h2_ar")
+    left = dict(rho=1.0, p=1.0e5, Y={"AR": 1.0})
+    right = dict(rho=0.125, p=1.0e4, Y={"AR": 1.0})
+    c = cases.mix_tube(mech, 400, 7, scheme=scheme, left=left, right=right, length=1.0, reconstruction=2)
+    z = pyoracle.OracleZone(c)
+    z.initialize()
+    t, t_end = 0.0, 5e-4
+    while t < t_end - 1e-12:
+        t += z.step()
+    xs = np.linspace(0.0, 1.0, 400)
+    ex = exact_riemann(5.0 / 3.0, (1.0, 0.0, 1.0e5), (0.125, 0.0, 1.0e4), xs, 0.5, t)
+    bv = z["bv"]
+    scale = (1.0, math.sqrt(5.0 / 3.0 * 1.0e5), 1.0e5)
+    for n, slot in enumerate((0, 1, 4)):
+        got = c.interior(bv[slot])[0, 3]
+        err = np.abs(got - ex[n]).mean() / scale[n]
+        assert err < 6e-3, (slot, err)
+
+
+@pytest.mark.parametrize("scheme", [2, 3, 4])
+def test_oracle_pv_species_fluxes_sum_to_mass_flux(scheme):
+    """With first-order reconstruction the face mass fractions sum to one, so
+    the species fluxes of every scheme sum to the mass flux (for Roe the
+    species waves cancel: sum_k (d(rho Y_k) - Y~_k d rho) = 0)."""
+    mech = mechanism.load("li2004")
+    c = cases.perturbed(cases.mix_wave(mech, 11, ny=9, nz=7, scheme=scheme, viscous=False, reconstruction=1),
+                        seed=3, amp=2e-2)
+    z = pyoracle.OracleZone(c)
+    z.initialize()
+    z.call("orc_compute_inviscid_flux")
+    ns = mech.n_spec
+    for key in ("fFlux", "gFlux", "hFlux"):
+        f = z[key]
+        mass = f[0]
+        spec = f[5:5 + ns].sum(axis=0)
+        nz_ = np.abs(mass) > 0
+        assert nz_.any()
+        assert np.abs(spec[nz_] - mass[nz_]).max() <= 1e-11 * np.abs(mass).max(), key
