@@ -129,13 +129,15 @@ def _air_param(**kw) -> dict:
     return p
 
 
-def ghost_layers(scheme: int) -> int:
-    """Ghost layers of an inviscid scheme (reference src/Parameter.cpp:196-252)."""
+def ghost_layers(scheme: int, viscous_order: int = 0) -> int:
+    """Ghost layers of an inviscid scheme (reference src/Parameter.cpp:196-252),
+    at least 4 with the 8th-order viscous scheme (:296-300)."""
+    g = 2
     if scheme in (71, 72):
-        return 4
-    if scheme in (51, 52):
-        return 3
-    return 2
+        g = 4
+    elif scheme in (51, 52):
+        g = 3
+    return max(g, 4) if viscous_order == 8 else g
 
 
 def _reference_scale(rho: float, u: float, p: float) -> tuple[float, float]:
@@ -147,14 +149,16 @@ def _reference_scale(rho: float, u: float, p: float) -> tuple[float, float]:
     return rho, v
 
 
-def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5, reconstruction: int = 2) -> Case:
+def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5, reconstruction: int = 2,
+        viscous_order: int = 0) -> Case:
     """Sod shock tube on x in [0,1] as an nx-by-ny 2-D block (the reference
     runs 1-D problems with 7 nodes in y), outflow on all four faces,
     left (1,0,1) / right (0.125,0,0.1) split at x = 0.5 (the right state is
     applied to x in [0.5, 1.5] inclusive, reference src/Field.cu:290).
     scheme: 52/72 WENO5/7 characteristic, 1 LF, 2 Roe, 3 AUSM+, 4 HLLC with
-    `reconstruction` 1 first order, 2 MUSCL, 3 NND2."""
-    ngg = ghost_layers(scheme)
+    `reconstruction` 1 first order, 2 MUSCL, 3 NND2; viscous_order 2 or 8
+    adds the viscous flux (Sutherland viscosity)."""
+    ngg = ghost_layers(scheme, viscous_order)
     xs = np.linspace(0.0, 1.0, nx)
     ys = np.arange(ny) * 0.01
     x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
@@ -171,14 +175,15 @@ def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5, reconstr
     bv[5] = p * MW_AIR / (rho * R_U)
     rho_ref, v_ref = _reference_scale(1.0, 0.0, 1.0)
     param = _air_param(dim=2, inviscid_scheme=scheme, reconstruction=reconstruction, cfl=cfl,
-                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref)
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref,
+                       viscous_order=viscous_order)
     faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
     return Case("sod", nx, ny, 1, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg)
 
 
 def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float = 0.05, reynolds: float = 1000.0,
               dt: float | None = None, cfl: float = 0.5, ny: int | None = None, nz: int | None = None,
-              reconstruction: int = 2) -> Case:
+              reconstruction: int = 2, viscous_order: int = 2) -> Case:
     """3-D viscous single-species wave on a curvilinear periodic block:
     x = xi + amp*sin(2 pi eta) sin(2 pi zeta), y = eta, z = zeta on [0,1]^3
     with n nodes per direction (node-based periodicity: node 0 and node n-1
@@ -188,7 +193,8 @@ def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float =
     to give rho U L / mu = Re.  dt: fixed step; None means CFL-controlled."""
     ny = n if ny is None else ny
     nz = n if nz is None else nz
-    ngg = ghost_layers(scheme)
+    vo = viscous_order if viscous else 0
+    ngg = ghost_layers(scheme, vo)
     p0 = 1.0 / GAMMA_AIR
     T0 = p0 * MW_AIR / (1.0 * R_U)
     mu0 = 1.7894e-5 * (T0 / 288.16) ** 1.5 * (288.16 + 110) / (T0 + 110)
@@ -210,7 +216,7 @@ def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float =
     bv[5] = p0 * MW_AIR / (bv[0] * R_U)
     rho_ref, v_ref = _reference_scale(1.0, 1.0, p0)
     param = _air_param(dim=3, inviscid_scheme=scheme, reconstruction=reconstruction,
-                       viscous_order=2 if viscous else 0, cfl=cfl,
+                       viscous_order=vo, cfl=cfl,
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref,
                        fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
     faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]
@@ -322,7 +328,7 @@ def _mix_reference(rho, u, p, gamma_est=1.4):
 
 
 def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool = False, left=None, right=None,
-             length: float = 0.1, reconstruction: int = 2) -> Case:
+             length: float = 0.1, reconstruction: int = 2, viscous_order: int = 0) -> Case:
     """Shock tube of a mixture as an nx-by-ny 2-D block on x in [0, length],
     outflow on all faces, split at the middle.  States are dicts with
     rho [kg/m^3], p [Pa] and Y (mass fractions by species name).  Default:
@@ -336,7 +342,7 @@ def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool 
         left = dict(rho=0.18075, p=35594.0, Y={"H2": 0.012772428, "O2": 0.101362139, "AR": 0.885865433})
     if right is None:
         right = dict(rho=0.072, p=7173.0, Y={"O2": 0.2, "AR": 0.8})
-    ngg = ghost_layers(scheme)
+    ngg = ghost_layers(scheme, viscous_order)
     xs = np.linspace(0.0, length, nx)
     ys = np.arange(ny) * length / 100.0
     x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
@@ -358,15 +364,16 @@ def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool 
     Rm = R_U * (sv / m.mw[:, None]).sum(axis=0)
     bv[5] = bv[4] / (bv[0] * Rm)
     rho_ref, v_ref = _mix_reference(left["rho"], 0.0, left["p"])
-    param = _mix_param(m, dim=2, inviscid_scheme=scheme, reconstruction=reconstruction, cfl=0.5, weno_eps_scale=(rho_ref * v_ref) ** 2,
-                       v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac)
+    param = _mix_param(m, dim=2, inviscid_scheme=scheme, reconstruction=reconstruction, cfl=0.5,
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
+                       viscous_order=viscous_order)
     faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
     return Case("mix_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m)
 
 
 def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int | None = None,
              nz: int | None = None, length: float = 2e-3, reacting: bool = False, T0: float = 600.0,
-             dt: float | None = None, reconstruction: int = 2) -> Case:
+             dt: float | None = None, reconstruction: int = 2, viscous_order: int = 2) -> Case:
     """Curvilinear periodic 3-D block of a non-uniform H2/N2 - air mixture:
     x = xi + 0.05 sin(2 pi eta) sin(2 pi zeta) on [0, length]^3 (node-based
     periodicity), mixture fraction Z = 0.5 + 0.4 sin(2 pi x / length) between
@@ -376,7 +383,8 @@ def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int 
     m = mech if reacting else without_reactions(mech)
     ny = n if ny is None else ny
     nz = n if nz is None else nz
-    ngg = ghost_layers(scheme)
+    vo = viscous_order if viscous else 0
+    ngg = ghost_layers(scheme, vo)
     xi, eta, zeta = np.linspace(0, 1, n), np.linspace(0, 1, ny), np.linspace(0, 1, nz)
     Z3, Y3, X3 = np.meshgrid(zeta, eta, xi, indexing="ij")
     x = (X3 + 0.05 * np.sin(2 * np.pi * Y3) * np.sin(2 * np.pi * Z3)) * length
@@ -401,7 +409,7 @@ def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int 
     bv[1] = 50.0
     rho_ref, v_ref = _mix_reference(float(bv[0].mean()), 50.0, 101325.0)
     param = _mix_param(m, dim=3, inviscid_scheme=scheme, reconstruction=reconstruction,
-                       viscous_order=2 if viscous else 0, cfl=0.5,
+                       viscous_order=vo, cfl=0.5,
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
                        fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
     faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]

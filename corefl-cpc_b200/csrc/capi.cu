@@ -34,6 +34,8 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
                                        int n_face, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
 cudaError_t launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t st);
+cudaError_t launch_viscous8(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces, int n_face,
+                            double *fvis, cudaStream_t st, int *n_launch);
 cudaError_t launch_wu_reaction(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
                                int schedule, int *nsub_out, int *err, unsigned int *counter, int n_sm,
                                cudaStream_t st);
@@ -68,10 +70,12 @@ namespace {
 // Ghost layers the inviscid scheme reads (reference src/Parameter.cpp:196-252):
 // 4 for WENO7, 3 for WENO5, 2 for the primitive-variable schemes; none for
 // chemistry-only contexts.
-int ghost_layers(int scheme) {
-  if (scheme == 71 || scheme == 72) return 4;
-  if (scheme == 51 || scheme == 52) return 3;
-  return scheme == 0 ? 0 : 2;
+int ghost_layers(int scheme, int viscous_order) {
+  int g = scheme == 0 ? 0 : 2;
+  if (scheme == 71 || scheme == 72) g = 4;
+  if (scheme == 51 || scheme == 52) g = 3;
+  if (viscous_order == 8 && g < 4) g = 4;  // 8th-order viscous stencil (reference src/Parameter.cpp:298-300)
+  return g;
 }
 
 // compute_inviscid_flux dispatch (reference src/InviscidScheme.cu:12-26);
@@ -84,8 +88,11 @@ cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, con
   return th ? launch_pv_mix(z, p, *th, st, n) : launch_pv_air(z, p, st, n);
 }
 
-// compute_viscous_flux dispatch (reference src/ViscousScheme.cu:7-73).
-cudaError_t launch_viscous(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, int *n) {
+// compute_viscous_flux dispatch (reference src/ViscousScheme.cu:7-73): the
+// 2nd-order face scheme or the 8th-order collocated one.
+cudaError_t launch_viscous(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces, int n_face,
+                           cudaStream_t st, int *n) {
+  if (p.viscous_order == 8) return launch_viscous8(z, p, th, faces, n_face, z.fvis8, st, n);
   return th ? launch_viscous_mix(z, p, *th, st, n) : launch_viscous_air(z, p, st, n);
 }
 
@@ -105,7 +112,10 @@ int validate(const cfk_param *p, std::string &why) {
   }
   if (s >= 1 && s <= 4 && !(p->limiter == 0 || p->limiter == 1)) { why = "limiter must be 0 or 1"; return -1; }
   if (s == 2 && !(p->entropy_fix_factor >= 0)) { why = "entropy_fix_factor must be >= 0"; return -1; }
-  if (p->viscous_order != 0 && p->viscous_order != 2) { why = "viscous_order must be 0 or 2"; return -1; }
+  if (p->viscous_order != 0 && p->viscous_order != 2 && p->viscous_order != 8) {
+    why = "viscous_order must be 0, 2 or 8";
+    return -1;
+  }
   if (p->sensor_threshold > 1e-10 && !(s == 52 || s == 72)) {
     why = "shockSensor_threshold > 0 (hybrid scheme) needs inviscid_scheme 52 or 72";
     return -1;
@@ -130,7 +140,7 @@ int validate(const cfk_param *p, std::string &why) {
     why = "passive scalars beside the species are not supported (n_scalar must equal n_spec)";
     return -1;
   }
-  if (p->n_spec > 0 && p->viscous_order == 2 && p->gradPInDiffusionFlux) {
+  if (p->n_spec > 0 && p->viscous_order > 0 && p->gradPInDiffusionFlux) {
     why = "gradPInDiffusionFlux is not supported";
     return -1;
   }
@@ -220,6 +230,7 @@ int cfk_destroy(cfk_ctx *c) {
   for (auto e : c->pool) cudaEventDestroy(e);
   for (void *ptr : c->owned) cudaFree(ptr);
   if (c->own_sensor) cudaFree(c->own_sensor);
+  if (c->own_fvis8) cudaFree(c->own_fvis8);
   cudaFree(c->d_dt_bits);
   cudaFree(c->d_mech);
   delete c;
@@ -231,8 +242,8 @@ const char *cfk_last_error(const cfk_ctx *c) { return c ? c->err.c_str() : "null
 int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   if (!c || !zn) return CFK_ERR_ARG;
   if (zn->mx < 1 || zn->my < 1 || zn->mz < 1) return fail(c, CFK_ERR_ARG, "zone extents must be positive");
-  const int need_g = ghost_layers(c->hp.inviscid_scheme);
-  if (zn->ngg < need_g) return fail(c, CFK_ERR_ARG, "ngg too small for the inviscid scheme");
+  const int need_g = ghost_layers(c->hp.inviscid_scheme, c->hp.viscous_order);
+  if (zn->ngg < need_g) return fail(c, CFK_ERR_ARG, "ngg too small for the inviscid or viscous scheme");
   if ((c->hp.dim == 2) != (zn->mz == 1)) return fail(c, CFK_ERR_ARG, "dim does not match mz");
   if (c->hp.inviscid_scheme != 0 && (!zn->cv || !zn->bv || !zn->qn || !zn->dq || !zn->metric || !zn->jac))
     return fail(c, CFK_ERR_ARG, "cv, bv, qn, dq, metric and jac are required");
@@ -256,12 +267,27 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   z.thermal_conductivity = zn->thermal_conductivity; z.rho_D = zn->rho_D;
   z.reaction_timeScale = zn->reaction_timeScale; z.dq = zn->dq; z.dt_local = zn->dt_local; z.Cn = zn->Cn;
   z.shock_sensor = zn->shock_sensor;
+  z.fvis8 = nullptr;
+  if (c->hp.viscous_order == 8) {
+    // node fluxes of the 8th-order viscous scheme, owned by the context
+    const size_t n8 = (size_t)z.d.plane(z.d.ngg) * 3 * (c->hp.n_var - 1);
+    if (c->own_fvis8_n < n8) {
+      if (c->own_fvis8) cudaFree(c->own_fvis8);
+      c->own_fvis8 = nullptr;
+      c->own_fvis8_n = 0;
+      CFK_CHECK(c, cudaMalloc(&c->own_fvis8, n8 * sizeof(double)), "8th-order viscous flux allocation");
+      c->own_fvis8_n = n8;
+    }
+    CFK_CHECK(c, cudaMemset(c->own_fvis8, 0, n8 * sizeof(double)), "8th-order viscous flux reset");
+    z.fvis8 = c->own_fvis8;
+  }
   if (c->p.sensor_threshold > 1e-10 && !z.shock_sensor) {
     // the hybrid scheme needs a sensor array whose ghost layers are zero
     // (reference src/Field.cu:526, allocated with cudaMemset 0)
     const size_t P = (size_t)z.d.plane(z.d.ngg);
     if (c->own_sensor_n < P) {
       if (c->own_sensor) cudaFree(c->own_sensor);
+  if (c->own_fvis8) cudaFree(c->own_fvis8);
       c->own_sensor = nullptr;
       c->own_sensor_n = 0;
       CFK_CHECK(c, cudaMalloc(&c->own_sensor, P * sizeof(double)), "shock sensor allocation");
@@ -278,7 +304,7 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
 int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
   if (!c || !out) return CFK_ERR_ARG;
   CFK_CHECK(c, cudaSetDevice(c->hp.device), "cudaSetDevice");
-  const int g = ghost_layers(c->hp.inviscid_scheme);
+  const int g = ghost_layers(c->hp.inviscid_scheme, c->hp.viscous_order);
   cfk_zone zn{};
   zn.mx = mx; zn.my = my; zn.mz = mz; zn.ngg = g;
   const size_t P = (size_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g), N = (size_t)mx * my * mz;
@@ -405,7 +431,8 @@ int cfk_compute_viscous_flux(cfk_ctx *c, void *stream) {
   if (c->hp.viscous_order == 0) return CFK_OK;
   if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
-  CFK_CHECK(c, launch_viscous(c->z, c->p, thermo_host(c), S(stream), &n), "viscous flux");
+  CFK_CHECK(c, launch_viscous(c->z, c->p, thermo_host(c), c->hp.faces, c->hp.n_face, S(stream), &n),
+            "viscous flux");
   c->launches += n;
   return CFK_OK;
 }
@@ -568,9 +595,9 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
   }
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
-    if (p.viscous_order == 2) {
+    if (p.viscous_order > 0) {
       PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
-      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
+      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
     }
     if (c->have_mech && p.n_reac > 0) {
       // explicit chemical source of a reacting mixture (reference src/RK.cuh:147-149)
@@ -628,7 +655,8 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
     ++n;
   }
   CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
-  if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
+  if (p.viscous_order > 0)
+    CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
   CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
   CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "Cn copy");
   // wu_reaction_subStep (:475-502)
@@ -643,7 +671,8 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   CFK_CHECK(c, cudaMemcpyAsync(z.qn, z.cv, P * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "qn copy");
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
-    if (p.viscous_order == 2) CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), st, &n), "viscous flux");
+    if (p.viscous_order > 0)
+    CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
     CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;

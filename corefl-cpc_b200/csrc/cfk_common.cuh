@@ -43,6 +43,7 @@ struct Zone {
   double *acoustic_speed, *gamma, *thermal_conductivity, *rho_D, *reaction_timeScale;
   double *dq, *dt_local, *Cn;
   double *shock_sensor;  // ngg ghosts, zero outside the interior; hybrid WENO only
+  double *fvis8;         // node viscous fluxes of the 8th-order scheme, 3 x (n_var - 1) planes, ngg ghosts
 };
 
 // Kernel-side scalar settings.

@@ -24,6 +24,8 @@ struct cfk_ctx {
   std::vector<void *> owned;  // device arrays owned by the context
   double *own_sensor = nullptr;  // context-allocated shock sensor (zone without one)
   size_t own_sensor_n = 0;
+  double *own_fvis8 = nullptr;   // node viscous fluxes of the 8th-order scheme
+  size_t own_fvis8_n = 0;
   Mech *d_mech = nullptr;
   Mech h_mech{};  // host copy, passed by value to the kernels that read it from the constant bank
   bool have_mech = false;

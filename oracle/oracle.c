@@ -541,7 +541,13 @@ static void viscous_direction(orc_zone *z, const orc_param *p, int dir) {
   }
 }
 
+void orc_viscous_flux_8th(orc_zone *z, const orc_param *p);
+
 void orc_compute_viscous_flux(orc_zone *z, const orc_param *p) {
+  if (p->viscous_order == 8) {
+    orc_viscous_flux_8th(z, p);
+    return;
+  }
   if (p->viscous_order != 2) return;
   viscous_direction(z, p, 0);
   viscous_direction(z, p, 1);
