@@ -24,6 +24,7 @@ cudaError_t weno_mix_init_attributes();
 cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
 cudaError_t viscous_mix_init_attributes();
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t viscous_air_init_attributes();
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
                              int rk, int *err, cudaStream_t st, bool minus_cn = false);
 cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
@@ -191,6 +192,7 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   e = weno_air_init_attributes();
   if (e == cudaSuccess) e = pv_air_init_attributes();
   if (e == cudaSuccess) e = pv_mix_init_attributes();
+  if (e == cudaSuccess) e = viscous_air_init_attributes();
   if (e == cudaSuccess) e = weno_mix_init_attributes();
   if (e == cudaSuccess) e = viscous_mix_init_attributes();
   if (e != cudaSuccess) {

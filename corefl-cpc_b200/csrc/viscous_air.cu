@@ -10,23 +10,43 @@
 namespace cfk {
 
 namespace {
+// Tile: TN nodes along the sweep x C columns; faces n0-1 .. n0+TN-1 need the
+// TN + 2 nodes n0-1 .. n0+TN, whose per-node values are staged once.
 template <int DIR>
 struct VisTile {
   static constexpr int TN = DIR == 0 ? 63 : 15;
-  static constexpr int C = DIR == 0 ? 4 : 32;
+  static constexpr int C = DIR == 0 ? 4 : 16;
   static constexpr int NF = TN + 1;
+  static constexpr int NP = TN + 2;  // staged nodes per column
   static constexpr int NT = 256;
+  // per node: u v w T (4), transverse differences f(+1)-f(-1) of u v w T along
+  // the two other directions (8), metric (9), metric row of DIR times J (3), mu
+  static constexpr int NQ = 25;
+  static constexpr int QV = 0, QD = 4, QM = 12, QK = 21, QMU = 24;
+  __device__ static int spt(int q, int c, int t) {
+    return DIR == 0 ? (q * C + c) * NP + t : (q * NP + t) * C + c;
+  }
   __device__ static int sfl(int v, int c, int t) {
     return DIR == 0 ? (v * C + c) * NF + t : (v * NF + t) * C + c;
   }
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(NQ * C * NP + 4 * C * NF); }
 };
 }  // namespace
 
+// Three phases, as in the WENO kernels: stage the per-node values of the
+// tile (each node's bv, transverse differences, metrics and mu are loaded
+// once instead of once per adjacent face), compute the face fluxes into
+// shared memory, difference them into dq.  The face arithmetic is the
+// reference's except that its transverse derivative
+// 0.25 * (f(A+) - f(A-) + f(B+) - f(B-)) is summed as
+// 0.25 * ((f(A+) - f(A-)) + (f(B+) - f(B-))) from the staged node differences.
 template <int DIR>
-__global__ void __launch_bounds__(256) viscous_air_flux_diff(Zone z, double Pr) {
+__global__ void __launch_bounds__(256, 3) viscous_air_flux_diff(Zone z, double Pr) {
   using T = VisTile<DIR>;
-  constexpr int TN = T::TN, C = T::C, NF = T::NF;
-  __shared__ double sflx[4 * C * NF];
+  constexpr int TN = T::TN, C = T::C, NF = T::NF, NP = T::NP;
+  extern __shared__ double sm[];
+  double *spts = sm;
+  double *sflx = sm + T::NQ * C * NP;
   const Dims d = z.d;
   const int g = d.ngg;
   const int64_t sz = d.plane(g), szq = d.plane(0);
@@ -45,30 +65,53 @@ __global__ void __launch_bounds__(256) viscous_air_flux_diff(Zone z, double Pr) 
     if (DIR == 0) { c = item / n_t; t = item - c * n_t; }
     else { t = item / C; c = item - t * C; }
   };
-  const int64_t sd = d.stride(g, DIR);
-  constexpr int DA = (DIR + 1) % 3, DB = (DIR + 2) % 3;
-  const int64_t sa = d.stride(g, DA), sb = d.stride(g, DB);
+  // the two transverse directions, lower-numbered first
+  constexpr int TLO = DIR == 0 ? 1 : 0, THI = DIR == 2 ? 1 : 2;
+  const int64_t slo = d.stride(g, TLO), shi = d.stride(g, THI);
+  const int mo = 3 * DIR;
 
+  // ---- stage: nodes n0-1 .. n0+TN ----------------------------------------
+  for (int item = threadIdx.x; item < NP * C; item += T::NT) {
+    int c, t;
+    split(item, NP, c, t);
+    const int a = n0 - 1 + t;
+    if (cbase + c >= ncol_max || a > m) continue;
+    const int64_t id = node_idx(g, c, a);
+    const int slots[4] = {1, 2, 3, 5};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double *f = z.bv + slots[q] * sz + id;
+      spts[T::spt(T::QV + q, c, t)] = f[0];
+      spts[T::spt(T::QD + 2 * q, c, t)] = f[slo] - f[-slo];
+      spts[T::spt(T::QD + 2 * q + 1, c, t)] = f[shi] - f[-shi];
+    }
+    const double jac = z.jac[id];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) spts[T::spt(T::QM + l, c, t)] = z.metric[id + l * sz];
+#pragma unroll
+    for (int l = 0; l < 3; ++l) spts[T::spt(T::QK + l, c, t)] = z.metric[id + (mo + l) * sz] * jac;
+    spts[T::spt(T::QMU, c, t)] = z.mul[id];
+  }
+  __syncthreads();
+
+  // ---- faces -------------------------------------------------------------
   for (int item = threadIdx.x; item < NF * C; item += T::NT) {
     int c, t;
     split(item, NF, c, t);
     const int f = n0 - 1 + t;
     if (cbase + c >= ncol_max || f > m - 1) continue;
-    const int64_t id = node_idx(g, c, f), idn = id + sd;
-    const double *mt = z.metric;
+    const double *s = spts;
+    auto A = [&](int q) { return s[T::spt(q, c, t)]; };
+    auto B = [&](int q) { return s[T::spt(q, c, t + 1)]; };
     double gm[9];
 #pragma unroll
-    for (int l = 0; l < 9; ++l) gm[l] = 0.5 * (mt[id + l * sz] + mt[idn + l * sz]);
-    // d/d(xi_dir) across the face and the averaged central cross derivatives
-    const double *pv = z.bv;
+    for (int l = 0; l < 9; ++l) gm[l] = 0.5 * (A(T::QM + l) + B(T::QM + l));
     double dd[4][3];
-    const int slots[4] = {1, 2, 3, 5};
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const double *fa = pv + slots[a] * sz;
-      dd[a][DIR] = fa[idn] - fa[id];
-      dd[a][DA] = 0.25 * (fa[id + sa] - fa[id - sa] + fa[idn + sa] - fa[idn - sa]);
-      dd[a][DB] = 0.25 * (fa[id + sb] - fa[id - sb] + fa[idn + sb] - fa[idn - sb]);
+    for (int q = 0; q < 4; ++q) {
+      dd[q][DIR] = B(T::QV + q) - A(T::QV + q);
+      dd[q][TLO] = 0.25 * (A(T::QD + 2 * q) + B(T::QD + 2 * q));
+      dd[q][THI] = 0.25 * (A(T::QD + 2 * q + 1) + B(T::QD + 2 * q + 1));
     }
     const double u_x = dd[0][0] * gm[0] + dd[0][1] * gm[3] + dd[0][2] * gm[6];
     const double u_y = dd[0][0] * gm[1] + dd[0][1] * gm[4] + dd[0][2] * gm[7];
@@ -79,24 +122,22 @@ __global__ void __launch_bounds__(256) viscous_air_flux_diff(Zone z, double Pr) 
     const double w_x = dd[2][0] * gm[0] + dd[2][1] * gm[3] + dd[2][2] * gm[6];
     const double w_y = dd[2][0] * gm[1] + dd[2][1] * gm[4] + dd[2][2] * gm[7];
     const double w_z = dd[2][0] * gm[2] + dd[2][1] * gm[5] + dd[2][2] * gm[8];
-    const double mul = 0.5 * (z.mul[id] + z.mul[idn]);
+    const double mul = 0.5 * (A(T::QMU) + B(T::QMU));
     const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
     const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
     const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
     const double tau_xy = mul * (u_y + v_x);
     const double tau_xz = mul * (u_z + w_x);
     const double tau_yz = mul * (v_z + w_y);
-    const int mo = 3 * DIR;
-    const double ja = z.jac[id], jb = z.jac[idn];
-    const double gk0 = 0.5 * (mt[id + mo * sz] * ja + mt[idn + mo * sz] * jb);
-    const double gk1 = 0.5 * (mt[id + (mo + 1) * sz] * ja + mt[idn + (mo + 1) * sz] * jb);
-    const double gk2 = 0.5 * (mt[id + (mo + 2) * sz] * ja + mt[idn + (mo + 2) * sz] * jb);
+    const double gk0 = 0.5 * (A(T::QK) + B(T::QK));
+    const double gk1 = 0.5 * (A(T::QK + 1) + B(T::QK + 1));
+    const double gk2 = 0.5 * (A(T::QK + 2) + B(T::QK + 2));
     const double f0 = gk0 * tau_xx + gk1 * tau_xy + gk2 * tau_xz;
     const double f1 = gk0 * tau_xy + gk1 * tau_yy + gk2 * tau_yz;
     const double f2 = gk0 * tau_xz + gk1 * tau_yz + gk2 * tau_zz;
-    const double um = 0.5 * (pv[id + sz] + pv[idn + sz]);
-    const double vm = 0.5 * (pv[id + 2 * sz] + pv[idn + 2 * sz]);
-    const double wm = 0.5 * (pv[id + 3 * sz] + pv[idn + 3 * sz]);
+    const double um = 0.5 * (A(T::QV) + B(T::QV));
+    const double vm = 0.5 * (A(T::QV + 1) + B(T::QV + 1));
+    const double wm = 0.5 * (A(T::QV + 2) + B(T::QV + 2));
     const double t_x = dd[3][0] * gm[0] + dd[3][1] * gm[3] + dd[3][2] * gm[6];
     const double t_y = dd[3][0] * gm[1] + dd[3][1] * gm[4] + dd[3][2] * gm[7];
     const double t_z = dd[3][0] * gm[2] + dd[3][1] * gm[5] + dd[3][2] * gm[8];
@@ -127,8 +168,21 @@ static cudaError_t launch_vis_dir(const Zone &z, double Pr, cudaStream_t st) {
   if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
-  viscous_air_flux_diff<DIR><<<grid, T::NT, 0, st>>>(z, Pr);
+  viscous_air_flux_diff<DIR><<<grid, T::NT, T::smem_bytes(), st>>>(z, Pr);
   return cudaGetLastError();
+}
+
+// Opt the three sweeps in to their dynamic shared-memory size (> 48 KB).
+cudaError_t viscous_air_init_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(viscous_air_flux_diff<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)VisTile<0>::smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(viscous_air_flux_diff<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)VisTile<1>::smem_bytes());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(viscous_air_flux_diff<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)VisTile<2>::smem_bytes());
+  return e;
 }
 
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch) {
