@@ -160,6 +160,126 @@ __global__ void __launch_bounds__(256, 3) viscous_air_flux_diff(Zone z, double P
   }
 }
 
+// Column march for the y and z sweeps: one thread per i column walks TM
+// nodes along the sweep, keeping the previous node's values and face flux in
+// registers, so every node is loaded once, loads stay coalesced along i and
+// no block barrier separates load and compute.  Same face arithmetic as the
+// staged kernel above.
+namespace {
+struct VisNode {
+  double v[4];     // u, v, w, T
+  double dlo[4];   // f(+1) - f(-1) along the lower-numbered transverse direction
+  double dhi[4];   // ... along the higher-numbered one
+  double mt[9];    // metric
+  double mk[3];    // metric row of the sweep times J
+  double mu;
+};
+
+template <int DIR>
+__device__ __forceinline__ void load_node(const Zone &z, int64_t id, int64_t sz, int64_t slo, int64_t shi,
+                                          VisNode &n) {
+  const int slots[4] = {1, 2, 3, 5};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double *f = z.bv + slots[q] * sz + id;
+    n.v[q] = __ldg(f);
+    n.dlo[q] = __ldg(f + slo) - __ldg(f - slo);
+    n.dhi[q] = __ldg(f + shi) - __ldg(f - shi);
+  }
+  const double jac = __ldg(z.jac + id);
+#pragma unroll
+  for (int l = 0; l < 9; ++l) n.mt[l] = __ldg(z.metric + id + l * sz);
+#pragma unroll
+  for (int l = 0; l < 3; ++l) n.mk[l] = n.mt[3 * DIR + l] * jac;
+  n.mu = __ldg(z.mul + id);
+}
+
+template <int DIR>
+__device__ __forceinline__ void face_flux(const VisNode &A, const VisNode &B, double Pr, double F[4]) {
+  constexpr int TLO = DIR == 0 ? 1 : 0, THI = DIR == 2 ? 1 : 2;
+  double gm[9];
+#pragma unroll
+  for (int l = 0; l < 9; ++l) gm[l] = 0.5 * (A.mt[l] + B.mt[l]);
+  double dd[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    dd[q][DIR] = B.v[q] - A.v[q];
+    dd[q][TLO] = 0.25 * (A.dlo[q] + B.dlo[q]);
+    dd[q][THI] = 0.25 * (A.dhi[q] + B.dhi[q]);
+  }
+  const double u_x = dd[0][0] * gm[0] + dd[0][1] * gm[3] + dd[0][2] * gm[6];
+  const double u_y = dd[0][0] * gm[1] + dd[0][1] * gm[4] + dd[0][2] * gm[7];
+  const double u_z = dd[0][0] * gm[2] + dd[0][1] * gm[5] + dd[0][2] * gm[8];
+  const double v_x = dd[1][0] * gm[0] + dd[1][1] * gm[3] + dd[1][2] * gm[6];
+  const double v_y = dd[1][0] * gm[1] + dd[1][1] * gm[4] + dd[1][2] * gm[7];
+  const double v_z = dd[1][0] * gm[2] + dd[1][1] * gm[5] + dd[1][2] * gm[8];
+  const double w_x = dd[2][0] * gm[0] + dd[2][1] * gm[3] + dd[2][2] * gm[6];
+  const double w_y = dd[2][0] * gm[1] + dd[2][1] * gm[4] + dd[2][2] * gm[7];
+  const double w_z = dd[2][0] * gm[2] + dd[2][1] * gm[5] + dd[2][2] * gm[8];
+  const double mul = 0.5 * (A.mu + B.mu);
+  const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+  const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+  const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double tau_xy = mul * (u_y + v_x);
+  const double tau_xz = mul * (u_z + w_x);
+  const double tau_yz = mul * (v_z + w_y);
+  const double gk0 = 0.5 * (A.mk[0] + B.mk[0]);
+  const double gk1 = 0.5 * (A.mk[1] + B.mk[1]);
+  const double gk2 = 0.5 * (A.mk[2] + B.mk[2]);
+  F[0] = gk0 * tau_xx + gk1 * tau_xy + gk2 * tau_xz;
+  F[1] = gk0 * tau_xy + gk1 * tau_yy + gk2 * tau_yz;
+  F[2] = gk0 * tau_xz + gk1 * tau_yz + gk2 * tau_zz;
+  const double um = 0.5 * (A.v[0] + B.v[0]);
+  const double vm = 0.5 * (A.v[1] + B.v[1]);
+  const double wm = 0.5 * (A.v[2] + B.v[2]);
+  const double t_x = dd[3][0] * gm[0] + dd[3][1] * gm[3] + dd[3][2] * gm[6];
+  const double t_y = dd[3][0] * gm[1] + dd[3][1] * gm[4] + dd[3][2] * gm[7];
+  const double t_z = dd[3][0] * gm[2] + dd[3][1] * gm[5] + dd[3][2] * gm[8];
+  constexpr double cp = kGammaAir * kRAir / (kGammaAir - 1);
+  const double conductivity = mul / Pr * cp;
+  F[3] = um * F[0] + vm * F[1] + wm * F[2] + conductivity * (gk0 * t_x + gk1 * t_y + gk2 * t_z);
+}
+
+constexpr int kMarchTM = 32;   // nodes per thread
+constexpr int kMarchNT = 128;  // threads (i columns) per CTA
+}  // namespace
+
+template <int DIR>
+__global__ void __launch_bounds__(kMarchNT) viscous_air_march(Zone z, double Pr) {
+  static_assert(DIR == 1 || DIR == 2, "the x sweep uses the staged kernel");
+  const Dims d = z.d;
+  const int i = blockIdx.x * kMarchNT + threadIdx.x;
+  if (i >= d.mx) return;
+  const int n0 = blockIdx.y * kMarchTM, other = blockIdx.z;
+  const int m = d.ext(DIR);
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), szq = d.plane(0);
+  const int64_t sd = d.stride(g, DIR), sdq = d.stride(0, DIR);
+  constexpr int TLO = DIR == 0 ? 1 : 0, THI = DIR == 2 ? 1 : 2;
+  const int64_t slo = d.stride(g, TLO), shi = d.stride(g, THI);
+  int64_t id = DIR == 1 ? d.idx(g, i, n0 - 1, other) : d.idx(g, i, other, n0 - 1);
+  int64_t iq = DIR == 1 ? d.idx(0, i, n0, other) : d.idx(0, i, other, n0);
+  VisNode A, B;
+  load_node<DIR>(z, id, sz, slo, shi, A);
+  load_node<DIR>(z, id + sd, sz, slo, shi, B);
+  double Fp[4];
+  face_flux<DIR>(A, B, Pr, Fp);  // face n0 - 1/2
+  const int n_end = min(n0 + kMarchTM, m);
+  for (int n = n0; n < n_end; ++n) {
+    // face n + 1/2 between node n (B) and node n + 1
+    id += sd;
+    A = B;
+    load_node<DIR>(z, id + sd, sz, slo, shi, B);
+    double F[4];
+    face_flux<DIR>(A, B, Pr, F);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) z.dq[iq + (v + 1) * szq] += F[v] - Fp[v];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Fp[v] = F[v];
+    iq += sdq;
+  }
+}
+
 template <int DIR>
 static cudaError_t launch_vis_dir(const Zone &z, double Pr, cudaStream_t st) {
   using T = VisTile<DIR>;
@@ -168,7 +288,13 @@ static cudaError_t launch_vis_dir(const Zone &z, double Pr, cudaStream_t st) {
   if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
-  viscous_air_flux_diff<DIR><<<grid, T::NT, T::smem_bytes(), st>>>(z, Pr);
+  if (DIR == 0) {
+    viscous_air_flux_diff<DIR><<<grid, T::NT, T::smem_bytes(), st>>>(z, Pr);
+  } else {
+    const dim3 gm((d.mx + kMarchNT - 1) / kMarchNT, (d.ext(DIR) + kMarchTM - 1) / kMarchTM,
+                  DIR == 1 ? d.mz : d.my);
+    viscous_air_march<DIR == 0 ? 1 : DIR><<<gm, kMarchNT, 0, st>>>(z, Pr);
+  }
   return cudaGetLastError();
 }
 
