@@ -111,14 +111,14 @@ def _upload(ctx, zone, case):
     ctx.sync()
 
 
-def cpu_baseline_sample(target_s: float = 15.0, n: int = 49):
+def cpu_baseline_sample(scheme: int, reconstruction: int, target_s: float = 15.0, n: int = 49):
     """The oracle (the reference's algorithm restated in C, OpenMP on all host
     threads) on a bounded sample of the workload: the same wave and settings
     on an n^3 block, stepped until ~target_s of CPU work."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle  # test/baseline infrastructure only
 
-    case = cases.sine_wave(n=n, scheme=args.scheme, viscous=True, cfl=0.5, reconstruction=args.reconstruction)
+    case = cases.sine_wave(n=n, scheme=scheme, viscous=True, cfl=0.5, reconstruction=reconstruction)
     z = pyoracle.OracleZone(case)
     z.initialize()
     z.step()  # warm
@@ -138,7 +138,7 @@ def run_reference(args, rank, world):
     # bounded sample per step, sized so that the whole run stays within minutes
     total = max(args.steps + args.warmup, 1)
     per = max(3.0, min(20.0, 150.0 / total))
-    res = cpu_baseline_sample(target_s=per * args.steps)
+    res = cpu_baseline_sample(args.scheme, args.reconstruction, target_s=per * args.steps)
     line = {
         "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(res["steps"], 1),
@@ -522,7 +522,7 @@ def main():
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample()
+            cpu = cpu_baseline_sample(args.scheme, args.reconstruction)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
