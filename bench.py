@@ -46,6 +46,17 @@ N_NODES = 257
 FLOPS_PER_FACE_WENO7_CH = 2980.0
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of each rank's x (one all-reduce); x itself without a process group."""
+    if not dist:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -192,10 +203,7 @@ def reacting_bench(args, local, world, dist):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, f"cuda:{local}")
         n = nsub.cpu().numpy()
         out[name] = {"cells_per_s": case.N * k * world / (ms * 1e-3), "ms_per_step": ms / k, "steps": k,
                      "substeps_mean": float(n.mean()), "substeps_max": int(n.max())}
@@ -445,10 +453,8 @@ def main():
     launches = ctx.kernel_launches - launches0
     phases = ctx.profile_read()
     ctx.set_profiling(False)
+    ms = max_over_ranks(ms, dist, f"cuda:{local}")
     if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     nodes = case.N
     value = nodes * args.steps * world / (ms * 1e-3)
@@ -540,10 +546,7 @@ def main():
     e1.record(s_comp)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_e2e], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dist, f"cuda:{local}")
     e2e = {"value": nodes * args.e2e_steps * world / (ms_e2e * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes, "steps": args.e2e_steps,
            "ms_per_step": ms_e2e / args.e2e_steps,
