@@ -49,7 +49,7 @@ def test_max_over_ranks_with_two_gloo_ranks():
     with socket.socket() as sk:
         sk.bind(("127.0.0.1", 0))
         port = sk.getsockname()[1]
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
     assert dict(out) == {0: 15.0, 1: 15.0}
