@@ -131,7 +131,8 @@ def _air_param(**kw) -> dict:
 
 def ghost_layers(scheme: int, viscous_order: int = 0) -> int:
     """Ghost layers of an inviscid scheme (reference src/Parameter.cpp:196-252),
-    at least 4 with the 8th-order viscous scheme (:296-300)."""
+    at least 4 with the 8th-order viscous scheme (:296-300) and 2 with the
+    4th-order one."""
     g = 2
     if scheme in (71, 72):
         g = 4

@@ -93,7 +93,7 @@ cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, con
 // 2nd-order face scheme or the 8th-order collocated one.
 cudaError_t launch_viscous(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces, int n_face,
                            cudaStream_t st, int *n) {
-  if (p.viscous_order == 8) return launch_viscous8(z, p, th, faces, n_face, z.fvis8, st, n);
+  if (p.viscous_order == 8 || p.viscous_order == 4) return launch_viscous8(z, p, th, faces, n_face, z.fvis8, st, n);
   return th ? launch_viscous_mix(z, p, *th, st, n) : launch_viscous_air(z, p, st, n);
 }
 
@@ -113,8 +113,8 @@ int validate(const cfk_param *p, std::string &why) {
   }
   if (s >= 1 && s <= 4 && !(p->limiter == 0 || p->limiter == 1)) { why = "limiter must be 0 or 1"; return -1; }
   if (s == 2 && !(p->entropy_fix_factor >= 0)) { why = "entropy_fix_factor must be >= 0"; return -1; }
-  if (p->viscous_order != 0 && p->viscous_order != 2 && p->viscous_order != 8) {
-    why = "viscous_order must be 0, 2 or 8";
+  if (p->viscous_order != 0 && p->viscous_order != 2 && p->viscous_order != 4 && p->viscous_order != 8) {
+    why = "viscous_order must be 0, 2, 4 or 8";
     return -1;
   }
   if (p->sensor_threshold > 1e-10 && !(s == 52 || s == 72)) {
@@ -270,8 +270,8 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   z.reaction_timeScale = zn->reaction_timeScale; z.dq = zn->dq; z.dt_local = zn->dt_local; z.Cn = zn->Cn;
   z.shock_sensor = zn->shock_sensor;
   z.fvis8 = nullptr;
-  if (c->hp.viscous_order == 8) {
-    // node fluxes of the 8th-order viscous scheme, owned by the context
+  if (c->hp.viscous_order == 8 || c->hp.viscous_order == 4) {
+    // node fluxes of the collocated viscous schemes, owned by the context
     const size_t n8 = (size_t)z.d.plane(z.d.ngg) * 3 * (c->hp.n_var - 1);
     if (c->own_fvis8_n < n8) {
       if (c->own_fvis8) cudaFree(c->own_fvis8);

@@ -1,5 +1,8 @@
-// 8th-order collocated viscous scheme (viscous_order = 8), air and 9-species
-// mixtures.
+// Collocated viscous schemes, air and 9-species mixtures: the reference's
+// 8th-order scheme (viscous_order = 8) and a 4th-order variant
+// (viscous_order = 4, not in the reference) built from the same pieces: the
+// reference's 4th-order central operator (its row for the third node from a
+// wall) in the interior and its two one-sided rows at physical faces.
 //
 // Restates the order-8 branch of compute_viscous_flux (reference
 // src/ViscousScheme.cu:41-70) as three steps:
@@ -31,8 +34,16 @@ namespace {
 
 // derivative along one direction at node n of nn; f points at the node, s
 // is the stride; left/right: the line ends at a physical boundary face.
+template <int ORDER>
 __device__ __forceinline__ double d8(const double *__restrict__ f, int64_t s, int n, int nn, bool left, bool right) {
   auto F = [&](int o) { return f[o * s]; };
+  if constexpr (ORDER == 4) {
+    if (left && n == 0) return -25.0 / 12 * F(0) + 4.0 * F(1) - 3 * F(2) + 4.0 / 3 * F(3) - 0.25 * F(4);
+    if (left && n == 1) return -0.25 * F(-1) - 5.0 / 6 * F(0) + 1.5 * F(1) - 0.5 * F(2) + 1.0 / 12 * F(3);
+    if (right && n == nn - 1) return 25.0 / 12 * F(0) - 4.0 * F(-1) + 3 * F(-2) - 4.0 / 3 * F(-3) + 0.25 * F(-4);
+    if (right && n == nn - 2) return 0.25 * F(1) + 5.0 / 6 * F(0) - 1.5 * F(-1) + 0.5 * F(-2) - 1.0 / 12 * F(-3);
+    return -1.0 / 12 * (F(2) - F(-2)) + 2.0 / 3 * (F(1) - F(-1));
+  }
   double df = 0;
   bool computed = false;
   if (left) {
@@ -76,15 +87,16 @@ struct Bnd {
   bool l[3], r[3];  // physical (non-periodic) boundary face on the min / max side of each direction
 };
 
+template <int ORDER>
 __device__ __forceinline__ void grad3(const double *f, int64_t sj, int64_t sk, int i, int j, int k, const Dims &d,
                                       const Bnd &b, double &dx, double &dy, double &dz) {
-  dx = d8(f, 1, i, d.mx, b.l[0], b.r[0]);
-  dy = d8(f, sj, j, d.my, b.l[1], b.r[1]);
-  dz = d8(f, sk, k, d.mz, b.l[2], b.r[2]);
+  dx = d8<ORDER>(f, 1, i, d.mx, b.l[0], b.r[0]);
+  dy = d8<ORDER>(f, sj, j, d.my, b.l[1], b.r[1]);
+  dz = d8<ORDER>(f, sk, k, d.mz, b.l[2], b.r[2]);
 }
 
 // NS = 0: calorically perfect air
-template <int NS>
+template <int NS, int ORDER>
 __global__ void __launch_bounds__(128) visc8_collocated(Zone z, double *fvis, Bnd b, double Pr,
                                                         const __grid_constant__ Thermo thermo) {
   constexpr int NV = 5 + NS;
@@ -95,10 +107,10 @@ __global__ void __launch_bounds__(128) visc8_collocated(Zone z, double *fvis, Bn
   const int64_t sz = d.plane(g), sj = d.stride(g, 1), sk = d.stride(g, 2);
   const int64_t id = d.idx(g, i, j, k);
   double u_xi, u_eta, u_zeta, v_xi, v_eta, v_zeta, w_xi, w_eta, w_zeta, t_xi, t_eta, t_zeta;
-  grad3(z.bv + sz + id, sj, sk, i, j, k, d, b, u_xi, u_eta, u_zeta);
-  grad3(z.bv + 2 * sz + id, sj, sk, i, j, k, d, b, v_xi, v_eta, v_zeta);
-  grad3(z.bv + 3 * sz + id, sj, sk, i, j, k, d, b, w_xi, w_eta, w_zeta);
-  grad3(z.bv + 5 * sz + id, sj, sk, i, j, k, d, b, t_xi, t_eta, t_zeta);
+  grad3<ORDER>(z.bv + sz + id, sj, sk, i, j, k, d, b, u_xi, u_eta, u_zeta);
+  grad3<ORDER>(z.bv + 2 * sz + id, sj, sk, i, j, k, d, b, v_xi, v_eta, v_zeta);
+  grad3<ORDER>(z.bv + 3 * sz + id, sj, sk, i, j, k, d, b, w_xi, w_eta, w_zeta);
+  grad3<ORDER>(z.bv + 5 * sz + id, sj, sk, i, j, k, d, b, t_xi, t_eta, t_zeta);
   const double *mt = z.metric + id;
   const double xi_x = mt[0], xi_y = mt[sz], xi_z = mt[2 * sz];
   const double eta_x = mt[3 * sz], eta_y = mt[4 * sz], eta_z = mt[5 * sz];
@@ -157,7 +169,7 @@ __global__ void __launch_bounds__(128) visc8_collocated(Zone z, double *fvis, Bn
       yk[l] = y[0];
       diffusivity[l] = z.rho_D[id + l * sz];
       double y_xi, y_eta, y_zeta;
-      grad3(y, sj, sk, i, j, k, d, b, y_xi, y_eta, y_zeta);
+      grad3<ORDER>(y, sj, sk, i, j, k, d, b, y_xi, y_eta, y_zeta);
       const double y_x = y_xi * xi_x + y_eta * eta_x + y_zeta * zeta_x;
       const double y_y = y_xi * xi_y + y_eta * eta_y + y_zeta * zeta_y;
       const double y_z = y_xi * xi_z + y_eta * eta_z + y_zeta * zeta_z;
@@ -226,7 +238,7 @@ __global__ void visc8_periodic_exchange(Zone z, double *fvis, int nplanes, int d
   }
 }
 
-template <int NV>
+template <int NV, int ORDER>
 __global__ void __launch_bounds__(128) visc8_derivative(Zone z, const double *fvis, Bnd b) {
   const Dims d = z.d;
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
@@ -240,8 +252,8 @@ __global__ void __launch_bounds__(128) visc8_derivative(Zone z, const double *fv
   for (int l = 1; l < NV; ++l) {
     const double *fv = fvis + (l - 1) * sz + id, *gv = fvis + (NV - 1 + l - 1) * sz + id,
                  *hv = fvis + (2 * (NV - 1) + l - 1) * sz + id;
-    double s = d8(fv, 1, i, d.mx, b.l[0], b.r[0]) + d8(gv, sj, j, d.my, b.l[1], b.r[1]);
-    if (three_d) s += d8(hv, sk, k, d.mz, b.l[2], b.r[2]);
+    double s = d8<ORDER>(fv, 1, i, d.mx, b.l[0], b.r[0]) + d8<ORDER>(gv, sj, j, d.my, b.l[1], b.r[1]);
+    if (three_d) s += d8<ORDER>(hv, sk, k, d.mz, b.l[2], b.r[2]);
     z.dq[iq + l * szq] += s * jac;
   }
 }
@@ -263,8 +275,11 @@ cudaError_t launch_viscous8(const Zone &z, const Param &p, const Thermo *th, con
   const Bnd b = boundary_flags(faces, n_face);
   const dim3 grid((d.mx + 127) / 128, d.my, d.mz);
   static const Thermo no_thermo{};
-  if (th) visc8_collocated<kMaxSpec><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th);
-  else visc8_collocated<0><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo);
+  const bool o4 = p.viscous_order == 4;
+  if (th && o4) visc8_collocated<kMaxSpec, 4><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th);
+  else if (th) visc8_collocated<kMaxSpec, 8><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th);
+  else if (o4) visc8_collocated<0, 4><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo);
+  else visc8_collocated<0, 8><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   *n_launch += 1;
@@ -277,8 +292,10 @@ cudaError_t launch_viscous8(const Zone &z, const Param &p, const Thermo *th, con
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     *n_launch += 1;
   }
-  if (th) visc8_derivative<5 + kMaxSpec><<<grid, 128, 0, st>>>(z, fvis, b);
-  else visc8_derivative<5><<<grid, 128, 0, st>>>(z, fvis, b);
+  if (th && o4) visc8_derivative<5 + kMaxSpec, 4><<<grid, 128, 0, st>>>(z, fvis, b);
+  else if (th) visc8_derivative<5 + kMaxSpec, 8><<<grid, 128, 0, st>>>(z, fvis, b);
+  else if (o4) visc8_derivative<5, 4><<<grid, 128, 0, st>>>(z, fvis, b);
+  else visc8_derivative<5, 8><<<grid, 128, 0, st>>>(z, fvis, b);
   *n_launch += 1;
   return cudaGetLastError();
 }

@@ -53,7 +53,7 @@ typedef struct cfk_param {
   int inviscid_scheme;     /* 2 Roe, 3 AUSM+, 4 HLLC (MUSCL/NND2/1st), 51/52/71/72 WENO */
   int reconstruction;      /* 1 first order, 2 MUSCL, 3 NND2 */
   int limiter;             /* 0 minmod, 1 van Leer */
-  int viscous_order;       /* 0 or 2 */
+  int viscous_order;       /* 0, 2 or 8 as in the reference; 4: the added 4th-order collocated scheme */
   int positive_preserving;
   int gradPInDiffusionFlux;
   int fixed_dt;

@@ -544,7 +544,7 @@ static void viscous_direction(orc_zone *z, const orc_param *p, int dir) {
 void orc_viscous_flux_8th(orc_zone *z, const orc_param *p);
 
 void orc_compute_viscous_flux(orc_zone *z, const orc_param *p) {
-  if (p->viscous_order == 8) {
+  if (p->viscous_order == 8 || p->viscous_order == 4) {
     orc_viscous_flux_8th(z, p);
     return;
   }

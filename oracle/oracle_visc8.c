@@ -1,5 +1,10 @@
 /*
- * CPU oracle: the 8th-order collocated viscous scheme (viscous_order = 8).
+ * CPU oracle: the collocated viscous schemes, 8th order (viscous_order = 8,
+ * the reference's) and 4th order (viscous_order = 4: the same scheme with the
+ * reference's 4th-order central operator of its n = 2 boundary row used in
+ * the interior, and its n = 0 / n = 1 one-sided rows at physical faces; the
+ * reference has no 4th-order viscous scheme, so this one is checked by its
+ * own exactness and convergence, not against a reference build).
  * TEST INFRASTRUCTURE ONLY (see oracle.h).
  *
  * Restates, in the reference's arithmetic order:
@@ -41,10 +46,19 @@ static inline long pstride(const orc_zone *z, int g, int dir) {
 }
 
 /* d f / d(xi_dir) at node index n (0..nn-1) of a line through f[id], stride s */
+static int g_order = 8; /* set by the entry point before the kernels run */
+
 static double d8(const double *f, long id, long s, int n, int nn, int left, int right) {
   double df = 0;
   int computed = 0;
 #define F(o) f[id + (long)(o) * s]
+  if (g_order == 4) {
+    if (left && n == 0) return -25.0 / 12 * F(0) + 4.0 * F(1) - 3 * F(2) + 4.0 / 3 * F(3) - 0.25 * F(4);
+    if (left && n == 1) return -0.25 * F(-1) - 5.0 / 6 * F(0) + 1.5 * F(1) - 0.5 * F(2) + 1.0 / 12 * F(3);
+    if (right && n == nn - 1) return 25.0 / 12 * F(0) - 4.0 * F(-1) + 3 * F(-2) - 4.0 / 3 * F(-3) + 0.25 * F(-4);
+    if (right && n == nn - 2) return 0.25 * F(1) + 5.0 / 6 * F(0) - 1.5 * F(-1) + 0.5 * F(-2) - 1.0 / 12 * F(-3);
+    return -1.0 / 12 * (F(2) - F(-2)) + 2.0 / 3 * (F(1) - F(-1));
+  }
   if (left) {
     if (n == 0) {
       df = -25.0 / 12 * F(0) + 4.0 * F(1) - 3 * F(2) + 4.0 / 3 * F(3) - 0.25 * F(4);
@@ -260,6 +274,7 @@ static void derivative(orc_zone *z, const orc_param *p, const int bt[3][2]) {
 }
 
 void orc_viscous_flux_8th(orc_zone *z, const orc_param *p) {
+  g_order = p->viscous_order == 4 ? 4 : 8;
   int bt[3][2];
   boundary_types(p, bt);
   collocated(z, p, bt);

@@ -1,5 +1,6 @@
-"""The 8th-order collocated viscous scheme (viscous_order = 8) in the CPU oracle
-(reference src/ViscousScheme.cu:41-70, 129-612).
+"""The collocated viscous schemes in the CPU oracle: 8th order (viscous_order =
+8, reference src/ViscousScheme.cu:41-70, 129-612) and its 4th-order variant
+(viscous_order = 4, which the reference does not have).
 
 Pins: (1) on a Cartesian block with physical (outflow) faces and a velocity
 that is cubic across the block, every node -- including the four next to each
@@ -34,8 +35,12 @@ def _viscous_dq(case):
     return oz
 
 
-def test_one_sided_boundary_stencils_exact_for_cubic_shear():
-    c = cases.sod(24, 12, scheme=4, viscous_order=8)
+import pytest
+
+
+@pytest.mark.parametrize("order", [8, 4])
+def test_one_sided_boundary_stencils_exact_for_cubic_shear(order):
+    c = cases.sod(24, 12, scheme=4, viscous_order=order)
     g = c.ngg
     # physical y of every padded node: sod puts node j at y = 0.01 j
     jj = np.broadcast_to(np.arange(-g, c.my + g)[None, :, None], c.shape()).reshape(-1)
@@ -75,3 +80,11 @@ def test_periodic_sine_shear_converges_at_eighth_order():
     assert e33 < 1e-6
     assert e17 / e33 > 150  # 2^8 = 256
     assert _periodic_sine_error(33, 2) > 100 * e33
+
+
+def test_periodic_sine_shear_converges_at_fourth_order():
+    """viscous_order = 4 (not in the reference): the same collocated scheme
+    with 4th-order central differences converges at 4th order."""
+    e17, e33 = _periodic_sine_error(17, 4), _periodic_sine_error(33, 4)
+    assert 12 < e17 / e33 < 20  # 2^4 = 16
+    assert e33 < _periodic_sine_error(33, 2) / 5

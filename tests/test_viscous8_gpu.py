@@ -1,7 +1,8 @@
-"""Parity of the 8th-order collocated viscous scheme (viscous_order = 8:
-node fluxes, periodic exchange in face order, derivative; reference
-src/ViscousScheme.cu:41-70, 129-612) against the CPU oracle.  Bar: single
-viscous calls 1e-11, RK3 / Wu steps 1e-12 per step."""
+"""Parity of the collocated viscous schemes against the CPU oracle: the
+reference's 8th-order scheme (viscous_order = 8: node fluxes, periodic
+exchange in face order, derivative; reference src/ViscousScheme.cu:41-70,
+129-612) and its 4th-order variant (viscous_order = 4).  Bar: single viscous
+calls 1e-11, RK3 / Wu steps 1e-12 per step."""
 import pytest
 
 import cases
@@ -27,19 +28,25 @@ def _single_viscous(case):
     return rel_err(gz.get("dq")[1:], oz["dq"][1:], momentum=(0, 1, 2))
 
 
-def test_air_periodic_3d_single_call():
-    case = cases.perturbed(cases.sine_wave(n=19, ny=37, nz=30, scheme=72, viscous_order=8), seed=7, amp=1e-2)
+ORDERS = pytest.mark.parametrize("order", [8, 4])
+
+
+@ORDERS
+def test_air_periodic_3d_single_call(order):
+    case = cases.perturbed(cases.sine_wave(n=19, ny=37, nz=30, scheme=72, viscous_order=order), seed=7, amp=1e-2)
     assert _single_viscous(case) <= 1e-11
 
 
-def test_air_walls_2d_single_call():
+@ORDERS
+def test_air_walls_2d_single_call(order):
     """Physical faces on every side: the one-sided boundary stencils."""
-    case = cases.perturbed(cases.sod(64, 13, scheme=4, viscous_order=8), seed=2, amp=1e-2)
+    case = cases.perturbed(cases.sod(64, 13, scheme=4, viscous_order=order), seed=2, amp=1e-2)
     assert _single_viscous(case) <= 1e-11
 
 
-def test_mixture_periodic_3d_single_call():
-    case = cases.perturbed(cases.mix_wave(mechanism.load("li2004"), 13, ny=17, nz=19, scheme=72, viscous_order=8),
+@ORDERS
+def test_mixture_periodic_3d_single_call(order):
+    case = cases.perturbed(cases.mix_wave(mechanism.load("li2004"), 13, ny=17, nz=19, scheme=72, viscous_order=order),
                            seed=4, amp=1e-2)
     assert _single_viscous(case) <= 1e-11
 
@@ -50,8 +57,14 @@ def test_air_rk3_steps(scheme):
     _lockstep(case, 3)
 
 
-def test_air_sod_viscous8_steps():
-    _lockstep(cases.sod(200, 9, scheme=52, viscous_order=8), 10)
+@ORDERS
+def test_air_sod_viscous_collocated_steps(order):
+    _lockstep(cases.sod(200, 9, scheme=52, viscous_order=order), 10)
+
+
+def test_air_rk3_steps_fourth_order():
+    case = cases.perturbed(cases.sine_wave(n=19, ny=37, nz=30, scheme=72, viscous_order=4), seed=7)
+    _lockstep(case, 3)
 
 
 def test_mixture_rk3_steps():
