@@ -221,17 +221,37 @@ __device__ __forceinline__ void face_node(const FaceGeom &fg, int t, int &i, int
   i = fg.lo[0] + a; j = fg.lo[1] + b; k = fg.lo[2] + c;
 }
 
+// Work split of a boundary-face kernel.  On i faces the ghost layers of a
+// face node are consecutive in memory, so ngg + 1 threads share a node: part
+// 0 does the face node's own work, part gg fills ghost layer gg (the ghost
+// fills read interior nodes only, never the face node, so the parts are
+// independent); the lanes of a warp then cover whole runs of ghost cells
+// instead of one cell per row.  On j and k faces one thread does the node and
+// all its ghost layers, the lanes running along i.
+__device__ __forceinline__ bool face_work(const FaceGeom &fg, int g, int &i, int &j, int &k, int &gg_lo,
+                                          int &gg_hi, bool &face_part) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int parts = fg.face == 0 ? g + 1 : 1;
+  const int node = t / parts, part = t - node * parts;
+  if (node >= fg.n[0] * fg.n[1] * fg.n[2]) return false;
+  face_node(fg, node, i, j, k);
+  face_part = fg.face != 0 || part == 0;
+  gg_lo = fg.face == 0 ? part : 1;
+  gg_hi = fg.face == 0 ? part : g;
+  if (fg.face == 0 && part == 0) { gg_lo = 1; gg_hi = 0; }
+  return true;
+}
+
 template <bool MIX>
 __global__ void bc_outflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
-  int i, j, k;
-  face_node(fg, t, i, j, k);
   const Dims d = z.d;
   const int g = d.ngg;
+  int i, j, k, gg_lo, gg_hi;
+  bool face_part;
+  if (!face_work(fg, g, i, j, k, gg_lo, gg_hi, face_part)) return;
   const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
   const int64_t s = d.stride(g, fg.face) * fg.direction;
-  for (int gg = 1; gg <= g; ++gg) {
+  for (int gg = gg_lo; gg <= gg_hi; ++gg) {
     const int64_t gi = id + gg * s;
     for (int l = 0; l < 6; ++l) z.bv[gi + l * sz] = z.bv[id + l * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[id + l * sz];
@@ -241,12 +261,11 @@ __global__ void bc_outflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg
 
 template <bool MIX>
 __global__ void bc_symmetry_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
-  int i, j, k;
-  face_node(fg, t, i, j, k);
   const Dims d = z.d;
   const int g = d.ngg;
+  int i, j, k, gg_lo, gg_hi;
+  bool face_part;
+  if (!face_work(fg, g, i, j, k, gg_lo, gg_hi, face_part)) return;
   const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
   const int64_t s = d.stride(g, fg.face) * fg.direction;
   const int64_t in = id - s;
@@ -254,20 +273,22 @@ __global__ void bc_symmetry_kernel(Zone z, Param p, const Thermo *th, FaceGeom f
   double k_x = z.metric[id + mf * sz], k_y = z.metric[id + (mf + 1) * sz], k_z = z.metric[id + (mf + 2) * sz];
   const double k_magnitude = sqrt(k_x * k_x + k_y * k_y + k_z * k_z);
   k_x /= k_magnitude; k_y /= k_magnitude; k_z /= k_magnitude;
-  const double u1 = z.bv[in + sz], v1 = z.bv[in + 2 * sz], w1 = z.bv[in + 3 * sz];
-  double u_k = k_x * u1 + k_y * v1 + k_z * w1;
-  z.bv[id + sz] = u1 - k_x * u_k;
-  z.bv[id + 2 * sz] = v1 - k_y * u_k;
-  z.bv[id + 3 * sz] = w1 - k_z * u_k;
-  z.bv[id] = z.bv[in];
-  z.bv[id + 4 * sz] = z.bv[in + 4 * sz];
-  z.bv[id + 5 * sz] = z.bv[in + 5 * sz];
-  for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = z.sv[in + l * sz];
-  for (int gg = 1; gg <= g; ++gg) {
+  if (face_part) {
+    const double u1 = z.bv[in + sz], v1 = z.bv[in + 2 * sz], w1 = z.bv[in + 3 * sz];
+    const double u_k = k_x * u1 + k_y * v1 + k_z * w1;
+    z.bv[id + sz] = u1 - k_x * u_k;
+    z.bv[id + 2 * sz] = v1 - k_y * u_k;
+    z.bv[id + 3 * sz] = w1 - k_z * u_k;
+    z.bv[id] = z.bv[in];
+    z.bv[id + 4 * sz] = z.bv[in + 4 * sz];
+    z.bv[id + 5 * sz] = z.bv[in + 5 * sz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = z.sv[in + l * sz];
+  }
+  for (int gg = gg_lo; gg <= gg_hi; ++gg) {
     const int64_t gi = id + gg * s, ii = id - gg * s;
     z.bv[gi] = z.bv[ii];
     const double u = z.bv[ii + sz], v = z.bv[ii + 2 * sz], w = z.bv[ii + 3 * sz];
-    u_k = k_x * u + k_y * v + k_z * w;
+    const double u_k = k_x * u + k_y * v + k_z * w;
     z.bv[gi + sz] = u - 2 * u_k * k_x;
     z.bv[gi + 2 * sz] = v - 2 * u_k * k_y;
     z.bv[gi + 3 * sz] = w - 2 * u_k * k_z;
@@ -280,29 +301,30 @@ __global__ void bc_symmetry_kernel(Zone z, Param p, const Thermo *th, FaceGeom f
 
 template <bool MIX>
 __global__ void bc_periodic_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
-  int i, j, k;
-  face_node(fg, t, i, j, k);
   const Dims d = z.d;
   const int g = d.ngg;
+  int i, j, k, gg_lo, gg_hi;
+  bool face_part;
+  if (!face_work(fg, g, i, j, k, gg_lo, gg_hi, face_part)) return;
   const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
   const int64_t sd = d.stride(g, fg.face);
   const int64_t s = sd * fg.direction;
   const int mface = d.ext(fg.face);
   const int64_t io = id + (int64_t)(fg.direction < 0 ? (mface - 1) : -(mface - 1)) * sd;
-  for (int l = 0; l < 6; ++l) {
-    const double ave = 0.5 * (z.bv[id + l * sz] + z.bv[io + l * sz]);
-    z.bv[id + l * sz] = ave;
-    z.bv[io + l * sz] = ave;
+  if (face_part) {
+    for (int l = 0; l < 6; ++l) {
+      const double ave = 0.5 * (z.bv[id + l * sz] + z.bv[io + l * sz]);
+      z.bv[id + l * sz] = ave;
+      z.bv[io + l * sz] = ave;
+    }
+    for (int l = 0; l < p.n_scalar; ++l) {
+      const double ave = 0.5 * (z.sv[id + l * sz] + z.sv[io + l * sz]);
+      z.sv[id + l * sz] = ave;
+      z.sv[io + l * sz] = ave;
+    }
+    cv_from_bv_point<MIX>(z, p, th, id);
   }
-  for (int l = 0; l < p.n_scalar; ++l) {
-    const double ave = 0.5 * (z.sv[id + l * sz] + z.sv[io + l * sz]);
-    z.sv[id + l * sz] = ave;
-    z.sv[io + l * sz] = ave;
-  }
-  cv_from_bv_point<MIX>(z, p, th, id);
-  for (int gg = 1; gg <= g; ++gg) {
+  for (int gg = gg_lo; gg <= gg_hi; ++gg) {
     const int64_t gi = id + gg * s, ii = io + gg * s;
     for (int l = 0; l < 6; ++l) z.bv[gi + l * sz] = z.bv[ii + l * sz];
     for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[ii + l * sz];
@@ -390,7 +412,7 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
     for (int n = 0; n < n_face; ++n) {
       if (faces[n].label != order[o]) continue;
       const FaceGeom fg = make_face(z.d, faces[n]);
-      const int cnt = fg.n[0] * fg.n[1] * fg.n[2];
+      const int cnt = fg.n[0] * fg.n[1] * fg.n[2] * (fg.face == 0 ? z.d.ngg + 1 : 1);
       const int blocks = (cnt + 127) / 128;
       const bool mix = p.n_spec > 0;
       if (order[o] == 6) {
