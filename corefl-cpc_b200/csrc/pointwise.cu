@@ -6,6 +6,18 @@
 
 namespace cfk {
 
+// Node index of a thread in a launch that flattens the (i, j) plane of an
+// nx x ny block into 1-D thread blocks (grid.y = the k planes), so that rows
+// shorter than a thread block do not leave most of its lanes idle.
+__device__ __forceinline__ bool flat_ij(int nx, int ny, int &i, int &j) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * ny) return false;
+  j = t / nx;
+  i = t - j * nx;
+  return true;
+}
+
+
 // SSP-RK3 coefficients (reference src/RK.cuh:11-15)
 __constant__ double kRkA[3] = {1.0, 0.75, 1.0 / 3.0};
 __constant__ double kRkB[3] = {0.0, 0.25, 2.0 / 3.0};
@@ -22,9 +34,9 @@ __global__ void __launch_bounds__(256) update_cv_and_bv_rk_kernel(Zone z, Param 
                                                                   const double *dt_dev, int rk, int *err,
                                                                   bool minus_cn) {
   const Dims d = z.d;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
-  if (i >= d.mx) return;
+  int i, j;
+  if (!flat_ij(d.mx, d.my, i, j)) return;
+  const int k = blockIdx.y;
   const int g = d.ngg;
   const int64_t sz = d.plane(g), szq = d.plane(0);
   const int64_t id = d.idx(g, i, j, k), iq = d.idx(0, i, j, k);
@@ -108,9 +120,11 @@ template <bool MIX>
 __global__ void cv_from_bv_kernel(Zone z, Param p, const Thermo *th) {
   const Dims d = z.d;
   const int g = d.ngg;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - g;
-  const int j = blockIdx.y - g, k = blockIdx.z - g;
-  if (i >= d.mx + g) return;
+  int i, j;
+  if (!flat_ij(d.mx + 2 * g, d.my + 2 * g, i, j)) return;
+  i -= g;
+  j -= g;
+  const int k = blockIdx.y - g;
   cv_from_bv_point<MIX>(z, p, th, d.idx(g, i, j, k));
 }
 
@@ -123,9 +137,11 @@ template <bool MIX>
 __global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo *th) {
   const Dims d = z.d;
   const int g = d.ngg;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - g;
-  const int j = blockIdx.y - g, k = blockIdx.z - g;
-  if (i >= d.mx + g) return;
+  int i, j;
+  if (!flat_ij(d.mx + 2 * g, d.my + 2 * g, i, j)) return;
+  i -= g;
+  j -= g;
+  const int k = blockIdx.y - g;
   const int64_t sz = d.plane(g);
   const int64_t id = d.idx(g, i, j, k);
   const double t = z.bv[id + 5 * sz];
@@ -151,10 +167,11 @@ template <bool MIX>
 __global__ void __launch_bounds__(256) local_time_step_kernel(Zone z, Param p, const Thermo *th,
                                                               unsigned long long *dt_min_bits, bool with_reaction) {
   const Dims d = z.d;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
+  int i, j;
+  const bool node = flat_ij(d.mx, d.my, i, j);
+  const int k = blockIdx.y;
   double dt = 1e6;
-  if (i < d.mx) {
+  if (node) {
     const int g = d.ngg;
     const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
     const double *mt = z.metric;
@@ -351,9 +368,12 @@ __global__ void eliminate_k_gradient_kernel(Zone z, Param p) {
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-static dim3 interior_grid(const Dims &d, int tpb) { return dim3((d.mx + tpb - 1) / tpb, d.my, d.mz); }
+// grids for flat_ij: the (i, j) plane flattened along x, one k plane per grid.y
+static dim3 interior_grid(const Dims &d, int tpb) {
+  return dim3((unsigned)(((int64_t)d.mx * d.my + tpb - 1) / tpb), d.mz);
+}
 static dim3 padded_grid(const Dims &d, int tpb) {
-  return dim3((d.mx + 2 * d.ngg + tpb - 1) / tpb, d.my + 2 * d.ngg, d.mz + 2 * d.ngg);
+  return dim3((unsigned)(((int64_t)(d.mx + 2 * d.ngg) * (d.my + 2 * d.ngg) + tpb - 1) / tpb), d.mz + 2 * d.ngg);
 }
 
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
