@@ -164,22 +164,29 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
       if (point_ok(threadIdx.x + r * kFT, px, py)) load_point(k + 1, px, py, nxt);
     }
     __syncthreads();
-    // x faces (33 per row) and y faces (9 per column) of plane k
-    for (int f = threadIdx.x; f < kFY * (kFX + 1); f += kFT) {
-      const int fy_ = f / (kFX + 1), fx_ = f - fy_ * (kFX + 1);
-      if (i0 - 1 + fx_ > d.mx - 1 || j0 + fy_ >= d.my) continue;
-      double F[4];
-      staged_face<0>(S, cur, fx_, fy_ + 1, cur, fx_ + 1, fy_ + 1, Pr, F);
+    // x faces (33 per row) and y faces (9 per column) of plane k as one work
+    // list, the y part starting on a warp boundary, so that the faces beyond
+    // one per thread spread over two warps instead of piling onto the first
+    constexpr int kNXF = kFY * (kFX + 1), kNYF = (kFY + 1) * kFX;
+    constexpr int kYF0 = (kNXF + 31) / 32 * 32;
+    for (int f = threadIdx.x; f < kYF0 + kNYF; f += kFT) {
+      if (f < kYF0) {
+        if (f >= kNXF) continue;
+        const int fy_ = f / (kFX + 1), fx_ = f - fy_ * (kFX + 1);
+        if (i0 - 1 + fx_ > d.mx - 1 || j0 + fy_ >= d.my) continue;
+        double F[4];
+        staged_face<0>(S, cur, fx_, fy_ + 1, cur, fx_ + 1, fy_ + 1, Pr, F);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) S.fx[q][fy_][fx_] = F[q];
-    }
-    for (int f = threadIdx.x; f < (kFY + 1) * kFX; f += kFT) {
-      const int fy_ = f / kFX, fx_ = f - fy_ * kFX;
-      if (i0 + fx_ >= d.mx || j0 - 1 + fy_ > d.my - 1) continue;
-      double F[4];
-      staged_face<1>(S, cur, fx_ + 1, fy_, cur, fx_ + 1, fy_ + 1, Pr, F);
+        for (int q = 0; q < 4; ++q) S.fx[q][fy_][fx_] = F[q];
+      } else {
+        const int e = f - kYF0;
+        const int fy_ = e / kFX, fx_ = e - fy_ * kFX;
+        if (i0 + fx_ >= d.mx || j0 - 1 + fy_ > d.my - 1) continue;
+        double F[4];
+        staged_face<1>(S, cur, fx_ + 1, fy_, cur, fx_ + 1, fy_ + 1, Pr, F);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) S.fy[q][fy_][fx_] = F[q];
+        for (int q = 0; q < 4; ++q) S.fy[q][fy_][fx_] = F[q];
+      }
     }
     double fzn[4] = {0, 0, 0, 0};
     if (three_d && mine) {
