@@ -62,88 +62,40 @@ struct AirTile {
 
 }  // namespace
 
-// HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
-// VAR: tile shape (TileShape).
-template <int DIR, int ORD, bool HYB, int VAR>
-__global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_ref, const double *sensor,
-                                                              double threshold) {
-  using T = AirTile<DIR, ORD, VAR>;
-  constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
-  extern __shared__ double sm[];
-  double *spts = sm;
-  double *sflx = sm + kNQ * C * NPT;
+// The 13 staged values of one stencil point from its conserved variables,
+// p, T, the sweep's metric row and J.
+template <class T>
+__device__ __forceinline__ void air_stage_point(double *s, int c, int t, double q0, double q1, double q2, double q3,
+                                                double q4, double pk, double tk, double m0, double m1, double m2,
+                                                double jac) {
+  const double Uk = (q1 * m0 + q2 * m1 + q3 * m2) / q0;
+  const double cGradK = norm3d(m0, m1, m2) * sqrt(kGammaAir * kRAir * tk);
+  s[T::spt(0, c, t)] = q0;
+  s[T::spt(1, c, t)] = q1;
+  s[T::spt(2, c, t)] = q2;
+  s[T::spt(3, c, t)] = q3;
+  s[T::spt(4, c, t)] = q4;
+  s[T::spt(5, c, t)] = q0 * Uk;
+  s[T::spt(6, c, t)] = fma(q1, Uk, pk * m0);
+  s[T::spt(7, c, t)] = fma(q2, Uk, pk * m1);
+  s[T::spt(8, c, t)] = fma(q3, Uk, pk * m2);
+  s[T::spt(9, c, t)] = (q4 + pk) * Uk;
+  s[T::spt(10, c, t)] = pk;
+  s[T::spt(11, c, t)] = 0.5 * jac;
+  s[T::spt(12, c, t)] = abs(Uk) + cGradK;
+}
 
-  const Dims d = z.d;
-  const int g = d.ngg;
-  const int64_t sz = d.plane(g), szq = d.plane(0);
-  const int m = d.ext(DIR);
-
-  // tile origin: n0 along DIR, column origin across
-  int n0, cbase, cfix;
-  if (DIR == 0) { n0 = blockIdx.x * TN; cbase = blockIdx.y * C; cfix = blockIdx.z; }
-  else { n0 = blockIdx.y * TN; cbase = blockIdx.x * C; cfix = blockIdx.z; }
-  const int ncol_max = DIR == 0 ? d.my : d.mx;
-
-  auto node_idx = [&](int g_, int c, int a) -> int64_t {
-    const int cc = cbase + c;
-    if (DIR == 0) return d.idx(g_, a, cc, cfix);
-    if (DIR == 1) return d.idx(g_, cc, a, cfix);
-    return d.idx(g_, cc, cfix, a);
-  };
-  auto split = [&](int item, int n_t, int &c, int &t) {
-    if (DIR == 0) { c = item / n_t; t = item - c * n_t; }
-    else { t = item / C; c = item - t * C; }
-  };
-
-  const int mmo = 3 * DIR;  // metric offset of this direction's grad(xi_dir)
-  // ---- stage ------------------------------------------------------------
-  for (int item = threadIdx.x; item < NPT * C; item += T::NT) {
-    int c, t;
-    split(item, NPT, c, t);
-    const int a = n0 - 1 - R + t;
-    if (cbase + c >= ncol_max || a > m + R) continue;
-    const int64_t id = node_idx(g, c, a);
-    const double q0 = z.cv[id], q1 = z.cv[id + sz], q2 = z.cv[id + 2 * sz], q3 = z.cv[id + 3 * sz],
-                 q4 = z.cv[id + 4 * sz];
-    const double pk = z.bv[id + 4 * sz], tk = z.bv[id + 5 * sz];
-    const double m0 = z.metric[id + mmo * sz], m1 = z.metric[id + (mmo + 1) * sz],
-                 m2 = z.metric[id + (mmo + 2) * sz];
-    const double jac = z.jac[id];
-    const double Uk = (q1 * m0 + q2 * m1 + q3 * m2) / q0;
-    const double cGradK = norm3d(m0, m1, m2) * sqrt(kGammaAir * kRAir * tk);
-    double *s = spts;
-    s[T::spt(0, c, t)] = q0;
-    s[T::spt(1, c, t)] = q1;
-    s[T::spt(2, c, t)] = q2;
-    s[T::spt(3, c, t)] = q3;
-    s[T::spt(4, c, t)] = q4;
-    s[T::spt(5, c, t)] = q0 * Uk;
-    s[T::spt(6, c, t)] = fma(q1, Uk, pk * m0);
-    s[T::spt(7, c, t)] = fma(q2, Uk, pk * m1);
-    s[T::spt(8, c, t)] = fma(q3, Uk, pk * m2);
-    s[T::spt(9, c, t)] = (q4 + pk) * Uk;
-    s[T::spt(10, c, t)] = pk;
-    s[T::spt(11, c, t)] = 0.5 * jac;
-    s[T::spt(12, c, t)] = abs(Uk) + cGradK;
-  }
-  __syncthreads();
-
-  // ---- face fluxes ------------------------------------------------------
+// Flux of the face between local points t + R and t + R + 1 of column c:
+// Roe average, characteristic basis, Lax-Friedrichs split of the 2R + 2
+// staged points, WENO (or, away from shocks in the hybrid scheme, the linear
+// upwind stencils) and back projection into sflx.  kx, ky, kz: the face
+// normal before normalisation.
+template <int ORD, class T>
+__device__ __forceinline__ void air_face(const double *s, double *sflx, int c, int t, double kx, double ky, double kz,
+                                         double eps_ref, bool shock) {
+  constexpr int R = T::R, NPF = T::NPF;
   constexpr double gm1 = kGammaAir - 1;
-  for (int item = threadIdx.x; item < NF * C; item += T::NT) {
-    int c, t;
-    split(item, NF, c, t);
-    const int f = n0 - 1 + t;  // face between node f and f+1 along DIR
-    if (cbase + c >= ncol_max || f > m - 1) continue;
-    const double *s = spts;
-    const int pc = t + R;  // local point of node f
-    // face normal, averaged with the (i+1) node in every direction as the
-    // reference does (reference src/WENO.cu:886-888, 1627-1629, 2303-2305)
-    const int64_t idf = node_idx(g, c, f);
-    double kx = 0.5 * (z.metric[idf + mmo * sz] + z.metric[idf + 1 + mmo * sz]);
-    double ky = 0.5 * (z.metric[idf + (mmo + 1) * sz] + z.metric[idf + 1 + (mmo + 1) * sz]);
-    double kz = 0.5 * (z.metric[idf + (mmo + 2) * sz] + z.metric[idf + 1 + (mmo + 2) * sz]);
-
+  const int pc = t + R;  // local point of node f
     const double rho_l = s[T::spt(0, c, pc)], rho_r = s[T::spt(0, c, pc + 1)];
     double temp1 = sqrt(rho_l * rho_r);
     const double rlc = 1 / (rho_l + temp1);
@@ -173,7 +125,6 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
     double lam = 0;
 #pragma unroll
     for (int q = 0; q < NPF; ++q) lam = max(lam, s[T::spt(12, c, t + q)]);
-    const bool shock = !HYB || face_shocked(sensor, idf, d.stride(g, DIR), g, threshold);
 
     double fChar[5];
 #pragma unroll
@@ -230,6 +181,74 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
     sflx[T::sfl(2, c, t)] = vm * f034 - ky * cm * f04 + ny * fChar[1] + qy * fChar[2];
     sflx[T::sfl(3, c, t)] = wm * f034 - kz * cm * f04 + nz * fChar[1] + qz * fChar[2];
     sflx[T::sfl(4, c, t)] = H * f034 - Uk_bar * cm * f04 + Un * fChar[1] + Uq * fChar[2] - cm * cm / gm1 * fChar[3];
+  }
+
+// HYB: hybrid UD/WENO scheme, the face switches on the shock sensor.
+// VAR: tile shape (TileShape).
+template <int DIR, int ORD, bool HYB, int VAR>
+__global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_ref, const double *sensor,
+                                                              double threshold) {
+  using T = AirTile<DIR, ORD, VAR>;
+  constexpr int R = T::R, NPF = T::NPF, TN = T::TN, C = T::C, NF = T::NF, NPT = T::NPT;
+  extern __shared__ double sm[];
+  double *spts = sm;
+  double *sflx = sm + kNQ * C * NPT;
+
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), szq = d.plane(0);
+  const int m = d.ext(DIR);
+
+  // tile origin: n0 along DIR, column origin across
+  int n0, cbase, cfix;
+  if (DIR == 0) { n0 = blockIdx.x * TN; cbase = blockIdx.y * C; cfix = blockIdx.z; }
+  else { n0 = blockIdx.y * TN; cbase = blockIdx.x * C; cfix = blockIdx.z; }
+  const int ncol_max = DIR == 0 ? d.my : d.mx;
+
+  auto node_idx = [&](int g_, int c, int a) -> int64_t {
+    const int cc = cbase + c;
+    if (DIR == 0) return d.idx(g_, a, cc, cfix);
+    if (DIR == 1) return d.idx(g_, cc, a, cfix);
+    return d.idx(g_, cc, cfix, a);
+  };
+  auto split = [&](int item, int n_t, int &c, int &t) {
+    if (DIR == 0) { c = item / n_t; t = item - c * n_t; }
+    else { t = item / C; c = item - t * C; }
+  };
+
+  const int mmo = 3 * DIR;  // metric offset of this direction's grad(xi_dir)
+  // ---- stage ------------------------------------------------------------
+  for (int item = threadIdx.x; item < NPT * C; item += T::NT) {
+    int c, t;
+    split(item, NPT, c, t);
+    const int a = n0 - 1 - R + t;
+    if (cbase + c >= ncol_max || a > m + R) continue;
+    const int64_t id = node_idx(g, c, a);
+    const double q0 = z.cv[id], q1 = z.cv[id + sz], q2 = z.cv[id + 2 * sz], q3 = z.cv[id + 3 * sz],
+                 q4 = z.cv[id + 4 * sz];
+    const double pk = z.bv[id + 4 * sz], tk = z.bv[id + 5 * sz];
+    const double m0 = z.metric[id + mmo * sz], m1 = z.metric[id + (mmo + 1) * sz],
+                 m2 = z.metric[id + (mmo + 2) * sz];
+    const double jac = z.jac[id];
+    air_stage_point<T>(spts, c, t, q0, q1, q2, q3, q4, pk, tk, m0, m1, m2, jac);
+  }
+  __syncthreads();
+
+  // ---- face fluxes ------------------------------------------------------
+  for (int item = threadIdx.x; item < NF * C; item += T::NT) {
+    int c, t;
+    split(item, NF, c, t);
+    const int f = n0 - 1 + t;  // face between node f and f+1 along DIR
+    if (cbase + c >= ncol_max || f > m - 1) continue;
+    // face normal, averaged with the (i+1) node in every direction as the
+    // reference does (reference src/WENO.cu:886-888, 1627-1629, 2303-2305)
+    const int64_t idf = node_idx(g, c, f);
+    double kx = 0.5 * (z.metric[idf + mmo * sz] + z.metric[idf + 1 + mmo * sz]);
+    double ky = 0.5 * (z.metric[idf + (mmo + 1) * sz] + z.metric[idf + 1 + (mmo + 1) * sz]);
+    double kz = 0.5 * (z.metric[idf + (mmo + 2) * sz] + z.metric[idf + 1 + (mmo + 2) * sz]);
+
+    const bool shock = !HYB || face_shocked(sensor, idf, d.stride(g, DIR), g, threshold);
+    air_face<ORD, T>(spts, sflx, c, t, kx, ky, kz, eps_ref, shock);
   }
   __syncthreads();
 
