@@ -238,6 +238,26 @@ def perturbed(case: Case, seed: int = 0, amp: float = 1e-3) -> Case:
     return dataclasses.replace(case, bv=bv)
 
 
+def with_walls(case: Case, thermal_type: int = 0, temperature: float | None = None, catalytic_type: int = 0,
+               yk=None, faces=((1, -1), (1, 1))) -> Case:
+    """Copy of `case` whose listed (face, direction) boundaries are no-slip
+    walls (label 2): thermal_type 0 isothermal at `temperature` (default 0.95
+    of the mean temperature of the initial field), 1 adiabatic; for mixtures
+    catalytic_type 1 holds the wall at mass fractions `yk`."""
+    walls = set(faces)
+    new_faces = [(f, d, 2 if (f, d) in walls else lab) for f, d, lab in case.faces]
+    for f, d in walls:
+        if not any((f, d) == (a, b) for a, b, _ in case.faces):
+            new_faces.append((f, d, 2))
+    param = dict(case.param)
+    if temperature is None:
+        temperature = 0.95 * float(np.mean(case.bv[5]))
+    param.update(wall_thermal_type=thermal_type, wall_temperature=temperature, wall_catalytic_type=catalytic_type)
+    if yk is not None:
+        param["wall_yk"] = list(yk)
+    return dataclasses.replace(case, param=param, faces=new_faces, name=case.name + "_walls")
+
+
 def _gas_constant(case: Case) -> np.ndarray:
     """Specific gas constant per padded node: air, or R_u sum Y_k / W_k."""
     if case.mech is None:

@@ -17,6 +17,11 @@ class cfk_face(ctypes.Structure):
     _fields_ = [("face", ctypes.c_int), ("direction", ctypes.c_int), ("label", ctypes.c_int)]
 
 
+class cfk_wall(ctypes.Structure):
+    _fields_ = [("thermal_type", ctypes.c_int), ("catalytic_type", ctypes.c_int), ("temperature", ctypes.c_double),
+                ("yk", ctypes.c_double * 9)]
+
+
 class cfk_param(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
@@ -28,6 +33,7 @@ class cfk_param(ctypes.Structure):
         ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("weno_eps_scale", ctypes.c_double),
         ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double), ("sensor_threshold", ctypes.c_double),
         ("device", ctypes.c_int), ("shock_sensor", ctypes.c_int), ("sensor_eps", ctypes.c_double),
+        ("wall", cfk_wall),
     ]
 
 
@@ -190,7 +196,12 @@ def lib() -> ctypes.CDLL:
 def make_param(p: dict, faces) -> cfk_param:
     cp = cfk_param()
     for k, v in p.items():
-        if k in dict(cfk_param._fields_):
+        if k == "wall_yk":
+            for l, y in enumerate(v):
+                cp.wall.yk[l] = y
+        elif k.startswith("wall_"):
+            setattr(cp.wall, k[5:], v)
+        elif k in dict(cfk_param._fields_):
             setattr(cp, k, v)
     cp.n_face = len(faces)
     for n, (f, dr, lab) in enumerate(faces):

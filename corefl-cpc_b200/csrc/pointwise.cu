@@ -349,6 +349,77 @@ __global__ void bc_periodic_kernel(Zone z, Param p, const Thermo *th, FaceGeom f
   }
 }
 
+// apply_wall (reference src/BoundCond.cu:2761-3031) without its jet,
+// shock-blowing and wall-fluctuation branches (so v_blow = 0).  The face node
+// takes zero velocity, its inner neighbour's pressure, the wall temperature
+// (isothermal) or the inner neighbour's temperature (adiabatic), the inner
+// neighbour's mass fractions (non-catalytic) or the wall's (catalytic) and
+// rho = p / (R T).  Ghost layer gg mirrors inner node gg: velocity reversed,
+// pressure copied, temperature copied (adiabatic) or reflected about the wall
+// temperature, T_g = 2 T_w - T_i, replaced by T_w at or below 0.1 T_w
+// (isothermal).  A catalytic ghost's gas constant is the wall's, summed from
+// yk in the order the reference sums the face node's fractions, so the ghost
+// parts never read the face node that part 0 writes.
+template <bool MIX>
+__global__ void bc_wall_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg, cfk_wall wall) {
+  const Dims d = z.d;
+  const int g = d.ngg;
+  int i, j, k, gg_lo, gg_hi;
+  bool face_part;
+  if (!face_work(fg, g, i, j, k, gg_lo, gg_hi, face_part)) return;
+  const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+  const int64_t s = d.stride(g, fg.face) * fg.direction;
+  const bool isothermal = wall.thermal_type == 0;
+  const bool catalytic = MIX && wall.catalytic_type == 1;
+  if (face_part) {
+    const int64_t in = id - s;
+    const double t_wall = isothermal ? wall.temperature : z.bv[in + 5 * sz];
+    const double pw = z.bv[in + 4 * sz];
+    double R = kRAir;
+    if (MIX) {
+      R = 0;
+      for (int l = 0; l < p.n_spec; ++l) {
+        const double y = catalytic ? wall.yk[l] : z.sv[in + l * sz];
+        z.sv[id + l * sz] = y;
+        R += y * th->gas_const[l];
+      }
+    }
+    z.bv[id] = pw / (t_wall * R);
+    z.bv[id + sz] = 0;
+    z.bv[id + 2 * sz] = 0;
+    z.bv[id + 3 * sz] = 0;
+    z.bv[id + 4 * sz] = pw;
+    z.bv[id + 5 * sz] = t_wall;
+    cv_from_bv_point<MIX>(z, p, th, id);
+  }
+  const double v_blow = 0;
+  for (int gg = gg_lo; gg <= gg_hi; ++gg) {
+    const int64_t gi = id + gg * s, ii = id - gg * s;
+    const double p_i = z.bv[ii + 4 * sz], t_i = z.bv[ii + 5 * sz];
+    double t_g = t_i;
+    if (isothermal) {
+      t_g = 2 * wall.temperature - t_i;
+      if (t_g <= 0.1 * wall.temperature) t_g = wall.temperature;
+    }
+    double R = kRAir;
+    if (MIX) {
+      R = 0;
+      for (int l = 0; l < p.n_spec; ++l) {
+        const double y = catalytic ? wall.yk[l] : z.sv[ii + l * sz];
+        z.sv[gi + l * sz] = y;
+        R += y * th->gas_const[l];
+      }
+    }
+    z.bv[gi] = p_i / (t_g * R);
+    z.bv[gi + sz] = -z.bv[ii + sz];
+    z.bv[gi + 2 * sz] = v_blow * 2 - z.bv[ii + 2 * sz];
+    z.bv[gi + 3 * sz] = -z.bv[ii + 3 * sz];
+    z.bv[gi + 4 * sz] = p_i;
+    z.bv[gi + 5 * sz] = t_g;
+    cv_from_bv_point<MIX>(z, p, th, gi);
+  }
+}
+
 // eliminate_k_gradient (reference src/FieldOperation.cu:47-72)
 __global__ void eliminate_k_gradient_kernel(Zone z, Param p) {
   const Dims d = z.d;
@@ -426,9 +497,9 @@ static FaceGeom make_face(const Dims &d, const cfk_face &f) {
 }
 
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
-                                       int n_face, cudaStream_t st, int *n_launch) {
-  static const int order[3] = {6, 3, 8};  // outflow, symmetry, periodic (reference priority order)
-  for (int o = 0; o < 3; ++o) {
+                                       int n_face, const cfk_wall &wall, cudaStream_t st, int *n_launch) {
+  static const int order[4] = {6, 3, 2, 8};  // outflow, symmetry, wall, periodic (reference priority order)
+  for (int o = 0; o < 4; ++o) {
     for (int n = 0; n < n_face; ++n) {
       if (faces[n].label != order[o]) continue;
       const FaceGeom fg = make_face(z.d, faces[n]);
@@ -441,6 +512,9 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
       } else if (order[o] == 3) {
         if (mix) bc_symmetry_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
         else bc_symmetry_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);
+      } else if (order[o] == 2) {
+        if (mix) bc_wall_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg, wall);
+        else bc_wall_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg, wall);
       } else {
         if (mix) bc_periodic_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
         else bc_periodic_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);

@@ -111,6 +111,39 @@ double struct_real(const Struct &st, const char *k, double dflt) {
   return dflt;
 }
 
+std::string struct_string(const Struct &st, const char *k) {
+  auto it = st.find(k);
+  if (it == st.end()) return std::string();
+  if (auto p = std::get_if<std::string>(&it->second)) return *p;
+  return std::string();
+}
+
+// The wall condition of the boundary_conditions list (reference
+// src/BoundCond.cpp:480-528, Wall::Wall): thermal_type isothermal (default,
+// also for an unknown name, as there), adiabatic or equilibrium_radiation
+// (kept as 2, which cfk_create rejects); temperature defaults to 300 K.
+// Returns false when more than one wall struct is listed.
+bool read_wall(const Setup &s, cfk_wall &w, std::string &err) {
+  w.thermal_type = 0;
+  w.catalytic_type = 0;
+  w.temperature = 300.0;
+  auto list = s.arrays.find("boundary_conditions");
+  if (list == s.arrays.end()) return true;
+  int n_wall = 0;
+  for (const std::string &name : list->second) {
+    auto it = s.structs.find(name);
+    if (it == s.structs.end() || struct_string(it->second, "type") != "wall") continue;
+    if (++n_wall > 1) {
+      err = "more than one wall condition in boundary_conditions; cfk_param carries one";
+      return false;
+    }
+    const std::string t = struct_string(it->second, "thermal_type");
+    w.thermal_type = t == "adiabatic" ? 1 : t == "equilibrium_radiation" ? 2 : 0;
+    w.temperature = struct_real(it->second, "temperature", 300.0);
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char *errbuf, size_t err_len) {
@@ -169,6 +202,7 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
     p.v_ref = std::fabs(velocity) < 1 ? c : velocity;
   }
   p.weno_eps_scale = p.rho_ref * p.v_ref * p.rho_ref * p.v_ref;
+  if (!read_wall(s, p.wall, err)) return report(err);
   p.n_face = 0;
   *out = p;
   return CFK_OK;

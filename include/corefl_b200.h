@@ -35,12 +35,28 @@ enum cfk_status {
 
 typedef struct cfk_ctx cfk_ctx;
 
+#define CFK_MAX_SPEC 9   /* species of a mechanism (cfk_mechanism, cfk_wall) */
+#define CFK_MAX_REAC 24  /* reactions of a mechanism */
+
 /* A boundary face of the block (reference src/Mesh.cpp:14-31, Boundary).
  * face 0/1/2 = i/j/k, direction -1 = min side, +1 = max side;
- * label 6 = outflow, 8 = periodic, 3 = symmetry. */
+ * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall (cfk_param.wall). */
 typedef struct cfk_face {
   int face, direction, label;
 } cfk_face;
+
+/* The no-slip wall of the faces labelled 2 (reference src/BoundCond.h:88-125,
+ * Wall, as read by src/BoundCond.cpp:480-528).  thermal_type 0 isothermal at
+ * `temperature`, 1 adiabatic (the reference's third type, equilibrium
+ * radiation, needs the wall-distance field and is rejected).  catalytic_type
+ * (mixtures only; ignored for air, as in the reference) 0 non-catalytic —
+ * the wall takes its inner neighbour's mass fractions — or 1 fully catalytic
+ * with the wall mass fractions yk[0..n_spec). */
+typedef struct cfk_wall {
+  int thermal_type, catalytic_type;
+  double temperature;
+  double yk[CFK_MAX_SPEC];
+} cfk_wall;
 
 /* Scalar settings of the path: the DParameter fields it reads
  * (reference src/DParameter.cuh:13-207) plus the boundary list. */
@@ -69,6 +85,7 @@ typedef struct cfk_param {
   int device;              /* CUDA device ordinal the context runs on */
   int shock_sensor;        /* 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump */
   double sensor_eps;       /* shockSensor_epsilon (reference default -1) */
+  cfk_wall wall;           /* read for faces labelled 2 */
 } cfk_param;
 
 /* Device pointers of one block, field for field the arrays of the reference's
@@ -92,8 +109,6 @@ typedef struct cfk_zone {
  * reac_type: 0 irreversible, 1 elementary, 3 merged duplicate, 4 third body,
  * 5 Lindemann, 6/7 Troe with 3/4 parameters; rev_type 1 = explicit reverse
  * Arrhenius (REV).  Ea and Ea2 are in K (already divided by R_c). */
-#define CFK_MAX_SPEC 9
-#define CFK_MAX_REAC 24
 typedef struct cfk_mechanism {
   int n_spec, n_reac;
   double mw[CFK_MAX_SPEC];
@@ -165,8 +180,8 @@ int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);
 int cfk_update_physical_properties(cfk_ctx *ctx, void *stream);
 /* Replaces compute_cv_from_bv<M> (reference src/FieldOperation.cuh:39-64). */
 int cfk_compute_cv_from_bv(cfk_ctx *ctx, void *stream);
-/* Replaces DBoundCond::apply_boundary_conditions<M> for outflow, symmetry and
- * periodic faces (reference src/BoundCond.cu:3489-3619) and, for 2-D blocks,
+/* Replaces DBoundCond::apply_boundary_conditions<M> for outflow, symmetry, wall
+ * and periodic faces (reference src/BoundCond.cu:3489-3619) and, for 2-D blocks,
  * eliminate_k_gradient (reference src/FieldOperation.cu:47-72). */
 int cfk_apply_boundary_conditions(cfk_ctx *ctx, void *stream);
 /* Local CFL step into dt_local and its minimum.  Replaces local_time_step<M>

@@ -823,7 +823,8 @@ double orc_global_time_step(const orc_zone *z) {
 
 /* ------------------------------------------------------------------------ */
 /* Boundary conditions: outflow (src/BoundCond.cu:2065-2171, plain branch),  */
-/* periodic (src/BoundCond.cu:3033-3080), symmetry (src/BoundCond.cu:2002)   */
+/* periodic (src/BoundCond.cu:3033-3080), symmetry (src/BoundCond.cu:2002),  */
+/* no-slip wall (src/BoundCond.cu:2761-3031)                                 */
 /* applied per label in the reference's priority order                       */
 /* (src/BoundCond.cu:3489-3619): outflow, inflow, symmetry, wall, periodic.  */
 /* Each face covers its tangential range widened by ngg ghosts               */
@@ -898,14 +899,87 @@ static void apply_periodic_face(orc_zone *z, const orc_param *p, const orc_face 
       }
 }
 
+/* apply_wall (src/BoundCond.cu:2761-3031) without its jet, shock-blowing and
+ * wall-fluctuation branches (so v_blow = 0).  The boundary node takes zero
+ * velocity, its inner neighbour's pressure, the wall temperature (isothermal)
+ * or the inner neighbour's temperature (adiabatic), the mass fractions of the
+ * inner neighbour (non-catalytic) or of the wall (catalytic), and
+ * rho = p / (R T).  Ghost layer g mirrors inner node g: velocity reversed,
+ * pressure copied, temperature copied (adiabatic) or reflected about the wall
+ * temperature, T_g = 2 T_w - T_i, replaced by T_w when at or below 0.1 T_w
+ * (isothermal).  As in the reference the catalytic ghosts' gas constant is
+ * summed from the boundary node's (just written) mass fractions. */
+static void apply_wall_face(orc_zone *z, const orc_param *p, const orc_face *f) {
+  const int g = z->ngg;
+  const long sz = psz(z, g);
+  int lo[3], hi[3];
+  face_range(z, f, lo, hi);
+  const long s = pstride(z, g, f->face) * f->direction;
+  const int ns = p->mech ? p->n_spec : 0;
+  const int catalytic = ns > 0 && p->wall_catalytic_type == 1;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        const long id = pidx(z, g, i, j, k), in = id - s;
+        double *bv = z->bv, *sv = z->sv;
+        const double t_wall = p->wall_thermal_type == 0 ? p->wall_temperature : bv[in + 5 * sz];
+        const double pw = bv[in + 4 * sz];
+        double R = R_AIR;
+        if (ns > 0) {
+          R = 0;
+          for (int l = 0; l < ns; ++l) {
+            sv[id + l * sz] = catalytic ? p->wall_yk[l] : sv[in + l * sz];
+            R += sv[id + l * sz] * p->mech->gas_const[l];
+          }
+        }
+        bv[id] = pw / (t_wall * R);
+        bv[id + sz] = 0;
+        bv[id + 2 * sz] = 0;
+        bv[id + 3 * sz] = 0;
+        bv[id + 4 * sz] = pw;
+        bv[id + 5 * sz] = t_wall;
+        cv_from_bv_point(z, p, id);
+        const double v_blow = 0;
+        for (int gg = 1; gg <= g; ++gg) {
+          const long ii = id - gg * s, gi = id + gg * s;
+          const double p_i = bv[ii + 4 * sz], t_i = bv[ii + 5 * sz];
+          double t_g = t_i;
+          if (p->wall_thermal_type == 0) {
+            t_g = 2 * t_wall - t_i;
+            if (t_g <= 0.1 * t_wall) t_g = t_wall;
+          }
+          if (ns > 0) {
+            R = 0;
+            for (int l = 0; l < ns; ++l) {
+              if (catalytic) {
+                sv[gi + l * sz] = p->wall_yk[l];
+                R += sv[id + l * sz] * p->mech->gas_const[l];
+              } else {
+                sv[gi + l * sz] = sv[ii + l * sz];
+                R += sv[ii + l * sz] * p->mech->gas_const[l];
+              }
+            }
+          }
+          bv[gi] = p_i / (t_g * R);
+          bv[gi + sz] = -bv[ii + sz];
+          bv[gi + 2 * sz] = v_blow * 2 - bv[ii + 2 * sz];
+          bv[gi + 3 * sz] = -bv[ii + 3 * sz];
+          bv[gi + 4 * sz] = p_i;
+          bv[gi + 5 * sz] = t_g;
+          cv_from_bv_point(z, p, gi);
+        }
+      }
+}
+
 void orc_apply_boundary_conditions(orc_zone *z, const orc_param *p) {
-  static const int order[] = {6, 3, 8};
-  for (int o = 0; o < 3; ++o)
+  static const int order[] = {6, 3, 2, 8};
+  for (int o = 0; o < 4; ++o)
     for (int n = 0; n < p->n_face; ++n) {
       const orc_face *f = &p->faces[n];
       if (f->label != order[o]) continue;
       if (f->label == 6) apply_outflow_face(z, p, f);
       else if (f->label == 3) apply_symmetry_face(z, p, f);
+      else if (f->label == 2) apply_wall_face(z, p, f);
       else if (f->label == 8) apply_periodic_face(z, p, f);
     }
 }

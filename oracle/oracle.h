@@ -24,7 +24,7 @@ extern "C" {
 
 /* Boundary face description (reference src/Mesh.cpp:14-31 register_boundary):
  * face 0/1/2 = i/j/k, direction -1 (min side) or +1 (max side),
- * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = adiabatic wall. */
+ * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall. */
 typedef struct {
   int face, direction, label;
 } orc_face;
@@ -90,6 +90,12 @@ typedef struct {
   const orc_mech *mech;  /* NULL for the calorically perfect air model */
   int shock_sensor;      /* 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump */
   double sensor_eps;     /* shockSensor_epsilon */
+  /* the wall of the faces labelled 2 (src/BoundCond.h:88-125): thermal type
+   * 0 isothermal at wall_temperature, 1 adiabatic; catalytic type (mixtures)
+   * 0 non-catalytic, 1 fully catalytic with mass fractions wall_yk */
+  int wall_thermal_type, wall_catalytic_type;
+  double wall_temperature;
+  double wall_yk[ORC_MAX_SPEC];
 } orc_param;
 
 /* zone memory management (host, zero-filled) */

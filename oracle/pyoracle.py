@@ -40,7 +40,8 @@ class orc_param(ctypes.Structure):
         ("weno_eps_scale", ctypes.c_double), ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double),
         ("sensor_threshold", ctypes.c_double), ("chem_advance_method", ctypes.c_int), ("n_face", ctypes.c_int),
         ("faces", orc_face * 6), ("mech", ctypes.c_void_p), ("shock_sensor", ctypes.c_int),
-        ("sensor_eps", ctypes.c_double),
+        ("sensor_eps", ctypes.c_double), ("wall_thermal_type", ctypes.c_int), ("wall_catalytic_type", ctypes.c_int),
+        ("wall_temperature", ctypes.c_double), ("wall_yk", ctypes.c_double * 20),
     ]
 
 
@@ -185,7 +186,10 @@ class OracleZone:
             setattr(self.z, k, _ptr(a))
         self.p = orc_param()
         for k, v in c.param.items():
-            if k in dict(orc_param._fields_):
+            if k == "wall_yk":
+                for l, y in enumerate(v):
+                    self.p.wall_yk[l] = y
+            elif k in dict(orc_param._fields_):
                 setattr(self.p, k, v)
         self.p.n_face = len(c.faces)
         for n, (f, d, lab) in enumerate(c.faces):

@@ -125,7 +125,9 @@ def test_param_from_setup_reads_reference_keys(tmp_path):
         "int shock_sensor = 1\n"
         "real shockSensor_threshold = 0.02\n"
         "real shockSensor_epsilon = 1e-6\n"
-        "array string boundary_conditions {\n  outflow\n}\n"
+        "array string boundary_conditions {\n  outflow wall\n}\n"
+        "struct wall {\n    string type = wall\n    int label = 2\n    string  thermal_type    =   isothermal"
+        "  // isothermal or adiabatic\n    real    temperature     =   322\n}\n"
         "string reference_state = left\n"
         "struct  left {\n    string type = inflow\n    int label = 5\n    real velocity = 0\n"
         "    real pressure = 1\n    real density = 1\n}\n")
@@ -136,6 +138,7 @@ def test_param_from_setup_reads_reference_keys(tmp_path):
     assert p.inviscid_scheme == 52 and p.viscous_order == 0 and p.cfl == 0.5 and p.fixed_dt == 0
     assert p.n_var == 5 and p.Pr == 0.72
     assert p.shock_sensor == 1 and p.sensor_threshold == 0.02 and p.sensor_eps == 1e-6
+    assert p.wall.thermal_type == 0 and p.wall.temperature == 322.0
     # |u| < 1, so v_ref is the speed of sound sqrt(gamma p / rho)
     assert p.v_ref == pytest.approx(np.sqrt(1.4), rel=1e-12)
     assert p.weno_eps_scale == pytest.approx(1.4, rel=1e-12)
