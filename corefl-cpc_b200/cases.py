@@ -258,6 +258,46 @@ def with_walls(case: Case, thermal_type: int = 0, temperature: float | None = No
     return dataclasses.replace(case, param=param, faces=new_faces, name=case.name + "_walls")
 
 
+def split_i(case: Case, h: int, periodic_i: bool | None = None):
+    """Two blocks cut from `case` along i, sharing the node plane i = h:
+    A holds nodes 0..h, B nodes h..mx-1.  Every padded array is sliced from
+    the whole block's, so both blocks carry exactly its metrics and state.
+    Returns (A, B, links) where links lists the inner faces as the mesh's
+    inner-interface records: (block, src, tar, target_block), block 0-based,
+    ranges and target_block 1-based as the reference's inner%4d.txt holds them.
+    The cut is an inner face; if the i faces of `case` are periodic
+    (periodic_i None: read from case.faces), A's i-min and B's i-max faces
+    become an inner face too, else they keep the case's i-face labels."""
+    g = case.ngg
+    if periodic_i is None:
+        periodic_i = any(f == 0 and lab == 8 for f, _, lab in case.faces)
+    shape = lambda a: a.reshape(a.shape[:-1] + (case.mz + 2 * g, case.my + 2 * g, case.mx + 2 * g))
+
+    def cut(a, lo, hi):
+        if a is None:
+            return None
+        b = shape(a)[..., lo:hi + 2 * g + 1]
+        return np.ascontiguousarray(b.reshape(a.shape[:-1] + (b.shape[-3] * b.shape[-2] * b.shape[-1],)))
+
+    def block(lo, hi, keep):
+        faces = [fc for fc in case.faces if fc[0] != 0 or (not periodic_i and (fc[0], fc[1]) == keep)]
+        return dataclasses.replace(case, name=f"{case.name}_i{lo}-{hi}", mx=hi - lo + 1, metric=cut(case.metric, lo, hi),
+                                   jac=cut(case.jac, lo, hi), bv=cut(case.bv, lo, hi), sv=cut(case.sv, lo, hi),
+                                   faces=faces, x=cut(case.x, lo, hi))
+
+    A = block(0, h, (0, -1))
+    B = block(h, case.mx - 1, (0, 1))
+    my, mz = case.my, case.mz
+    if case.mz == 1:
+        rng = lambda i: [i, i, 1, my, 1, 1]
+    else:
+        rng = lambda i: [i, i, -1, -my, 1, mz]
+    links = [(0, rng(A.mx), rng(1), 2), (1, rng(1), rng(A.mx), 1)]
+    if periodic_i:
+        links += [(0, rng(1), rng(B.mx), 2), (1, rng(B.mx), rng(1), 1)]
+    return A, B, links
+
+
 def _gas_constant(case: Case) -> np.ndarray:
     """Specific gas constant per padded node: air, or R_u sum Y_k / W_k."""
     if case.mech is None:

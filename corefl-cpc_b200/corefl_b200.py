@@ -22,6 +22,16 @@ class cfk_wall(ctypes.Structure):
                 ("yk", ctypes.c_double * 9)]
 
 
+_I3 = ctypes.c_int * 3
+
+
+class cfk_inner_face(ctypes.Structure):
+    _fields_ = [("range_start", _I3), ("range_end", _I3), ("face", ctypes.c_int), ("direction", ctypes.c_int),
+                ("target_start", _I3), ("target_end", _I3), ("target_block", ctypes.c_int),
+                ("target_face", ctypes.c_int), ("target_direction", ctypes.c_int), ("src_tar", _I3),
+                ("loop_dir", _I3), ("target_loop_dir", _I3), ("n_point", _I3)]
+
+
 class cfk_param(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
@@ -154,6 +164,9 @@ def lib() -> ctypes.CDLL:
             "cfk_update_physical_properties": (i, [vp, vp]),
             "cfk_compute_cv_from_bv": (i, [vp, vp]),
             "cfk_apply_boundary_conditions": (i, [vp, vp]),
+            "cfk_eliminate_k_gradient": (i, [vp, vp]),
+            "cfk_register_inner_face": (i, [i, i, vp, vp, i, ctypes.POINTER(cfk_inner_face)]),
+            "cfk_inner_communication": (i, [vp, vp, ctypes.POINTER(cfk_inner_face), vp]),
             "cfk_local_time_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step_graph": (i, [vp, _DP, vp]),
@@ -191,6 +204,17 @@ def lib() -> ctypes.CDLL:
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def register_inner_face(dim, ngg, src, tar, target_block) -> cfk_inner_face:
+    """cfk_register_inner_face: an inner face from the two records of the
+    mesh's inner-interface file (1-based, sign-coded ranges)."""
+    f = cfk_inner_face()
+    rc = lib().cfk_register_inner_face(dim, ngg, (ctypes.c_int * 6)(*src), (ctypes.c_int * 6)(*tar), target_block,
+                                       ctypes.byref(f))
+    if rc != 0:
+        raise CfkError(f"cfk_register_inner_face({src}, {tar}) failed ({rc})")
+    return f
 
 
 def make_param(p: dict, faces) -> cfk_param:
@@ -348,6 +372,12 @@ class Context:
 
     def cv_from_bv(self, stream=None):
         self._ck(self.L.cfk_compute_cv_from_bv(self.h, stream), "cv_from_bv")
+
+    def eliminate_k_gradient(self, stream=None):
+        self._ck(self.L.cfk_eliminate_k_gradient(self.h, stream), "eliminate_k_gradient")
+
+    def inner_communication(self, target: "Context", face: cfk_inner_face, stream=None):
+        self._ck(self.L.cfk_inner_communication(self.h, target.h, ctypes.byref(face), stream), "inner_communication")
 
     def boundary_conditions(self, stream=None):
         self._ck(self.L.cfk_apply_boundary_conditions(self.h, stream), "bc")

@@ -2,6 +2,7 @@
 // RK3 steps (plain and CUDA-graph replayed) and host<->device helpers.
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -34,6 +35,9 @@ cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, uns
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
                                        int n_face, const cfk_wall &wall, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
+cudaError_t launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t st);
+cudaError_t launch_inner_communication(const Zone &z, const Zone &tz, const Param &p, const Thermo *th,
+                                       const cfk_inner_face &f, cudaStream_t st);
 cudaError_t launch_shock_sensor(const Zone &z, const Param &p, cudaStream_t st);
 cudaError_t launch_viscous8(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces, int n_face,
                             double *fvis, cudaStream_t st, int *n_launch);
@@ -571,6 +575,65 @@ int cfk_apply_boundary_conditions(cfk_ctx *c, void *stream) {
   CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, S(stream), &n),
             "boundary conditions");
   c->launches += n;
+  return CFK_OK;
+}
+
+int cfk_eliminate_k_gradient(cfk_ctx *c, void *stream) {
+  NEED_ZONE(c);
+  if (c->z.d.mz != 1) return fail(c, CFK_ERR_ARG, "eliminate_k_gradient is for 2-D blocks (mz == 1)");
+  CFK_CHECK(c, launch_eliminate_k_gradient(c->z, c->p, S(stream)), "eliminate_k_gradient");
+  c->launches += 1;
+  return CFK_OK;
+}
+
+// Host checks of an inner face: a well-formed loop, and every node it maps —
+// in this block and in the target — inside the padded arrays.  The index maps
+// are affine, so the two ends of each axis bound them.
+static int check_inner_face(const Dims &d, const Dims &td, const cfk_inner_face &f, std::string &why) {
+  if (f.face < 0 || f.face > 2 || (f.direction != 1 && f.direction != -1)) { why = "bad face/direction"; return -1; }
+  int seen = 0;
+  long long total = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (f.src_tar[a] < 0 || f.src_tar[a] > 2) { why = "src_tar must map onto axes 0..2"; return -1; }
+    seen |= 1 << f.src_tar[a];
+    if ((f.loop_dir[a] != 1 && f.loop_dir[a] != -1) || (f.target_loop_dir[a] != 1 && f.target_loop_dir[a] != -1)) {
+      why = "loop directions must be +1 or -1";
+      return -1;
+    }
+    if (f.n_point[a] < 1) { why = "n_point must be >= 1"; return -1; }
+    total *= f.n_point[a];
+  }
+  if (seen != 7) { why = "src_tar must be a permutation of the axes"; return -1; }
+  if (total > (1LL << 30)) { why = "face loop too large"; return -1; }
+  const int m[3] = {d.mx, d.my, d.mz}, tm[3] = {td.mx, td.my, td.mz};
+  for (int a = 0; a < 3; ++a) {
+    const int last = f.range_start[a] + f.loop_dir[a] * (f.n_point[a] - 1);
+    const int lo = std::min(f.range_start[a], last), hi = std::max(f.range_start[a], last);
+    if (lo < -d.ngg || hi > m[a] - 1 + d.ngg) { why = "inner face leaves this block's padded range"; return -1; }
+    const int b = f.src_tar[a];
+    const int t0 = f.target_start[a], t1 = f.target_start[a] + f.target_loop_dir[a] * f.loop_dir[b] * (f.n_point[b] - 1);
+    if (std::min(t0, t1) < -td.ngg || std::max(t0, t1) > tm[a] - 1 + td.ngg) {
+      why = "inner face leaves the target block's padded range";
+      return -1;
+    }
+    if (b == f.face && tm[a] <= td.ngg) { why = "target block not thicker than ngg along the face normal"; return -1; }
+  }
+  if (m[f.face] <= d.ngg) { why = "block not thicker than ngg along the face normal"; return -1; }
+  return 0;
+}
+
+int cfk_inner_communication(cfk_ctx *c, cfk_ctx *t, const cfk_inner_face *f, void *stream) {
+  NEED_ZONE(c);
+  if (!t || !f) return fail(c, CFK_ERR_ARG, "inner_communication: null target or face");
+  if (!t->bound) return fail(c, CFK_ERR_STATE, "inner_communication: target has no zone bound");
+  if (t->hp.device != c->hp.device) return fail(c, CFK_ERR_ARG, "inner_communication: blocks on different devices");
+  if (t->z.d.ngg != c->z.d.ngg || (t->z.d.mz == 1) != (c->z.d.mz == 1) || t->p.n_var != c->p.n_var ||
+      t->p.n_scalar != c->p.n_scalar || t->p.n_spec != c->p.n_spec)
+    return fail(c, CFK_ERR_ARG, "inner_communication: blocks differ in ngg, dimension or variables");
+  std::string why;
+  if (check_inner_face(c->z.d, t->z.d, *f, why) != 0) return fail(c, CFK_ERR_ARG, "inner_communication: " + why);
+  CFK_CHECK(c, launch_inner_communication(c->z, t->z, c->p, thermo_of(c), *f, S(stream)), "inner_communication");
+  c->launches += 1;
   return CFK_OK;
 }
 

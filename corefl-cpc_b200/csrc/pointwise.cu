@@ -420,6 +420,59 @@ __global__ void bc_wall_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg, c
   }
 }
 
+// inner_communication (reference src/DataCommunication.cu:36-102): one thread
+// per node of the face's loop (face node + ghost layers along the normal, the
+// face's own nodes across it).  Ghost nodes take the target block's primitive
+// variables.  A face node moving faster than 1e-15 is averaged with the
+// target's face node, both sides written, or takes the target's values when
+// the target node is at rest (a wall on the other side); a face node at rest
+// is left as it is.  This block's cv is recomputed at every visited node.
+// Threads write distinct nodes: ghost reads touch target nodes behind the
+// target face (at least one layer in, never a face node) and the host checks
+// that both blocks are thicker than ngg along the face normal.
+template <bool MIX>
+__global__ void inner_face_kernel(Zone z, Zone tz, Param p, const Thermo *th, cfk_inner_face f, int n_total) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_total) return;
+  const int r = t / f.n_point[0];
+  const int n[3] = {t - r * f.n_point[0], r % f.n_point[1], r / f.n_point[1]};
+  int idx[3], d_idx[3], idt[3];
+  for (int a = 0; a < 3; ++a) {
+    d_idx[a] = f.loop_dir[a] * n[a];
+    idx[a] = f.range_start[a] + d_idx[a];
+  }
+  for (int a = 0; a < 3; ++a) idt[a] = f.target_start[a] + f.target_loop_dir[a] * d_idx[f.src_tar[a]];
+  const int g = z.d.ngg;
+  const int64_t sz = z.d.plane(g), tsz = tz.d.plane(g);
+  const int64_t id = z.d.idx(g, idx[0], idx[1], idx[2]), it = tz.d.idx(g, idt[0], idt[1], idt[2]);
+  const int face_node = f.direction > 0 ? f.range_start[f.face] : f.range_end[f.face];
+  if (idx[f.face] == face_node) {
+    const double u_this = norm3d(z.bv[id + sz], z.bv[id + 2 * sz], z.bv[id + 3 * sz]);
+    if (fabs(u_this) > 1e-15) {
+      const double u_that = norm3d(tz.bv[it + tsz], tz.bv[it + 2 * tsz], tz.bv[it + 3 * tsz]);
+      if (fabs(u_that) < 1e-15) {
+        for (int l = 0; l < 6; ++l) z.bv[id + l * sz] = tz.bv[it + l * tsz];
+        for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = tz.sv[it + l * tsz];
+      } else {
+        for (int l = 0; l < 6; ++l) {
+          const double ave = 0.5 * (tz.bv[it + l * tsz] + z.bv[id + l * sz]);
+          z.bv[id + l * sz] = ave;
+          tz.bv[it + l * tsz] = ave;
+        }
+        for (int l = 0; l < p.n_scalar; ++l) {
+          const double ave = 0.5 * (tz.sv[it + l * tsz] + z.sv[id + l * sz]);
+          z.sv[id + l * sz] = ave;
+          tz.sv[it + l * tsz] = ave;
+        }
+      }
+    }
+  } else {
+    for (int l = 0; l < 6; ++l) z.bv[id + l * sz] = tz.bv[it + l * tsz];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = tz.sv[it + l * tsz];
+  }
+  cv_from_bv_point<MIX>(z, p, th, id);
+}
+
 // eliminate_k_gradient (reference src/FieldOperation.cu:47-72)
 __global__ void eliminate_k_gradient_kernel(Zone z, Param p) {
   const Dims d = z.d;
@@ -528,6 +581,20 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
     eliminate_k_gradient_kernel<<<dim3((z.d.mx + 2 * z.d.ngg + 127) / 128, z.d.my + 2 * z.d.ngg), 128, 0, st>>>(z, p);
     ++*n_launch;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t st) {
+  eliminate_k_gradient_kernel<<<dim3((z.d.mx + 2 * z.d.ngg + 127) / 128, z.d.my + 2 * z.d.ngg), 128, 0, st>>>(z, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inner_communication(const Zone &z, const Zone &tz, const Param &p, const Thermo *th,
+                                       const cfk_inner_face &f, cudaStream_t st) {
+  const int n_total = f.n_point[0] * f.n_point[1] * f.n_point[2];
+  const int blocks = (n_total + 127) / 128;
+  if (p.n_spec > 0) inner_face_kernel<true><<<blocks, 128, 0, st>>>(z, tz, p, th, f, n_total);
+  else inner_face_kernel<false><<<blocks, 128, 0, st>>>(z, tz, p, th, f, n_total);
   return cudaGetLastError();
 }
 

@@ -58,6 +58,23 @@ typedef struct cfk_wall {
   double yk[CFK_MAX_SPEC];
 } cfk_wall;
 
+/* A face this block shares with a block of the same mesh: the reference's
+ * InnerFace after register_boundary (reference src/Mesh.h:33-59,
+ * src/Mesh.cpp:39-172).  0-based node indices; range_* run over this block's
+ * face nodes and the ngg ghost layers behind them (face direction) and the
+ * face's own nodes (tangential directions, corners excluded); node n of the
+ * loop maps to target node target_start[a] + target_loop_dir[a] *
+ * d[src_tar[a]] with d[b] = loop_dir[b] * n[b].  Build it with
+ * cfk_register_inner_face. */
+typedef struct cfk_inner_face {
+  int range_start[3], range_end[3];
+  int face, direction;               /* normal axis 0/1/2; -1 min side, +1 max side */
+  int target_start[3], target_end[3];
+  int target_block, target_face, target_direction;
+  int src_tar[3], loop_dir[3], target_loop_dir[3];
+  int n_point[3];
+} cfk_inner_face;
+
 /* Scalar settings of the path: the DParameter fields it reads
  * (reference src/DParameter.cuh:13-207) plus the boundary list. */
 typedef struct cfk_param {
@@ -184,6 +201,36 @@ int cfk_compute_cv_from_bv(cfk_ctx *ctx, void *stream);
  * and periodic faces (reference src/BoundCond.cu:3489-3619) and, for 2-D blocks,
  * eliminate_k_gradient (reference src/FieldOperation.cu:47-72). */
 int cfk_apply_boundary_conditions(cfk_ctx *ctx, void *stream);
+/* eliminate_k_gradient on its own (reference src/FieldOperation.cu:47-72): a
+ * 2-D block's k = 0 plane copied into its k ghost layers.  The reference calls
+ * it after data_communication (reference src/RK.cuh:175-183), so a 2-D
+ * multi-block stage calls it again after its cfk_inner_communication calls. */
+int cfk_eliminate_k_gradient(cfk_ctx *ctx, void *stream);
+
+/* ---- multi-block meshes on one GPU ---------------------------------------- */
+/* Build an inner face from the two records of the mesh's inner-interface file
+ * (reference src/Mesh.cpp:927-958 and InnerFace::register_boundary,
+ * src/Mesh.cpp:39-172): src = this block's 1-based node range
+ * {x1, x2, y1, y2, z1, z2}, the normal axis marked by equal ends (1: min side)
+ * and, in 3-D, the first tangential axis by negated values; tar = the same
+ * for the target block, whose 1-based number is target_block (stored
+ * 0-based).  Host-only arithmetic; CFK_ERR_ARG for a record without a normal
+ * axis or, in 3-D, without a marked tangential axis. */
+int cfk_register_inner_face(int dim, int ngg, const int src[6], const int tar[6], int target_block,
+                            cfk_inner_face *out);
+/* Replaces inner_communication<M> of data_communication for one inner face
+ * (reference src/DataCommunication.cu:6-102): this block's ghost nodes behind
+ * the face take the target block's primitive variables; on the face itself
+ * the two blocks' nodes are averaged, both sides written (a node at rest — a
+ * wall — is left alone, and takes the target's values when only the target's
+ * node is at rest); this block's cv is recomputed on every node visited.
+ * `target` is the neighbouring block's context, or ctx itself; both bound on
+ * the same device with the same ngg, dimension and variable counts, and every
+ * node the face maps must lie inside both padded blocks (checked on the host,
+ * as is a face-normal extent above ngg for both blocks).  Call it per block and
+ * per face after every block's cfk_apply_boundary_conditions, in the order
+ * the reference visits them. */
+int cfk_inner_communication(cfk_ctx *ctx, cfk_ctx *target, const cfk_inner_face *face, void *stream);
 /* Local CFL step into dt_local and its minimum.  Replaces local_time_step<M>
  * + global_time_step (reference src/TimeAdvanceFunc.cuh:28-115,
  * src/TimeAdvanceFunc.cu:102-152).  *dt_out is written after a stream sync. */

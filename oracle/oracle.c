@@ -1028,6 +1028,123 @@ static void apply_symmetry_face(orc_zone *z, const orc_param *p, const orc_face 
       }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Multi-block meshes: InnerFace::register_boundary (src/Mesh.cpp:39-172)    */
+/* and inner_communication (src/DataCommunication.cu:36-102).                */
+/* ------------------------------------------------------------------------ */
+static int isgn(int a) { return a > 0 ? 1 : (a < 0 ? -1 : 0); }
+
+int orc_register_inner_face(int dim, int ngg, const int src[6], const int tar[6], int target_block,
+                            orc_inner_face *o) {
+  int rs[3], re[3], ts[3], te[3], st[3] = {0, 0, 0};
+  int face = -1, dir = 1, tface = -1, tdir = 1;
+  for (int i = 0; i < 3; ++i) {
+    rs[i] = src[2 * i]; re[i] = src[2 * i + 1];
+    ts[i] = tar[2 * i]; te[i] = tar[2 * i + 1];
+  }
+  for (int i = 0; i < dim && face < 0; ++i)
+    if (rs[i] == re[i]) {
+      face = i;
+      if (rs[i] == 1) dir = -1;
+      rs[i] -= 1; re[i] -= 1;
+    }
+  for (int i = 0; i < dim && tface < 0; ++i)
+    if (ts[i] == te[i]) {
+      tface = i;
+      if (ts[i] == 1) tdir = -1;
+      ts[i] -= 1; te[i] -= 1;
+    }
+  if (face < 0 || tface < 0) return -1;
+  st[tface] = -(dir * tdir) * (face + 1);
+  if (dim == 2) {
+    const int nf = 1 - face, tnf = 1 - tface;
+    rs[nf] = abs(rs[nf]) - 1; re[nf] = abs(re[nf]) - 1;
+    ts[tnf] = abs(ts[tnf]) - 1; te[tnf] = abs(te[tnf]) - 1;
+    st[tnf] = isgn((te[tnf] - ts[tnf]) * (re[nf] - rs[nf])) * (nf + 1);
+    st[2] = 3;
+    rs[2] = re[2] = ts[2] = te[2] = 0;
+  } else {
+    int nf = -1, tnf = -1;
+    for (int i = 0; i < dim && nf < 0; ++i)
+      if (rs[i] < 0) { nf = i; rs[i] = -rs[i] - 1; re[i] = -re[i] - 1; }
+    for (int i = 0; i < dim && tnf < 0; ++i)
+      if (ts[i] < 0) { tnf = i; ts[i] = -ts[i] - 1; te[i] = -te[i] - 1; }
+    if (nf < 0 || tnf < 0) return -1;
+    st[tnf] = isgn((te[tnf] - ts[tnf]) * (re[nf] - rs[nf])) * (nf + 1);
+    nf = 3 - face - nf;
+    tnf = 3 - tface - tnf;
+    rs[nf] -= 1; re[nf] -= 1;
+    ts[tnf] -= 1; te[tnf] -= 1;
+    st[tnf] = isgn((te[tnf] - ts[tnf]) * (re[nf] - rs[nf])) * (nf + 1);
+  }
+  rs[face] = dir < 0 ? -ngg : re[face];
+  re[face] = dir < 0 ? 0 : re[face] + ngg;
+  const int sg = isgn(st[tface]);
+  if (tdir > 0) ts[tface] = sg > 0 ? te[tface] - ngg : te[tface];
+  else ts[tface] = sg > 0 ? 0 : ngg;
+  for (int i = 0; i < 3; ++i) {
+    o->range_start[i] = rs[i]; o->range_end[i] = re[i];
+    o->target_start[i] = ts[i]; o->target_end[i] = te[i];
+    o->loop_dir[i] = rs[i] <= re[i] ? 1 : -1;
+    o->target_loop_dir[i] = isgn(st[i]);
+    o->src_tar[i] = abs(st[i]) - 1;
+    o->n_point[i] = abs(rs[i] - re[i]) + 1;
+  }
+  o->face = face; o->direction = dir;
+  o->target_face = tface; o->target_direction = tdir;
+  o->target_block = target_block - 1;
+  return 0;
+}
+
+/* The speed test uses sqrt(u^2 + v^2 + w^2) where the reference calls norm3d;
+ * the two can differ in the last bit, which matters only for speeds within
+ * an ulp of the 1e-15 threshold. */
+void orc_inner_communication(orc_zone *z, orc_zone *tz, const orc_param *p, const orc_inner_face *f) {
+  const int g = z->ngg;
+  const long sz = psz(z, g), tsz = psz(tz, g);
+  const int face_node = f->direction > 0 ? f->range_start[f->face] : f->range_end[f->face];
+  for (int n2 = 0; n2 < f->n_point[2]; ++n2)
+    for (int n1 = 0; n1 < f->n_point[1]; ++n1)
+      for (int n0 = 0; n0 < f->n_point[0]; ++n0) {
+        const int n[3] = {n0, n1, n2};
+        int idx[3], d_idx[3], idt[3];
+        for (int a = 0; a < 3; ++a) {
+          d_idx[a] = f->loop_dir[a] * n[a];
+          idx[a] = f->range_start[a] + d_idx[a];
+        }
+        for (int a = 0; a < 3; ++a) idt[a] = f->target_start[a] + f->target_loop_dir[a] * d_idx[f->src_tar[a]];
+        const long id = pidx(z, g, idx[0], idx[1], idx[2]), it = pidx(tz, g, idt[0], idt[1], idt[2]);
+        double *bv = z->bv, *tbv = tz->bv, *sv = z->sv, *tsv = tz->sv;
+        if (idx[f->face] == face_node) {
+          const double u_this = sqrt(bv[id + sz] * bv[id + sz] + bv[id + 2 * sz] * bv[id + 2 * sz] +
+                                     bv[id + 3 * sz] * bv[id + 3 * sz]);
+          if (fabs(u_this) > 1e-15) {
+            const double u_that = sqrt(tbv[it + tsz] * tbv[it + tsz] + tbv[it + 2 * tsz] * tbv[it + 2 * tsz] +
+                                       tbv[it + 3 * tsz] * tbv[it + 3 * tsz]);
+            if (fabs(u_that) < 1e-15) {
+              for (int l = 0; l < 6; ++l) bv[id + l * sz] = tbv[it + l * tsz];
+              for (int l = 0; l < p->n_scalar; ++l) sv[id + l * sz] = tsv[it + l * tsz];
+            } else {
+              for (int l = 0; l < 6; ++l) {
+                const double ave = 0.5 * (tbv[it + l * tsz] + bv[id + l * sz]);
+                bv[id + l * sz] = ave;
+                tbv[it + l * tsz] = ave;
+              }
+              for (int l = 0; l < p->n_scalar; ++l) {
+                const double ave = 0.5 * (tsv[it + l * tsz] + sv[id + l * sz]);
+                sv[id + l * sz] = ave;
+                tsv[it + l * tsz] = ave;
+              }
+            }
+          }
+        } else {
+          for (int l = 0; l < 6; ++l) bv[id + l * sz] = tbv[it + l * tsz];
+          for (int l = 0; l < p->n_scalar; ++l) sv[id + l * sz] = tsv[it + l * tsz];
+        }
+        cv_from_bv_point(z, p, id);
+      }
+}
+
 /* eliminate_k_gradient (src/FieldOperation.cu:47-72) */
 void orc_eliminate_k_gradient(orc_zone *z, const orc_param *p) {
   const int g = z->ngg;

@@ -98,6 +98,26 @@ typedef struct {
   double wall_yk[ORC_MAX_SPEC];
 } orc_param;
 
+/* A face shared by two blocks of a multi-block mesh, as InnerFace holds it
+ * after register_boundary (src/Mesh.h:33-59, src/Mesh.cpp:39-172). */
+typedef struct {
+  int range_start[3], range_end[3];
+  int face, direction;
+  int target_start[3], target_end[3];
+  int target_block, target_face, target_direction;
+  int src_tar[3], loop_dir[3], target_loop_dir[3];
+  int n_point[3];
+} orc_inner_face;
+
+/* InnerFace(...) + register_boundary from the inner-interface records: src and
+ * tar are {x1, x2, y1, y2, z1, z2} (1-based, sign-coded), target_block 1-based.
+ * Returns 0, or -1 for a record it cannot decode. */
+int orc_register_inner_face(int dim, int ngg, const int src[6], const int tar[6], int target_block,
+                            orc_inner_face *out);
+/* inner_communication (src/DataCommunication.cu:36-102) of one face of zone z
+ * with the target block tz (may be z itself). */
+void orc_inner_communication(orc_zone *z, orc_zone *tz, const orc_param *p, const orc_inner_face *f);
+
 /* zone memory management (host, zero-filled) */
 int orc_zone_alloc(orc_zone *z, int mx, int my, int mz, int ngg, int n_var, int n_spec, int n_scalar);
 void orc_zone_free(orc_zone *z);

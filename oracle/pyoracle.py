@@ -114,6 +114,27 @@ def make_mech(m) -> orc_mech:
 _lib = None
 
 
+_I3 = ctypes.c_int * 3
+
+
+class orc_inner_face(ctypes.Structure):
+    _fields_ = [("range_start", _I3), ("range_end", _I3), ("face", ctypes.c_int), ("direction", ctypes.c_int),
+                ("target_start", _I3), ("target_end", _I3), ("target_block", ctypes.c_int),
+                ("target_face", ctypes.c_int), ("target_direction", ctypes.c_int), ("src_tar", _I3),
+                ("loop_dir", _I3), ("target_loop_dir", _I3), ("n_point", _I3)]
+
+
+def register_inner_face(dim, ngg, src, tar, target_block) -> orc_inner_face:
+    """InnerFace registration from the two records of an inner-interface file
+    (1-based, sign-coded {x1, x2, y1, y2, z1, z2}; target_block 1-based)."""
+    f = orc_inner_face()
+    rc = lib().orc_register_inner_face(dim, ngg, (ctypes.c_int * 6)(*src), (ctypes.c_int * 6)(*tar), target_block,
+                                       ctypes.byref(f))
+    if rc != 0:
+        raise ValueError(f"cannot register inner face {src} -> {tar}")
+    return f
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
@@ -149,6 +170,11 @@ def lib() -> ctypes.CDLL:
         L.orc_wu_reaction_step.restype = None
         L.orc_finite_rate_chemistry.argtypes = [zp, pp]
         L.orc_finite_rate_chemistry.restype = None
+        L.orc_register_inner_face.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_int, ctypes.POINTER(orc_inner_face)]
+        L.orc_register_inner_face.restype = ctypes.c_int
+        L.orc_inner_communication.argtypes = [zp, zp, pp, ctypes.POINTER(orc_inner_face)]
+        L.orc_inner_communication.restype = None
         _lib = L
     return _lib
 
@@ -226,6 +252,10 @@ class OracleZone:
         self.L.orc_wu_reaction_step(ctypes.byref(self.z), ctypes.byref(self.p), dt,
                                     ns.ctypes.data if want_nsub else None)
         return ns
+
+    def inner_communication(self, target: "OracleZone", face: orc_inner_face):
+        self.L.orc_inner_communication(ctypes.byref(self.z), ctypes.byref(target.z), ctypes.byref(self.p),
+                                       ctypes.byref(face))
 
     def call(self, name, *args):
         return getattr(self.L, name)(ctypes.byref(self.z), ctypes.byref(self.p), *args)
