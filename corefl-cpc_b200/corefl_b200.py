@@ -32,6 +32,16 @@ class cfk_inner_face(ctypes.Structure):
                 ("loop_dir", _I3), ("target_loop_dir", _I3), ("n_point", _I3)]
 
 
+class cfk_plt_block(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
+        (n, ctypes.c_void_p) for n in ("x", "y", "z", "bv", "sv", "ov")]
+
+
+class cfk_plt_target(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int),
+                ("bv", ctypes.c_void_p), ("sv", ctypes.c_void_p)]
+
+
 class cfk_param(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
@@ -165,6 +175,10 @@ def lib() -> ctypes.CDLL:
             "cfk_compute_cv_from_bv": (i, [vp, vp]),
             "cfk_apply_boundary_conditions": (i, [vp, vp]),
             "cfk_eliminate_k_gradient": (i, [vp, vp]),
+            "cfk_write_flowfield": (i, [ctypes.c_char_p, ctypes.POINTER(cfk_plt_block), i, i,
+                                        ctypes.POINTER(ctypes.c_char_p), i, i, d, ctypes.c_char_p, ctypes.c_size_t]),
+            "cfk_read_flowfield": (i, [ctypes.c_char_p, ctypes.POINTER(cfk_plt_target), i,
+                                       ctypes.POINTER(ctypes.c_char_p), i, _DP, ctypes.c_char_p, ctypes.c_size_t]),
             "cfk_register_inner_face": (i, [i, i, vp, vp, i, ctypes.POINTER(cfk_inner_face)]),
             "cfk_inner_communication": (i, [vp, vp, ctypes.POINTER(cfk_inner_face), vp]),
             "cfk_local_time_step": (i, [vp, _DP, vp]),
@@ -215,6 +229,45 @@ def register_inner_face(dim, ngg, src, tar, target_block) -> cfk_inner_face:
     if rc != 0:
         raise CfkError(f"cfk_register_inner_face({src}, {tar}) failed ({rc})")
     return f
+
+
+def _host_ptr(a):
+    import numpy as np
+
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "float64 C-contiguous host arrays"
+    return a.ctypes.data
+
+
+def write_flowfield(path, blocks, names, ngg_output=0, n_scalar=0, n_other=0, solution_time=0.0):
+    """cfk_write_flowfield.  blocks: dicts with mx, my, mz, ngg and host
+    float64 arrays x, y, z (padded), bv (6 planes), sv, ov."""
+    arr = (cfk_plt_block * len(blocks))()
+    for n, b in enumerate(blocks):
+        arr[n] = cfk_plt_block(b["mx"], b["my"], b["mz"], b["ngg"],
+                               *[_host_ptr(b.get(k)) for k in ("x", "y", "z", "bv", "sv", "ov")])
+    cn = (ctypes.c_char_p * len(names))(*[x.encode() for x in names])
+    err = ctypes.create_string_buffer(256)
+    rc = lib().cfk_write_flowfield(str(path).encode(), arr, len(blocks), ngg_output, cn, n_scalar, n_other,
+                                   solution_time, err, 256)
+    if rc != 0:
+        raise CfkError(f"cfk_write_flowfield: {rc}: {err.value.decode()}")
+
+
+def read_flowfield(path, targets, species=()):
+    """cfk_read_flowfield into host arrays.  targets: dicts with mx, my, mz,
+    ngg and float64 arrays bv (6 planes) and sv; returns the solution time."""
+    arr = (cfk_plt_target * len(targets))()
+    for n, b in enumerate(targets):
+        arr[n] = cfk_plt_target(b["mx"], b["my"], b["mz"], b["ngg"], _host_ptr(b.get("bv")), _host_ptr(b.get("sv")))
+    sp = (ctypes.c_char_p * max(1, len(species)))(*[x.encode() for x in species])
+    t = ctypes.c_double()
+    err = ctypes.create_string_buffer(256)
+    rc = lib().cfk_read_flowfield(str(path).encode(), arr, len(targets), sp, len(species), ctypes.byref(t), err, 256)
+    if rc != 0:
+        raise CfkError(f"cfk_read_flowfield: {rc}: {err.value.decode()}")
+    return t.value
 
 
 def make_param(p: dict, faces) -> cfk_param:

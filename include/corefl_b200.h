@@ -207,6 +207,43 @@ int cfk_apply_boundary_conditions(cfk_ctx *ctx, void *stream);
  * multi-block stage calls it again after its cfk_inner_communication calls. */
 int cfk_eliminate_k_gradient(cfk_ctx *ctx, void *stream);
 
+/* ---- flowfield files (host only) ------------------------------------------ */
+/* One block of a Tecplot V112 binary flowfield file: interior node counts,
+ * the ghost width of the host arrays below (the reference's padded layout),
+ * and the arrays — coordinates, the 6 basic variables (density, u, v, w,
+ * pressure, temperature), n_scalar scalars (species mass fractions) and
+ * n_other further planes (Mach number, ...). */
+typedef struct cfk_plt_block {
+  int mx, my, mz, ngg;
+  const double *x, *y, *z;
+  const double *bv, *sv, *ov;
+} cfk_plt_block;
+/* A block to restart: sizes, ghost width and the host arrays to fill. */
+typedef struct cfk_plt_target {
+  int mx, my, mz, ngg;
+  double *bv, *sv;
+} cfk_plt_target;
+/* Write `path` as the reference's output/flowfield.plt (reference
+ * src/FieldIO.h:83-420, FieldIO::write_header + write_common_data_section):
+ * one zone per block over its nodes widened by ngg_output ghost layers,
+ * variables in the order x, y, z, bv, sv, ov with their min/max pairs, all in
+ * double precision.  var_names holds the 9 + n_scalar + n_other names.
+ * CFK_ERR_IO if the file cannot be written; err (may be NULL) gets a message. */
+int cfk_write_flowfield(const char *path, const cfk_plt_block *blocks, int n_block, int ngg_output,
+                        const char *const *var_names, int n_scalar, int n_other, double solution_time,
+                        char *err, size_t err_len);
+/* Restart from a flowfield file (reference src/Initialize.cu:97-345, the
+ * branch where the file's zones are the current blocks in the same order):
+ * every variable whose name is a basic variable (density/rho/roe, u, v, w,
+ * p/pressure, t/temperature, any case) or one of species_names is read into
+ * bv or sv over the file's nodes (the zone may carry up to the block's ngg
+ * ghost layers); other variables are skipped.  *solution_time (may be NULL)
+ * gets the zones' solution time.  On a truncated file the arrays may be
+ * partly filled and CFK_ERR_IO is returned. */
+int cfk_read_flowfield(const char *path, const cfk_plt_target *blocks, int n_block,
+                       const char *const *species_names, int n_spec, double *solution_time, char *err,
+                       size_t err_len);
+
 /* ---- multi-block meshes on one GPU ---------------------------------------- */
 /* Build an inner face from the two records of the mesh's inner-interface file
  * (reference src/Mesh.cpp:927-958 and InnerFace::register_boundary,
