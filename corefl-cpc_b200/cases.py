@@ -258,6 +258,29 @@ def with_walls(case: Case, thermal_type: int = 0, temperature: float | None = No
     return dataclasses.replace(case, param=param, faces=new_faces, name=case.name + "_walls")
 
 
+def with_inflow(case: Case, rho: float, u: float, p: float, v: float = 0.0, w: float = 0.0, Y=None,
+                subsonic: int = 0, faces=((0, -1),)) -> Case:
+    """Copy of `case` whose listed (face, direction) boundaries are constant
+    inflows (label 5) of density rho, velocity (u, v, w), pressure p and, for
+    mixtures, mass fractions Y (array in mechanism order); the temperature
+    and mean molecular weight follow from the state equation.  subsonic = the
+    reference's inflow_sub."""
+    marks = set(faces)
+    new_faces = [(f, d, 5 if (f, d) in marks else lab) for f, d, lab in case.faces]
+    for f, d in marks:
+        if not any((f, d) == (a, b) for a, b, _ in case.faces):
+            new_faces.append((f, d, 5))
+    if case.mech is None:
+        mw, sv = MW_AIR, []
+    else:
+        Y = np.asarray(Y, dtype=float)
+        mw, sv = 1.0 / float(np.sum(Y / case.mech.mw)), list(Y)
+    param = dict(case.param)
+    param.update(inflow_subsonic=subsonic, inflow_density=rho, inflow_u=u, inflow_v=v, inflow_w=w, inflow_pressure=p,
+                 inflow_temperature=p * mw / (rho * R_U), inflow_mw=mw, inflow_sv=sv)
+    return dataclasses.replace(case, param=param, faces=new_faces, name=case.name + "_inflow")
+
+
 def split_i(case: Case, h: int, periodic_i: bool | None = None):
     """Two blocks cut from `case` along i, sharing the node plane i = h:
     A holds nodes 0..h, B nodes h..mx-1.  Every padded array is sliced from

@@ -42,6 +42,11 @@ class cfk_plt_target(ctypes.Structure):
                 ("bv", ctypes.c_void_p), ("sv", ctypes.c_void_p)]
 
 
+class cfk_inflow(ctypes.Structure):
+    _fields_ = [("subsonic", ctypes.c_int)] + [(n, ctypes.c_double) for n in (
+        "density", "u", "v", "w", "pressure", "temperature", "mw")] + [("sv", ctypes.c_double * 9)]
+
+
 class cfk_param(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
@@ -53,7 +58,7 @@ class cfk_param(ctypes.Structure):
         ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("weno_eps_scale", ctypes.c_double),
         ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double), ("sensor_threshold", ctypes.c_double),
         ("device", ctypes.c_int), ("shock_sensor", ctypes.c_int), ("sensor_eps", ctypes.c_double),
-        ("wall", cfk_wall),
+        ("wall", cfk_wall), ("inflow", cfk_inflow),
     ]
 
 
@@ -276,8 +281,13 @@ def make_param(p: dict, faces) -> cfk_param:
         if k == "wall_yk":
             for l, y in enumerate(v):
                 cp.wall.yk[l] = y
+        elif k == "inflow_sv":
+            for l, y in enumerate(v):
+                cp.inflow.sv[l] = y
         elif k.startswith("wall_"):
             setattr(cp.wall, k[5:], v)
+        elif k.startswith("inflow_"):
+            setattr(cp.inflow, k[7:], v)
         elif k in dict(cfk_param._fields_):
             setattr(cp, k, v)
     cp.n_face = len(faces)

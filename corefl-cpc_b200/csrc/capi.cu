@@ -33,7 +33,8 @@ cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
                             cudaStream_t st, bool with_reaction = true);
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
-                                       int n_face, const cfk_wall &wall, cudaStream_t st, int *n_launch);
+                                       int n_face, const cfk_wall &wall, const cfk_inflow &inflow, cudaStream_t st,
+                                       int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
 cudaError_t launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t st);
 cudaError_t launch_inner_communication(const Zone &z, const Zone &tz, const Param &p, const Thermo *th,
@@ -161,9 +162,17 @@ int validate(const cfk_param *p, std::string &why) {
   for (int n = 0; n < p->n_face; ++n) {
     const cfk_face &f = p->faces[n];
     if (f.face < 0 || f.face > 2 || (f.direction != -1 && f.direction != 1) ||
-        !(f.label == 6 || f.label == 8 || f.label == 3 || f.label == 2)) {
+        !(f.label == 6 || f.label == 8 || f.label == 3 || f.label == 2 || f.label == 5)) {
       why = "unsupported boundary face description";
       return -1;
+    }
+    if (f.label == 5) {
+      const cfk_inflow &q = p->inflow;
+      if (!(q.density > 0) || !(q.pressure > 0) || !(q.temperature > 0) || (p->n_spec > 0 && !(q.mw > 0)) ||
+          (q.subsonic != 0 && q.subsonic != 1)) {
+        why = "inflow needs density, pressure, temperature (and mw for mixtures) > 0 and subsonic 0 or 1";
+        return -1;
+      }
     }
     if (f.label == 2) {
       const cfk_wall &w = p->wall;
@@ -572,7 +581,7 @@ int cfk_compute_cv_from_bv(cfk_ctx *c, void *stream) {
 int cfk_apply_boundary_conditions(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
   int n = 0;
-  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, S(stream), &n),
+  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, S(stream), &n),
             "boundary conditions");
   c->launches += n;
   return CFK_OK;
@@ -693,7 +702,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_BC, st, &n);
-      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, st, &n), "boundary conditions");
+      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, st, &n), "boundary conditions");
     }
     {
       PhaseScope ps(c, CFK_PH_PROPS, st, &n);
@@ -742,7 +751,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
             "wu_reaction_step");
   ++n;
-  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, st, &n), "boundary conditions");
+  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, st, &n), "boundary conditions");
   CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
   ++n;
   // wu_RK_subStep (:564-634): SSP-RK3 over dt/2 on dq - Cn, no property update
@@ -754,7 +763,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
     CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;
-    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, st, &n), "boundary conditions");
+    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, st, &n), "boundary conditions");
   }
   c->launches += n;
   if (dt_used) *dt_used = dt;

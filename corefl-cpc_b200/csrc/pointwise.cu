@@ -349,6 +349,83 @@ __global__ void bc_periodic_kernel(Zone z, Param p, const Thermo *th, FaceGeom f
   }
 }
 
+// apply_inflow (reference src/BoundCond.cu:2190-2705), constant inflow
+// without fluctuations.  The face node takes the inflow state, or — subsonic
+// inflow whose normal Mach number, from the face node's current velocity, is
+// not below -1 — the characteristic combination of the inflow state and the
+// inner node: p = (p1 + p_in - rho1 c1 (V_in - V1).n) / 2, rho = rho_in +
+// (p - p_in) / c1^2, V = V_in - (p - p_in) / (rho1 c1) n, T from the state
+// equation.  Ghost layer g takes the face values (supersonic) or reflects
+// inner node g about them with p and rho held above 0.1 of the face values
+// (subsonic).  One thread per face node and its ghost line: the face values
+// depend on the face node's values before they are overwritten.
+template <bool MIX>
+__global__ void bc_inflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg, cfk_inflow in) {
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= fg.n[0] * fg.n[1] * fg.n[2]) return;
+  int i, j, k;
+  face_node(fg, t, i, j, k);
+  const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+  const int64_t s = d.stride(g, fg.face) * fg.direction;
+  double density = in.density, u = in.u, v = in.v, w = in.w, pr = in.pressure, T = in.temperature;
+  if (in.subsonic) {
+    const int mf = 3 * fg.face;
+    double nx = z.metric[id + mf * sz], ny = z.metric[id + (mf + 1) * sz], nz = z.metric[id + (mf + 2) * sz];
+    const double grad_n_inv = fg.direction / sqrt(nx * nx + ny * ny + nz * nz);
+    nx *= grad_n_inv;
+    ny *= grad_n_inv;
+    nz *= grad_n_inv;
+    const double c0 = MIX ? z.acoustic_speed[id] : sqrt(kGammaAir * kRAir * z.bv[id + 5 * sz]);
+    const double Mn = (z.bv[id + sz] * nx + z.bv[id + 2 * sz] * ny + z.bv[id + 3 * sz] * nz) / c0;
+    if (!(Mn < -1.0)) {
+      const int64_t i1 = id - s;
+      const double c1 = MIX ? z.acoustic_speed[i1] : sqrt(kGammaAir * kRAir * z.bv[i1 + 5 * sz]);
+      const double rho1 = z.bv[i1], p1 = z.bv[i1 + 4 * sz];
+      pr = 0.5 * (p1 + in.pressure - rho1 * c1 * ((in.u - z.bv[i1 + sz]) * nx + (in.v - z.bv[i1 + 2 * sz]) * ny +
+                                                  (in.w - z.bv[i1 + 3 * sz]) * nz));
+      density = in.density + (pr - in.pressure) / (c1 * c1);
+      u = in.u - (pr - in.pressure) / (rho1 * c1) * nx;
+      v = in.v - (pr - in.pressure) / (rho1 * c1) * ny;
+      w = in.w - (pr - in.pressure) / (rho1 * c1) * nz;
+      T = MIX ? pr * in.mw / (density * kRu) : pr / (density * kRAir);
+    }
+  }
+  z.bv[id] = density;
+  z.bv[id + sz] = u;
+  z.bv[id + 2 * sz] = v;
+  z.bv[id + 3 * sz] = w;
+  z.bv[id + 4 * sz] = pr;
+  z.bv[id + 5 * sz] = T;
+  for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = in.sv[l];
+  cv_from_bv_point<MIX>(z, p, th, id);
+  for (int gg = 1; gg <= g; ++gg) {
+    const int64_t gi = id + gg * s;
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = in.sv[l];
+    if (in.subsonic) {
+      const int64_t ii = id - gg * s;
+      double rho2 = 2 * density - z.bv[ii], p2 = 2 * pr - z.bv[ii + 4 * sz];
+      if (p2 <= 0.1 * pr) p2 = 0.1 * pr;
+      if (rho2 <= 0.1 * density) rho2 = 0.1 * density;
+      z.bv[gi] = rho2;
+      z.bv[gi + sz] = 2 * u - z.bv[ii + sz];
+      z.bv[gi + 2 * sz] = 2 * v - z.bv[ii + 2 * sz];
+      z.bv[gi + 3 * sz] = 2 * w - z.bv[ii + 3 * sz];
+      z.bv[gi + 4 * sz] = p2;
+      z.bv[gi + 5 * sz] = MIX ? p2 * in.mw / (rho2 * kRu) : p2 / (rho2 * kRAir);
+    } else {
+      z.bv[gi] = density;
+      z.bv[gi + sz] = u;
+      z.bv[gi + 2 * sz] = v;
+      z.bv[gi + 3 * sz] = w;
+      z.bv[gi + 4 * sz] = pr;
+      z.bv[gi + 5 * sz] = T;
+    }
+    cv_from_bv_point<MIX>(z, p, th, gi);
+  }
+}
+
 // apply_wall (reference src/BoundCond.cu:2761-3031) without its jet,
 // shock-blowing and wall-fluctuation branches (so v_blow = 0).  The face node
 // takes zero velocity, its inner neighbour's pressure, the wall temperature
@@ -550,13 +627,16 @@ static FaceGeom make_face(const Dims &d, const cfk_face &f) {
 }
 
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
-                                       int n_face, const cfk_wall &wall, cudaStream_t st, int *n_launch) {
-  static const int order[4] = {6, 3, 2, 8};  // outflow, symmetry, wall, periodic (reference priority order)
-  for (int o = 0; o < 4; ++o) {
+                                       int n_face, const cfk_wall &wall, const cfk_inflow &inflow, cudaStream_t st,
+                                       int *n_launch) {
+  // reference priority order: outflow, inflow, symmetry, wall, periodic
+  static const int order[5] = {6, 5, 3, 2, 8};
+  for (int o = 0; o < 5; ++o) {
     for (int n = 0; n < n_face; ++n) {
       if (faces[n].label != order[o]) continue;
       const FaceGeom fg = make_face(z.d, faces[n]);
-      const int cnt = fg.n[0] * fg.n[1] * fg.n[2] * (fg.face == 0 ? z.d.ngg + 1 : 1);
+      const bool split = order[o] != 5;  // the inflow kernel keeps a face node's line in one thread
+      const int cnt = fg.n[0] * fg.n[1] * fg.n[2] * (split && fg.face == 0 ? z.d.ngg + 1 : 1);
       const int blocks = (cnt + 127) / 128;
       const bool mix = p.n_spec > 0;
       if (order[o] == 6) {
@@ -565,6 +645,9 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
       } else if (order[o] == 3) {
         if (mix) bc_symmetry_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
         else bc_symmetry_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);
+      } else if (order[o] == 5) {
+        if (mix) bc_inflow_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg, inflow);
+        else bc_inflow_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg, inflow);
       } else if (order[o] == 2) {
         if (mix) bc_wall_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg, wall);
         else bc_wall_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg, wall);

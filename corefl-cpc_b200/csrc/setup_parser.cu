@@ -144,6 +144,74 @@ bool read_wall(const Setup &s, cfk_wall &w, std::string &err) {
   return true;
 }
 
+int struct_int(const Struct &st, const char *k, int dflt) {
+  auto it = st.find(k);
+  if (it == st.end()) return dflt;
+  if (auto p = std::get_if<int>(&it->second)) return *p;
+  return dflt;
+}
+
+// The inflow condition of the boundary_conditions list, air (reference
+// src/BoundCond.cpp:9-260, Inflow::Inflow for a constant inflow): the state
+// from one of (mach, pressure, temperature), (density, velocity, pressure)
+// or (mach, temperature, reynolds), the velocity along aoa (degrees) or along
+// (u, v, w).  Profile and mixing-layer inflows and inflow fluctuations are
+// not part of this path and are reported; so is a second inflow struct.
+bool read_inflow(const Setup &s, cfk_inflow &q, std::string &err) {
+  std::memset(&q, 0, sizeof(q));
+  auto list = s.arrays.find("boundary_conditions");
+  if (list == s.arrays.end()) return true;
+  int n_inflow = 0;
+  for (const std::string &name : list->second) {
+    auto it = s.structs.find(name);
+    if (it == s.structs.end() || struct_string(it->second, "type") != "inflow") continue;
+    const Struct &st = it->second;
+    if (++n_inflow > 1) { err = "more than one inflow condition; cfk_param carries one"; return false; }
+    if (struct_int(st, "inflow_type", 0) != 0 || struct_int(st, "fluctuation_type", 0) != 0) {
+      err = "inflow " + name + ": profile, mixing-layer and fluctuating inflows are not supported";
+      return false;
+    }
+    const double R_u = 8314.462618, mw = 28.9647, gamma = 1.4, pi = 3.141592653589793;
+    double mach = struct_real(st, "mach", -1), pressure = struct_real(st, "pressure", -1);
+    double temperature = struct_real(st, "temperature", -1), velocity = struct_real(st, "velocity", 0);
+    double density = struct_real(st, "density", -1), aoa = struct_real(st, "aoa", -1000);
+    double u = struct_real(st, "u", 1), v = struct_real(st, "v", 0), w = struct_real(st, "w", 0);
+    const double reynolds = struct_real(st, "reynolds", -1);
+    if (temperature < 0) temperature = pressure * mw / (density * R_u);
+    const double viscosity = 1.7894e-5 * std::pow(temperature / 288.16, 1.5) * (288.16 + 110) / (temperature + 110);
+    const double c = std::sqrt(gamma * R_u / mw * temperature);
+    if (mach < 0) mach = velocity / c;
+    else velocity = mach * c;
+    if (aoa > -1000) {
+      u = std::cos(aoa * pi / 180) * velocity;
+      v = std::sin(aoa * pi / 180) * velocity;
+      w = 0;
+    } else {
+      u *= velocity;
+      v *= velocity;
+      w *= velocity;
+    }
+    if (density < 0) {
+      if (pressure < 0) {
+        if (reynolds < 0) { err = "inflow " + name + ": give pressure, density or reynolds"; return false; }
+        density = viscosity * reynolds / velocity;
+        pressure = density * temperature * R_u / mw;
+      } else {
+        density = pressure * mw / (R_u * temperature);
+      }
+    }
+    q.subsonic = struct_int(st, "inflow_sub", 0);
+    q.density = density;
+    q.u = u;
+    q.v = v;
+    q.w = w;
+    q.pressure = pressure;
+    q.temperature = temperature;
+    q.mw = mw;
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char *errbuf, size_t err_len) {
@@ -203,6 +271,7 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
   }
   p.weno_eps_scale = p.rho_ref * p.v_ref * p.rho_ref * p.v_ref;
   if (!read_wall(s, p.wall, err)) return report(err);
+  if (!read_inflow(s, p.inflow, err)) return report(err);
   p.n_face = 0;
   *out = p;
   return CFK_OK;

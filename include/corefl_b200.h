@@ -40,7 +40,8 @@ typedef struct cfk_ctx cfk_ctx;
 
 /* A boundary face of the block (reference src/Mesh.cpp:14-31, Boundary).
  * face 0/1/2 = i/j/k, direction -1 = min side, +1 = max side;
- * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall (cfk_param.wall). */
+ * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall (cfk_param.wall),
+ * 5 = inflow (cfk_param.inflow). */
 typedef struct cfk_face {
   int face, direction, label;
 } cfk_face;
@@ -75,6 +76,19 @@ typedef struct cfk_inner_face {
   int n_point[3];
 } cfk_inner_face;
 
+/* The constant inflow of the faces labelled 5 (reference src/BoundCond.h:22-87,
+ * Inflow with inflow_type 0 and no fluctuation): the state the reference
+ * derives in Inflow::Inflow (src/BoundCond.cpp:160-250) — density, velocity,
+ * pressure, temperature, the mean molecular weight (mixtures) and the
+ * scalars (mass fractions).  subsonic = the reference's inflow_sub: where the
+ * normal Mach number at the face is not below -1 the face takes the
+ * characteristic combination of the inflow state and the inner node. */
+typedef struct cfk_inflow {
+  int subsonic;
+  double density, u, v, w, pressure, temperature, mw;
+  double sv[CFK_MAX_SPEC];
+} cfk_inflow;
+
 /* Scalar settings of the path: the DParameter fields it reads
  * (reference src/DParameter.cuh:13-207) plus the boundary list. */
 typedef struct cfk_param {
@@ -103,6 +117,7 @@ typedef struct cfk_param {
   int shock_sensor;        /* 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump */
   double sensor_eps;       /* shockSensor_epsilon (reference default -1) */
   cfk_wall wall;           /* read for faces labelled 2 */
+  cfk_inflow inflow;       /* read for faces labelled 5 */
 } cfk_param;
 
 /* Device pointers of one block, field for field the arrays of the reference's
@@ -197,8 +212,8 @@ int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);
 int cfk_update_physical_properties(cfk_ctx *ctx, void *stream);
 /* Replaces compute_cv_from_bv<M> (reference src/FieldOperation.cuh:39-64). */
 int cfk_compute_cv_from_bv(cfk_ctx *ctx, void *stream);
-/* Replaces DBoundCond::apply_boundary_conditions<M> for outflow, symmetry, wall
- * and periodic faces (reference src/BoundCond.cu:3489-3619) and, for 2-D blocks,
+/* Replaces DBoundCond::apply_boundary_conditions<M> for outflow, inflow, symmetry,
+ * wall and periodic faces (reference src/BoundCond.cu:3489-3619) and, for 2-D blocks,
  * eliminate_k_gradient (reference src/FieldOperation.cu:47-72). */
 int cfk_apply_boundary_conditions(cfk_ctx *ctx, void *stream);
 /* eliminate_k_gradient on its own (reference src/FieldOperation.cu:47-72): a

@@ -824,7 +824,7 @@ double orc_global_time_step(const orc_zone *z) {
 /* ------------------------------------------------------------------------ */
 /* Boundary conditions: outflow (src/BoundCond.cu:2065-2171, plain branch),  */
 /* periodic (src/BoundCond.cu:3033-3080), symmetry (src/BoundCond.cu:2002),  */
-/* no-slip wall (src/BoundCond.cu:2761-3031)                                 */
+/* no-slip wall (src/BoundCond.cu:2761-3031), inflow (src/BoundCond.cu:2190) */
 /* applied per label in the reference's priority order                       */
 /* (src/BoundCond.cu:3489-3619): outflow, inflow, symmetry, wall, periodic.  */
 /* Each face covers its tangential range widened by ngg ghosts               */
@@ -971,13 +971,81 @@ static void apply_wall_face(orc_zone *z, const orc_param *p, const orc_face *f) 
       }
 }
 
+/* apply_inflow (src/BoundCond.cu:2190-2705), constant inflow without
+ * fluctuations (inflow_type 0, fluctuation_type 0). */
+static void apply_inflow_face(orc_zone *z, const orc_param *p, const orc_face *f) {
+  const int g = z->ngg;
+  const long sz = psz(z, g);
+  int lo[3], hi[3];
+  face_range(z, f, lo, hi);
+  const long s = pstride(z, g, f->face) * f->direction;
+  const int mix = p->mech != NULL;
+  double *bv = z->bv, *sv = z->sv;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        const long id = pidx(z, g, i, j, k);
+        double density = p->inflow_density, u = p->inflow_u, v = p->inflow_v, w = p->inflow_w;
+        double pr = p->inflow_pressure, T = p->inflow_temperature;
+        if (p->inflow_subsonic) {
+          const double *mt = z->metric;
+          const int mf = 3 * f->face;
+          double nx = mt[id + mf * sz], ny = mt[id + (mf + 1) * sz], nz = mt[id + (mf + 2) * sz];
+          const double grad_n_inv = f->direction / sqrt(nx * nx + ny * ny + nz * nz);
+          nx *= grad_n_inv;
+          ny *= grad_n_inv;
+          nz *= grad_n_inv;
+          const double c0 = mix ? z->acoustic_speed[id] : sqrt(GAMMA_AIR * R_AIR * bv[id + 5 * sz]);
+          const double Mn = (bv[id + sz] * nx + bv[id + 2 * sz] * ny + bv[id + 3 * sz] * nz) / c0;
+          if (!(Mn < -1.0)) {
+            const long i1 = id - s;
+            const double c1 = mix ? z->acoustic_speed[i1] : sqrt(GAMMA_AIR * R_AIR * bv[i1 + 5 * sz]);
+            const double rho1 = bv[i1], p1 = bv[i1 + 4 * sz];
+            pr = 0.5 * (p1 + p->inflow_pressure -
+                        rho1 * c1 * ((p->inflow_u - bv[i1 + sz]) * nx + (p->inflow_v - bv[i1 + 2 * sz]) * ny +
+                                     (p->inflow_w - bv[i1 + 3 * sz]) * nz));
+            density = p->inflow_density + (pr - p->inflow_pressure) / (c1 * c1);
+            u = p->inflow_u - (pr - p->inflow_pressure) / (rho1 * c1) * nx;
+            v = p->inflow_v - (pr - p->inflow_pressure) / (rho1 * c1) * ny;
+            w = p->inflow_w - (pr - p->inflow_pressure) / (rho1 * c1) * nz;
+            T = mix ? pr * p->inflow_mw / (density * R_U) : pr / (density * R_AIR);
+          }
+        }
+        bv[id] = density; bv[id + sz] = u; bv[id + 2 * sz] = v; bv[id + 3 * sz] = w;
+        bv[id + 4 * sz] = pr; bv[id + 5 * sz] = T;
+        for (int l = 0; l < p->n_scalar; ++l) sv[id + l * sz] = p->inflow_sv[l];
+        cv_from_bv_point(z, p, id);
+        for (int gg = 1; gg <= g; ++gg) {
+          const long gi = id + gg * s;
+          for (int l = 0; l < p->n_scalar; ++l) sv[gi + l * sz] = p->inflow_sv[l];
+          if (p->inflow_subsonic) {
+            const long ii = id - gg * s;
+            double rho2 = 2 * density - bv[ii], p2 = 2 * pr - bv[ii + 4 * sz];
+            if (p2 <= 0.1 * pr) p2 = 0.1 * pr;
+            if (rho2 <= 0.1 * density) rho2 = 0.1 * density;
+            bv[gi] = rho2;
+            bv[gi + sz] = 2 * u - bv[ii + sz];
+            bv[gi + 2 * sz] = 2 * v - bv[ii + 2 * sz];
+            bv[gi + 3 * sz] = 2 * w - bv[ii + 3 * sz];
+            bv[gi + 4 * sz] = p2;
+            bv[gi + 5 * sz] = mix ? p2 * p->inflow_mw / (rho2 * R_U) : p2 / (rho2 * R_AIR);
+          } else {
+            bv[gi] = density; bv[gi + sz] = u; bv[gi + 2 * sz] = v; bv[gi + 3 * sz] = w;
+            bv[gi + 4 * sz] = pr; bv[gi + 5 * sz] = T;
+          }
+          cv_from_bv_point(z, p, gi);
+        }
+      }
+}
+
 void orc_apply_boundary_conditions(orc_zone *z, const orc_param *p) {
-  static const int order[] = {6, 3, 2, 8};
-  for (int o = 0; o < 4; ++o)
+  static const int order[] = {6, 5, 3, 2, 8};
+  for (int o = 0; o < 5; ++o)
     for (int n = 0; n < p->n_face; ++n) {
       const orc_face *f = &p->faces[n];
       if (f->label != order[o]) continue;
       if (f->label == 6) apply_outflow_face(z, p, f);
+      else if (f->label == 5) apply_inflow_face(z, p, f);
       else if (f->label == 3) apply_symmetry_face(z, p, f);
       else if (f->label == 2) apply_wall_face(z, p, f);
       else if (f->label == 8) apply_periodic_face(z, p, f);

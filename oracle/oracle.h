@@ -24,7 +24,7 @@ extern "C" {
 
 /* Boundary face description (reference src/Mesh.cpp:14-31 register_boundary):
  * face 0/1/2 = i/j/k, direction -1 (min side) or +1 (max side),
- * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall. */
+ * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall, 5 = inflow. */
 typedef struct {
   int face, direction, label;
 } orc_face;
@@ -96,6 +96,11 @@ typedef struct {
   int wall_thermal_type, wall_catalytic_type;
   double wall_temperature;
   double wall_yk[ORC_MAX_SPEC];
+  /* the constant inflow of the faces labelled 5 (src/BoundCond.h:22-87):
+   * state as Inflow::Inflow derives it, inflow_sub as inflow_subsonic */
+  int inflow_subsonic;
+  double inflow_density, inflow_u, inflow_v, inflow_w, inflow_pressure, inflow_temperature, inflow_mw;
+  double inflow_sv[ORC_MAX_SPEC];
 } orc_param;
 
 /* A face shared by two blocks of a multi-block mesh, as InnerFace holds it

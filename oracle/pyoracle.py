@@ -42,6 +42,9 @@ class orc_param(ctypes.Structure):
         ("faces", orc_face * 6), ("mech", ctypes.c_void_p), ("shock_sensor", ctypes.c_int),
         ("sensor_eps", ctypes.c_double), ("wall_thermal_type", ctypes.c_int), ("wall_catalytic_type", ctypes.c_int),
         ("wall_temperature", ctypes.c_double), ("wall_yk", ctypes.c_double * 20),
+        ("inflow_subsonic", ctypes.c_int), ("inflow_density", ctypes.c_double), ("inflow_u", ctypes.c_double),
+        ("inflow_v", ctypes.c_double), ("inflow_w", ctypes.c_double), ("inflow_pressure", ctypes.c_double),
+        ("inflow_temperature", ctypes.c_double), ("inflow_mw", ctypes.c_double), ("inflow_sv", ctypes.c_double * 20),
     ]
 
 
@@ -212,9 +215,10 @@ class OracleZone:
             setattr(self.z, k, _ptr(a))
         self.p = orc_param()
         for k, v in c.param.items():
-            if k == "wall_yk":
+            if k in ("wall_yk", "inflow_sv"):
+                arr = getattr(self.p, k)
                 for l, y in enumerate(v):
-                    self.p.wall_yk[l] = y
+                    arr[l] = y
             elif k in dict(orc_param._fields_):
                 setattr(self.p, k, v)
         self.p.n_face = len(c.faces)
