@@ -281,6 +281,15 @@ def with_inflow(case: Case, rho: float, u: float, p: float, v: float = 0.0, w: f
     return dataclasses.replace(case, param=param, faces=new_faces, name=case.name + "_inflow")
 
 
+def with_back_pressure(case: Case, p_back: float) -> Case:
+    """Copy of `case` whose outflow faces hold the back pressure p_back
+    where the flow leaving them is subsonic (the reference's
+    if_backPressure / backPressure)."""
+    param = dict(case.param)
+    param.update(outflow_back_pressure_on=1, outflow_back_pressure=p_back)
+    return dataclasses.replace(case, param=param, name=case.name + "_pback")
+
+
 def split_i(case: Case, h: int, periodic_i: bool | None = None):
     """Two blocks cut from `case` along i, sharing the node plane i = h:
     A holds nodes 0..h, B nodes h..mx-1.  Every padded array is sliced from

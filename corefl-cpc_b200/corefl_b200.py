@@ -47,6 +47,10 @@ class cfk_inflow(ctypes.Structure):
         "density", "u", "v", "w", "pressure", "temperature", "mw")] + [("sv", ctypes.c_double * 9)]
 
 
+class cfk_outflow(ctypes.Structure):
+    _fields_ = [("back_pressure_on", ctypes.c_int), ("back_pressure", ctypes.c_double)]
+
+
 class cfk_param(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int), ("n_var", ctypes.c_int), ("n_spec", ctypes.c_int), ("n_scalar", ctypes.c_int),
@@ -58,7 +62,7 @@ class cfk_param(ctypes.Structure):
         ("cfl", ctypes.c_double), ("dt", ctypes.c_double), ("weno_eps_scale", ctypes.c_double),
         ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double), ("sensor_threshold", ctypes.c_double),
         ("device", ctypes.c_int), ("shock_sensor", ctypes.c_int), ("sensor_eps", ctypes.c_double),
-        ("wall", cfk_wall), ("inflow", cfk_inflow),
+        ("wall", cfk_wall), ("inflow", cfk_inflow), ("outflow", cfk_outflow),
     ]
 
 
@@ -288,6 +292,8 @@ def make_param(p: dict, faces) -> cfk_param:
             setattr(cp.wall, k[5:], v)
         elif k.startswith("inflow_"):
             setattr(cp.inflow, k[7:], v)
+        elif k.startswith("outflow_"):
+            setattr(cp.outflow, k[8:], v)
         elif k in dict(cfk_param._fields_):
             setattr(cp, k, v)
     cp.n_face = len(faces)

@@ -33,8 +33,8 @@ cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
                             cudaStream_t st, bool with_reaction = true);
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
-                                       int n_face, const cfk_wall &wall, const cfk_inflow &inflow, cudaStream_t st,
-                                       int *n_launch);
+                                       int n_face, const cfk_wall &wall, const cfk_inflow &inflow,
+                                       const cfk_outflow &outflow, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
 cudaError_t launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t st);
 cudaError_t launch_inner_communication(const Zone &z, const Zone &tz, const Param &p, const Thermo *th,
@@ -165,6 +165,12 @@ int validate(const cfk_param *p, std::string &why) {
         !(f.label == 6 || f.label == 8 || f.label == 3 || f.label == 2 || f.label == 5)) {
       why = "unsupported boundary face description";
       return -1;
+    }
+    if (f.label == 6 && p->outflow.back_pressure_on) {
+      if (p->outflow.back_pressure_on != 1 || !(p->outflow.back_pressure > 0)) {
+        why = "outflow back pressure: back_pressure_on must be 0 or 1 and back_pressure > 0";
+        return -1;
+      }
     }
     if (f.label == 5) {
       const cfk_inflow &q = p->inflow;
@@ -581,7 +587,7 @@ int cfk_compute_cv_from_bv(cfk_ctx *c, void *stream) {
 int cfk_apply_boundary_conditions(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
   int n = 0;
-  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, S(stream), &n),
+  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, S(stream), &n),
             "boundary conditions");
   c->launches += n;
   return CFK_OK;
@@ -702,7 +708,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_BC, st, &n);
-      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, st, &n), "boundary conditions");
+      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, st, &n), "boundary conditions");
     }
     {
       PhaseScope ps(c, CFK_PH_PROPS, st, &n);
@@ -751,7 +757,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
             "wu_reaction_step");
   ++n;
-  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, st, &n), "boundary conditions");
+  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, st, &n), "boundary conditions");
   CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
   ++n;
   // wu_RK_subStep (:564-634): SSP-RK3 over dt/2 on dq - Cn, no property update
@@ -763,7 +769,7 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
     CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;
-    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, st, &n), "boundary conditions");
+    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, st, &n), "boundary conditions");
   }
   c->launches += n;
   if (dt_used) *dt_used = dt;

@@ -259,8 +259,17 @@ __device__ __forceinline__ bool face_work(const FaceGeom &fg, int g, int &i, int
   return true;
 }
 
+// apply_outflow (reference src/BoundCond.cu:2065-2188).  Plain outflow: the
+// ghost layers copy the face node.  With a back pressure: where the face's
+// normal Mach number (gamma from the mixture's cp at the face) is below 1,
+// the state at the face is the characteristic one at the back pressure,
+// rho_b = rho1 + (p_b - p1)/c1^2, V_b = V1 - (p_b - p1)/(rho1 c1) n from the
+// inner node, and the ghosts reflect the inner nodes about it (mass
+// fractions about the face's); otherwise the ghosts copy the face state.  The
+// face node itself is left as it is, as in the reference, so every thread
+// reads only the face node and inner nodes and the i-face split is safe.
 template <bool MIX>
-__global__ void bc_outflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg) {
+__global__ void bc_outflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg, cfk_outflow of) {
   const Dims d = z.d;
   const int g = d.ngg;
   int i, j, k, gg_lo, gg_hi;
@@ -268,11 +277,93 @@ __global__ void bc_outflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg
   if (!face_work(fg, g, i, j, k, gg_lo, gg_hi, face_part)) return;
   const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
   const int64_t s = d.stride(g, fg.face) * fg.direction;
-  for (int gg = gg_lo; gg <= gg_hi; ++gg) {
-    const int64_t gi = id + gg * s;
-    for (int l = 0; l < 6; ++l) z.bv[gi + l * sz] = z.bv[id + l * sz];
-    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[id + l * sz];
-    cv_from_bv_point<MIX>(z, p, th, gi);
+  if (!of.back_pressure_on) {
+    for (int gg = gg_lo; gg <= gg_hi; ++gg) {
+      const int64_t gi = id + gg * s;
+      for (int l = 0; l < 6; ++l) z.bv[gi + l * sz] = z.bv[id + l * sz];
+      for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[id + l * sz];
+      cv_from_bv_point<MIX>(z, p, th, gi);
+    }
+    return;
+  }
+  if (gg_lo > gg_hi) return;
+  const int mf = 3 * fg.face;
+  double nx = z.metric[id + mf * sz], ny = z.metric[id + (mf + 1) * sz], nz = z.metric[id + (mf + 2) * sz];
+  const double grad_n_inv = fg.direction / sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= grad_n_inv;
+  ny *= grad_n_inv;
+  nz *= grad_n_inv;
+  double u_b = z.bv[id + sz], v_b = z.bv[id + 2 * sz], w_b = z.bv[id + 3 * sz];
+  const double u_face = nx * u_b + ny * v_b + nz * w_b;
+  double p_b = z.bv[id + 4 * sz], rho_b = z.bv[id];
+  double gamma = kGammaAir;
+  double yk_b[kMaxSpec];
+  if (MIX) {
+    double cpk[kMaxSpec];
+    compute_cp(th, z.bv[id + 5 * sz], cpk);
+    double cp = 0, R = 0;
+    for (int l = 0; l < p.n_spec; ++l) {
+      yk_b[l] = z.sv[id + l * sz];
+      cp += z.sv[id + l * sz] * cpk[l];
+      R += z.sv[id + l * sz] * th->gas_const[l];
+    }
+    gamma = cp / (cp - R);
+  }
+  const double a_b = sqrt(gamma * p_b / rho_b);
+  const double mach_b = fabs(u_face / a_b);
+  if (mach_b < 1) {
+    p_b = of.back_pressure;
+    const int64_t i1 = id - s;
+    const double d1 = z.bv[i1], u1 = z.bv[i1 + sz], v1 = z.bv[i1 + 2 * sz], w1 = z.bv[i1 + 3 * sz];
+    const double p1 = z.bv[i1 + 4 * sz];
+    gamma = kGammaAir;
+    if (MIX) {
+      double cpk[kMaxSpec];
+      compute_cp(th, z.bv[i1 + 5 * sz], cpk);
+      double cp = 0, R = 0;
+      for (int l = 0; l < p.n_spec; ++l) {
+        cp += z.sv[i1 + l * sz] * cpk[l];
+        R += z.sv[i1 + l * sz] * th->gas_const[l];
+      }
+      gamma = cp / (cp - R);
+    }
+    const double c1 = sqrt(gamma * p1 / d1);
+    const double temp = (p_b - p1) / c1;
+    rho_b = d1 + temp / c1;
+    u_b = u1 - nx * temp / d1;
+    v_b = v1 - ny * temp / d1;
+    w_b = w1 - nz * temp / d1;
+    for (int gg = gg_lo; gg <= gg_hi; ++gg) {
+      const int64_t gi = id + gg * s, ii = id - gg * s;
+      const double p_g = 2 * p_b - z.bv[ii + 4 * sz], rho_g = 2 * rho_b - z.bv[ii];
+      z.bv[gi] = rho_g;
+      z.bv[gi + sz] = 2 * u_b - z.bv[ii + sz];
+      z.bv[gi + 2 * sz] = 2 * v_b - z.bv[ii + 2 * sz];
+      z.bv[gi + 3 * sz] = 2 * w_b - z.bv[ii + 3 * sz];
+      z.bv[gi + 4 * sz] = p_g;
+      double R = kRAir;
+      if (MIX) {
+        R = 0;
+        for (int l = 0; l < p.n_spec; ++l) {
+          z.sv[gi + l * sz] = 2 * yk_b[l] - z.sv[ii + l * sz];
+          R += z.sv[gi + l * sz] * th->gas_const[l];
+        }
+      }
+      z.bv[gi + 5 * sz] = p_g / (rho_g * R);
+      cv_from_bv_point<MIX>(z, p, th, gi);
+    }
+  } else {
+    for (int gg = gg_lo; gg <= gg_hi; ++gg) {
+      const int64_t gi = id + gg * s;
+      z.bv[gi] = rho_b;
+      z.bv[gi + sz] = u_b;
+      z.bv[gi + 2 * sz] = v_b;
+      z.bv[gi + 3 * sz] = w_b;
+      z.bv[gi + 4 * sz] = p_b;
+      z.bv[gi + 5 * sz] = z.bv[id + 5 * sz];
+      for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = z.sv[id + l * sz];
+      cv_from_bv_point<MIX>(z, p, th, gi);
+    }
   }
 }
 
@@ -627,8 +718,8 @@ static FaceGeom make_face(const Dims &d, const cfk_face &f) {
 }
 
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
-                                       int n_face, const cfk_wall &wall, const cfk_inflow &inflow, cudaStream_t st,
-                                       int *n_launch) {
+                                       int n_face, const cfk_wall &wall, const cfk_inflow &inflow,
+                                       const cfk_outflow &outflow, cudaStream_t st, int *n_launch) {
   // reference priority order: outflow, inflow, symmetry, wall, periodic
   static const int order[5] = {6, 5, 3, 2, 8};
   for (int o = 0; o < 5; ++o) {
@@ -640,8 +731,8 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
       const int blocks = (cnt + 127) / 128;
       const bool mix = p.n_spec > 0;
       if (order[o] == 6) {
-        if (mix) bc_outflow_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
-        else bc_outflow_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);
+        if (mix) bc_outflow_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg, outflow);
+        else bc_outflow_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg, outflow);
       } else if (order[o] == 3) {
         if (mix) bc_symmetry_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg);
         else bc_symmetry_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg);

@@ -212,6 +212,36 @@ bool read_inflow(const Setup &s, cfk_inflow &q, std::string &err) {
   return true;
 }
 
+// The outflow condition of the boundary_conditions list (reference
+// src/BoundCond.cpp:597-618, Outflow::Outflow): if_backPressure and
+// backPressure.  A non-reflecting outflow is not part of this path and is
+// reported; so are two outflow structs with different back pressures.
+bool read_outflow(const Setup &s, cfk_outflow &o, std::string &err) {
+  o.back_pressure_on = 0;
+  o.back_pressure = 0;
+  auto list = s.arrays.find("boundary_conditions");
+  if (list == s.arrays.end()) return true;
+  int n_outflow = 0;
+  for (const std::string &name : list->second) {
+    auto it = s.structs.find(name);
+    if (it == s.structs.end() || struct_string(it->second, "type") != "outflow") continue;
+    const Struct &st = it->second;
+    if (struct_int(st, "nonReflecting", 0) > 0) {
+      err = "outflow " + name + ": non-reflecting outflow is not supported";
+      return false;
+    }
+    const int on = struct_int(st, "if_backPressure", 0);
+    const double pb = on == 1 ? struct_real(st, "backPressure", -1) : 0;
+    if (n_outflow++ > 0 && (on != o.back_pressure_on || pb != o.back_pressure)) {
+      err = "outflow conditions differ; cfk_param carries one";
+      return false;
+    }
+    o.back_pressure_on = on;
+    o.back_pressure = pb;
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char *errbuf, size_t err_len) {
@@ -272,6 +302,7 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
   p.weno_eps_scale = p.rho_ref * p.v_ref * p.rho_ref * p.v_ref;
   if (!read_wall(s, p.wall, err)) return report(err);
   if (!read_inflow(s, p.inflow, err)) return report(err);
+  if (!read_outflow(s, p.outflow, err)) return report(err);
   p.n_face = 0;
   *out = p;
   return CFK_OK;

@@ -41,7 +41,7 @@ typedef struct cfk_ctx cfk_ctx;
 /* A boundary face of the block (reference src/Mesh.cpp:14-31, Boundary).
  * face 0/1/2 = i/j/k, direction -1 = min side, +1 = max side;
  * label 6 = outflow, 8 = periodic, 3 = symmetry, 2 = no-slip wall (cfk_param.wall),
- * 5 = inflow (cfk_param.inflow). */
+ * 5 = inflow (cfk_param.inflow); outflow faces read cfk_param.outflow. */
 typedef struct cfk_face {
   int face, direction, label;
 } cfk_face;
@@ -89,6 +89,15 @@ typedef struct cfk_inflow {
   double sv[CFK_MAX_SPEC];
 } cfk_inflow;
 
+/* The outflow of the faces labelled 6 (reference src/BoundCond.h:125-134,
+ * Outflow).  back_pressure_on = the reference's if_backPressure: where the
+ * face's normal Mach number is below 1 the ghosts carry the characteristic
+ * state at back_pressure; otherwise (and without it) they copy the face. */
+typedef struct cfk_outflow {
+  int back_pressure_on;
+  double back_pressure;
+} cfk_outflow;
+
 /* Scalar settings of the path: the DParameter fields it reads
  * (reference src/DParameter.cuh:13-207) plus the boundary list. */
 typedef struct cfk_param {
@@ -118,6 +127,7 @@ typedef struct cfk_param {
   double sensor_eps;       /* shockSensor_epsilon (reference default -1) */
   cfk_wall wall;           /* read for faces labelled 2 */
   cfk_inflow inflow;       /* read for faces labelled 5 */
+  cfk_outflow outflow;     /* read for faces labelled 6 */
 } cfk_param;
 
 /* Device pointers of one block, field for field the arrays of the reference's

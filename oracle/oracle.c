@@ -850,15 +850,90 @@ static void apply_outflow_face(orc_zone *z, const orc_param *p, const orc_face *
   int lo[3], hi[3];
   face_range(z, f, lo, hi);
   const long s = pstride(z, g, f->face) * f->direction;
+  const int ns = p->mech ? p->n_spec : 0;
+  double *bv = z->bv, *sv = z->sv;
   for (int k = lo[2]; k <= hi[2]; ++k)
     for (int j = lo[1]; j <= hi[1]; ++j)
       for (int i = lo[0]; i <= hi[0]; ++i) {
         const long id = pidx(z, g, i, j, k);
-        for (int gg = 1; gg <= g; ++gg) {
-          const long gi = id + gg * s;
-          for (int l = 0; l < 6; ++l) z->bv[gi + l * sz] = z->bv[id + l * sz];
-          for (int l = 0; l < p->n_scalar; ++l) z->sv[gi + l * sz] = z->sv[id + l * sz];
-          cv_from_bv_point(z, p, gi);
+        if (!p->outflow_back_pressure_on) {
+          for (int gg = 1; gg <= g; ++gg) {
+            const long gi = id + gg * s;
+            for (int l = 0; l < 6; ++l) bv[gi + l * sz] = bv[id + l * sz];
+            for (int l = 0; l < p->n_scalar; ++l) sv[gi + l * sz] = sv[id + l * sz];
+            cv_from_bv_point(z, p, gi);
+          }
+          continue;
+        }
+        /* back-pressure branch (src/BoundCond.cu:2082-2171) */
+        const int mf = 3 * f->face;
+        const double *mt = z->metric;
+        double nx = mt[id + mf * sz], ny = mt[id + (mf + 1) * sz], nz = mt[id + (mf + 2) * sz];
+        const double grad_n_inv = f->direction / sqrt(nx * nx + ny * ny + nz * nz);
+        nx *= grad_n_inv; ny *= grad_n_inv; nz *= grad_n_inv;
+        double u_b = bv[id + sz], v_b = bv[id + 2 * sz], w_b = bv[id + 3 * sz];
+        const double u_face = nx * u_b + ny * v_b + nz * w_b;
+        double p_b = bv[id + 4 * sz], rho_b = bv[id];
+        double gamma = GAMMA_AIR, yk_b[ORC_MAX_SPEC], cpk[ORC_MAX_SPEC];
+        if (ns > 0) {
+          orc_cp(p->mech, bv[id + 5 * sz], cpk);
+          double cp = 0, R = 0;
+          for (int l = 0; l < ns; ++l) {
+            yk_b[l] = sv[id + l * sz];
+            cp += sv[id + l * sz] * cpk[l];
+            R += sv[id + l * sz] * p->mech->gas_const[l];
+          }
+          gamma = cp / (cp - R);
+        }
+        const double a_b = sqrt(gamma * p_b / rho_b);
+        const double mach_b = fabs(u_face / a_b);
+        if (mach_b < 1) {
+          p_b = p->outflow_back_pressure;
+          const long i1 = id - s;
+          const double d1 = bv[i1], u1 = bv[i1 + sz], v1 = bv[i1 + 2 * sz], w1 = bv[i1 + 3 * sz], p1 = bv[i1 + 4 * sz];
+          gamma = GAMMA_AIR;
+          if (ns > 0) {
+            orc_cp(p->mech, bv[i1 + 5 * sz], cpk);
+            double cp = 0, R = 0;
+            for (int l = 0; l < ns; ++l) {
+              cp += sv[i1 + l * sz] * cpk[l];
+              R += sv[i1 + l * sz] * p->mech->gas_const[l];
+            }
+            gamma = cp / (cp - R);
+          }
+          const double c1 = sqrt(gamma * p1 / d1);
+          const double temp = (p_b - p1) / c1;
+          rho_b = d1 + temp / c1;
+          u_b = u1 - nx * temp / d1;
+          v_b = v1 - ny * temp / d1;
+          w_b = w1 - nz * temp / d1;
+          for (int gg = 1; gg <= g; ++gg) {
+            const long gi = id + gg * s, ii = id - gg * s;
+            const double p_g = 2 * p_b - bv[ii + 4 * sz], rho_g = 2 * rho_b - bv[ii];
+            bv[gi] = rho_g;
+            bv[gi + sz] = 2 * u_b - bv[ii + sz];
+            bv[gi + 2 * sz] = 2 * v_b - bv[ii + 2 * sz];
+            bv[gi + 3 * sz] = 2 * w_b - bv[ii + 3 * sz];
+            bv[gi + 4 * sz] = p_g;
+            double R = R_AIR;
+            if (ns > 0) {
+              R = 0;
+              for (int l = 0; l < ns; ++l) {
+                sv[gi + l * sz] = 2 * yk_b[l] - sv[ii + l * sz];
+                R += sv[gi + l * sz] * p->mech->gas_const[l];
+              }
+            }
+            bv[gi + 5 * sz] = p_g / (rho_g * R);
+            cv_from_bv_point(z, p, gi);
+          }
+        } else {
+          for (int gg = 1; gg <= g; ++gg) {
+            const long gi = id + gg * s;
+            bv[gi] = rho_b; bv[gi + sz] = u_b; bv[gi + 2 * sz] = v_b; bv[gi + 3 * sz] = w_b;
+            bv[gi + 4 * sz] = p_b; bv[gi + 5 * sz] = bv[id + 5 * sz];
+            for (int l = 0; l < p->n_scalar; ++l) sv[gi + l * sz] = sv[id + l * sz];
+            cv_from_bv_point(z, p, gi);
+          }
         }
       }
 }

@@ -101,6 +101,9 @@ typedef struct {
   int inflow_subsonic;
   double inflow_density, inflow_u, inflow_v, inflow_w, inflow_pressure, inflow_temperature, inflow_mw;
   double inflow_sv[ORC_MAX_SPEC];
+  /* outflow faces (src/BoundCond.h:125-134): if_backPressure, backPressure */
+  int outflow_back_pressure_on;
+  double outflow_back_pressure;
 } orc_param;
 
 /* A face shared by two blocks of a multi-block mesh, as InnerFace holds it

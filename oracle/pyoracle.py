@@ -45,6 +45,7 @@ class orc_param(ctypes.Structure):
         ("inflow_subsonic", ctypes.c_int), ("inflow_density", ctypes.c_double), ("inflow_u", ctypes.c_double),
         ("inflow_v", ctypes.c_double), ("inflow_w", ctypes.c_double), ("inflow_pressure", ctypes.c_double),
         ("inflow_temperature", ctypes.c_double), ("inflow_mw", ctypes.c_double), ("inflow_sv", ctypes.c_double * 20),
+        ("outflow_back_pressure_on", ctypes.c_int), ("outflow_back_pressure", ctypes.c_double),
     ]
 
 
