@@ -146,8 +146,8 @@ int validate(const cfk_param *p, std::string &why) {
     why = "passive scalars beside the species are not supported (n_scalar must equal n_spec)";
     return -1;
   }
-  if (p->n_spec > 0 && p->viscous_order > 0 && p->gradPInDiffusionFlux) {
-    why = "gradPInDiffusionFlux is not supported";
+  if (p->gradPInDiffusionFlux != 0 && p->gradPInDiffusionFlux != 1) {
+    why = "gradPInDiffusionFlux must be 0 or 1";
     return -1;
   }
   if (s == 0 && p->n_spec == 0) { why = "inviscid_scheme 0 (no flux) is for reacting mixtures only"; return -1; }

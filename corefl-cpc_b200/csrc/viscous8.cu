@@ -98,7 +98,7 @@ __device__ __forceinline__ void grad3(const double *f, int64_t sj, int64_t sk, i
 // NS = 0: calorically perfect air
 template <int NS, int ORDER>
 __global__ void __launch_bounds__(128) visc8_collocated(Zone z, double *fvis, Bnd b, double Pr,
-                                                        const __grid_constant__ Thermo thermo) {
+                                                        const __grid_constant__ Thermo thermo, int gradp) {
   constexpr int NV = 5 + NS;
   const Dims d = z.d;
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
@@ -192,6 +192,27 @@ __global__ void __launch_bounds__(128) visc8_collocated(Zone z, double *fvis, Bn
     c0 -= mw_tot * sum_rhoDkYk * sx;
     c1 -= mw_tot * sum_rhoDkYk * sy;
     c2 -= mw_tot * sum_rhoDkYk * szt;
+    if (gradp) {  // pressure-gradient term of the driving force (reference src/ViscousScheme.cu:495-520)
+      double p_xi, p_eta, p_zeta;
+      grad3<ORDER>(z.bv + 4 * sz + id, sj, sk, i, j, k, d, b, p_xi, p_eta, p_zeta);
+      const double p_x = p_xi * xi_x + p_eta * eta_x + p_zeta * zeta_x;
+      const double p_y = p_xi * xi_y + p_eta * eta_y + p_zeta * zeta_y;
+      const double p_z = p_xi * xi_z + p_eta * eta_z + p_zeta * zeta_z;
+      const double pn = z.bv[id + 4 * sz];
+      const double gxp = (xi_x * p_x + xi_y * p_y + xi_z * p_z) / pn;
+      const double gyp = (eta_x * p_x + eta_y * p_y + eta_z * p_z) / pn;
+      const double gzp = (zeta_x * p_x + zeta_y * p_y + zeta_z * p_z) / pn;
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        const double coefficient = (mw_tot * th->imw[l] - 1) * yk[l];
+        dfx[l] += coefficient * gxp;
+        dfy[l] += coefficient * gyp;
+        dfz[l] += coefficient * gzp;
+        c0 += coefficient * gxp * diffusivity[l];
+        c1 += coefficient * gyp * diffusivity[l];
+        c2 += coefficient * gzp * diffusivity[l];
+      }
+    }
     double h[NS], cp_unused[NS];
     enthalpy_cp_ns<NS>(th, z.bv[id + 5 * sz], h, cp_unused);
 #pragma unroll
@@ -276,10 +297,11 @@ cudaError_t launch_viscous8(const Zone &z, const Param &p, const Thermo *th, con
   const dim3 grid((d.mx + 127) / 128, d.my, d.mz);
   static const Thermo no_thermo{};
   const bool o4 = p.viscous_order == 4;
-  if (th && o4) visc8_collocated<kMaxSpec, 4><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th);
-  else if (th) visc8_collocated<kMaxSpec, 8><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th);
-  else if (o4) visc8_collocated<0, 4><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo);
-  else visc8_collocated<0, 8><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo);
+  const int gradp = p.gradPInDiffusionFlux;
+  if (th && o4) visc8_collocated<kMaxSpec, 4><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th, gradp);
+  else if (th) visc8_collocated<kMaxSpec, 8><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, *th, gradp);
+  else if (o4) visc8_collocated<0, 4><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo, 0);
+  else visc8_collocated<0, 8><<<grid, 128, 0, st>>>(z, fvis, b, p.Pr, no_thermo, 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   *n_launch += 1;

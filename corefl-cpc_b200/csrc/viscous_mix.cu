@@ -6,8 +6,10 @@
 // Y_k grad W / W) with the correction velocity, and the enthalpy flux
 // sum h_k J_k at the face temperature), and compute_dFv_dx / dGv_dy / dHv_dz
 // (:75-127).  Same face tiling as viscous_air.cu; the face fluxes of all
-// 4 + NS viscous components stay in shared memory.  The optional
-// grad-p term of the diffusion flux (gradPInDiffusionFlux) is not included.
+// 4 + NS viscous components stay in shared memory.  With gradp set the
+// diffusion driving force also carries the pressure-gradient term
+// (W/W_k - 1) Y_k grad(xi).grad(p) / p of gradPInDiffusionFlux (reference
+// src/ViscousScheme.cu:742-766, 931-955, 1115-1139), p taken at the face.
 #include "cfk_common.cuh"
 #include "chem_fast.cuh"
 #include "thermo.cuh"
@@ -30,7 +32,8 @@ struct VisMixTile {
 }  // namespace
 
 template <int DIR, int NS>
-__global__ void __launch_bounds__(256) viscous_mix_flux_diff(Zone z, const __grid_constant__ Thermo thermo) {
+__global__ void __launch_bounds__(256) viscous_mix_flux_diff(Zone z, const __grid_constant__ Thermo thermo,
+                                                             int gradp) {
   using T = VisMixTile<DIR, NS>;
   constexpr int TN = T::TN, C = T::C, NF = T::NF;
   const Thermo *th = &thermo;
@@ -135,6 +138,22 @@ __global__ void __launch_bounds__(256) viscous_mix_flux_diff(Zone z, const __gri
     }
     mw_tot = 1.0 / mw_tot;
     correction -= mw_tot * sum_rhoDkYk * sum_grad_over_w;
+    if (gradp) {
+      const double *pp = pv + 4 * sz;
+      double d3[3];
+      d3[DIR] = pp[idn] - pp[id];
+      d3[DA] = 0.25 * (pp[id + sa] - pp[id - sa] + pp[idn + sa] - pp[idn - sa]);
+      d3[DB] = 0.25 * (pp[id + sb] - pp[id - sb] + pp[idn + sb] - pp[idn - sb]);
+      const double p_x = d3[0] * gm[0] + d3[1] * gm[3] + d3[2] * gm[6];
+      const double p_y = d3[0] * gm[1] + d3[1] * gm[4] + d3[2] * gm[7];
+      const double p_z = d3[0] * gm[2] + d3[1] * gm[5] + d3[2] * gm[8];
+      const double gp = (gk0 * p_x + gk1 * p_y + gk2 * p_z) / (0.5 * (pp[idn] + pp[id]));
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        ddf[l] += (mw_tot * th->imw[l] - 1) * yk[l] * gp;
+        correction += (mw_tot * th->imw[l] - 1) * yk[l] * gp * diffusivity[l];
+      }
+    }
     double h[NS], cp_unused[NS];
     enthalpy_cp_ns<NS>(th, 0.5 * (pv[id + 5 * sz] + pv[idn + 5 * sz]), h, cp_unused);
 #pragma unroll
@@ -163,14 +182,14 @@ __global__ void __launch_bounds__(256) viscous_mix_flux_diff(Zone z, const __gri
 namespace {
 
 template <int DIR>
-cudaError_t launch_vis_mix_dir(const Zone &z, const Thermo &th, cudaStream_t st) {
+cudaError_t launch_vis_mix_dir(const Zone &z, const Thermo &th, int gradp, cudaStream_t st) {
   using T = VisMixTile<DIR, kMaxSpec>;
   const Dims &d = z.d;
   dim3 grid;
   if (DIR == 0) grid = dim3((d.mx + T::TN - 1) / T::TN, (d.my + T::C - 1) / T::C, d.mz);
   else if (DIR == 1) grid = dim3((d.mx + T::C - 1) / T::C, (d.my + T::TN - 1) / T::TN, d.mz);
   else grid = dim3((d.mx + T::C - 1) / T::C, (d.mz + T::TN - 1) / T::TN, d.my);
-  viscous_mix_flux_diff<DIR, kMaxSpec><<<grid, T::NT, T::smem_bytes(), st>>>(z, th);
+  viscous_mix_flux_diff<DIR, kMaxSpec><<<grid, T::NT, T::smem_bytes(), st>>>(z, th, gradp);
   return cudaGetLastError();
 }
 
@@ -190,14 +209,14 @@ cudaError_t viscous_mix_init_attributes() {
 }
 
 cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch) {
-  (void)p;
-  cudaError_t e = launch_vis_mix_dir<0>(z, th, st);
+  const int gradp = p.gradPInDiffusionFlux;
+  cudaError_t e = launch_vis_mix_dir<0>(z, th, gradp, st);
   if (e != cudaSuccess) return e;
-  e = launch_vis_mix_dir<1>(z, th, st);
+  e = launch_vis_mix_dir<1>(z, th, gradp, st);
   if (e != cudaSuccess) return e;
   *n_launch += 2;
   if (z.d.mz > 1) {
-    e = launch_vis_mix_dir<2>(z, th, st);
+    e = launch_vis_mix_dir<2>(z, th, gradp, st);
     if (e != cudaSuccess) return e;
     *n_launch += 1;
   }

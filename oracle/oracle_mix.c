@@ -474,7 +474,8 @@ void orc_positive_preserving_face(const orc_zone *z, const orc_param *p, int dir
 
 /* ------------------------------------------------------------------------ */
 /* Species diffusion part of the viscous face flux (src/ViscousScheme.cu:    */
-/* 700-770 and the g/h analogues), without the optional grad-p term.         */
+/* 700-790 and the g/h analogues), with the grad-p term of                   */
+/* gradPInDiffusionFlux (:742-766, 931-955, 1115-1139) when it is set.       */
 /* ------------------------------------------------------------------------ */
 void orc_viscous_species_face(const orc_zone *z, const orc_param *p, int dir, int i, int j, int k,
                               const double gm[9], const double gk[3], double *fv) {
@@ -507,6 +508,21 @@ void orc_viscous_species_face(const orc_zone *z, const orc_param *p, int dir, in
   }
   mw_tot = 1.0 / mw_tot;
   CorrectionVelocityTerm -= mw_tot * sum_rhoDkYk * sum_GradXi_cdot_GradY_over_wl;
+  if (p->gradPInDiffusionFlux) {
+    const double *pv = z->bv + 4 * sz;
+    double d3[3];
+    d3[dir] = pv[idn] - pv[id];
+    d3[da] = 0.25 * (pv[id + sa] - pv[id - sa] + pv[idn + sa] - pv[idn - sa]);
+    d3[db] = 0.25 * (pv[id + sb] - pv[id - sb] + pv[idn + sb] - pv[idn - sb]);
+    const double p_x = d3[0] * gm[0] + d3[1] * gm[3] + d3[2] * gm[6];
+    const double p_y = d3[0] * gm[1] + d3[1] * gm[4] + d3[2] * gm[7];
+    const double p_z = d3[0] * gm[2] + d3[1] * gm[5] + d3[2] * gm[8];
+    const double gradXi_cdot_gradP_over_p = (gk[0] * p_x + gk[1] * p_y + gk[2] * p_z) / (0.5 * (pv[idn] + pv[id]));
+    for (int l = 0; l < ns; ++l) {
+      ddf[l] += (mw_tot * m->imw[l] - 1) * yk[l] * gradXi_cdot_gradP_over_p;
+      CorrectionVelocityTerm += (mw_tot * m->imw[l] - 1) * yk[l] * gradXi_cdot_gradP_over_p * diffusivity[l];
+    }
+  }
   double h[ORC_MAX_SPEC];
   const double tm = 0.5 * (z->bv[id + 5 * sz] + z->bv[idn + 5 * sz]);
   orc_enthalpy(m, tm, h);

@@ -170,7 +170,8 @@ static void collocated(orc_zone *z, const orc_param *p, const int bt[3][2]) {
         gv[id + 4 * sz] = eta_x * Ex + eta_y * Ey + eta_z * Ez;
         hv[id + 4 * sz] = zeta_x * Ex + zeta_y * Ey + zeta_z * Ez;
         if (!m) continue;
-        /* species diffusion (collocated_scalar), no grad-p term */
+        /* species diffusion (collocated_scalar), with the grad-p term of
+         * gradPInDiffusionFlux when it is set (src/ViscousScheme.cu:495-520) */
         double diffusivity[ORC_MAX_SPEC], yk[ORC_MAX_SPEC], dfx[ORC_MAX_SPEC], dfy[ORC_MAX_SPEC], dfz[ORC_MAX_SPEC];
         double sx = 0, sy = 0, szz = 0, sum_rhoDkYk = 0, cv0 = 0, cv1 = 0, cv2 = 0, mw_tot = 0;
         for (int l = 0; l < ns; ++l) {
@@ -202,6 +203,27 @@ static void collocated(orc_zone *z, const orc_param *p, const int bt[3][2]) {
         cv0 -= mw_tot * sum_rhoDkYk * sx;
         cv1 -= mw_tot * sum_rhoDkYk * sy;
         cv2 -= mw_tot * sum_rhoDkYk * szz;
+        if (p->gradPInDiffusionFlux) {
+          const double *pp = bv + 4 * sz;
+          const double p_xi = d8(pp, id, 1, i, mx, bt[0][0], bt[0][1]);
+          const double p_eta = d8(pp, id, sj, j, my, bt[1][0], bt[1][1]);
+          const double p_zeta = d8(pp, id, sk, k, mz, bt[2][0], bt[2][1]);
+          const double p_x = p_xi * xi_x + p_eta * eta_x + p_zeta * zeta_x;
+          const double p_y = p_xi * xi_y + p_eta * eta_y + p_zeta * zeta_y;
+          const double p_z = p_xi * xi_z + p_eta * eta_z + p_zeta * zeta_z;
+          const double gxp = (xi_x * p_x + xi_y * p_y + xi_z * p_z) / pp[id];
+          const double gyp = (eta_x * p_x + eta_y * p_y + eta_z * p_z) / pp[id];
+          const double gzp = (zeta_x * p_x + zeta_y * p_y + zeta_z * p_z) / pp[id];
+          for (int l = 0; l < ns; ++l) {
+            const double coefficient = (mw_tot * m->imw[l] - 1) * yk[l];
+            dfx[l] += coefficient * gxp;
+            dfy[l] += coefficient * gyp;
+            dfz[l] += coefficient * gzp;
+            cv0 += coefficient * gxp * diffusivity[l];
+            cv1 += coefficient * gyp * diffusivity[l];
+            cv2 += coefficient * gzp * diffusivity[l];
+          }
+        }
         double h[ORC_MAX_SPEC];
         orc_enthalpy(m, bv[id + 5 * sz], h);
         for (int l = 0; l < ns; ++l) {
