@@ -44,6 +44,16 @@ inline int64_t pidx(int mx, int my, int g, int i, int j, int k) {
 
 int64_t plane_size(int mx, int my, int mz, int g) { return (int64_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g); }
 
+// Appends one variable's node window (nodes widened by g, i fastest) to f,
+// one contiguous i-row per fwrite.
+bool write_window(FILE *f, const double *v, const cfk_plt_block &B, int g) {
+  const size_t row = (size_t)(B.mx + 2 * g);
+  for (int k = -g; k < B.mz + g; ++k)
+    for (int j = -g; j < B.my + g; ++j)
+      if (std::fwrite(v + pidx(B.mx, B.my, B.ngg, -g, j, k), sizeof(double), row, f) != row) return false;
+  return true;
+}
+
 }  // namespace
 
 extern "C" int cfk_write_flowfield(const char *path, const cfk_plt_block *blocks, int n_block, int ngg_output,
@@ -87,20 +97,25 @@ extern "C" int cfk_write_flowfield(const char *path, const cfk_plt_block *blocks
     w.put<int32_t>(0);                       // no auxiliary data
   }
   w.put<float>(357.0f);                      // end of header
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return report(err, err_len, std::string("cannot open ") + path + " for writing", CFK_ERR_IO);
+  bool ok = std::fwrite(w.buf.data(), 1, w.buf.size(), f) == w.buf.size();
   // II. data: per block the zone record, min/max of every variable, then the
-  // variables over the nodes widened by ngg_output, i fastest.
-  for (int b = 0; b < n_block; ++b) {
+  // variables over the nodes widened by ngg_output, i fastest — streamed
+  // row by row, so no copy of the field is held in memory.
+  for (int b = 0; ok && b < n_block; ++b) {
     const cfk_plt_block &B = blocks[b];
     const int64_t P = plane_size(B.mx, B.my, B.mz, B.ngg);
     std::vector<const double *> vars = {B.x, B.y, B.z};
     for (int l = 0; l < 6; ++l) vars.push_back(B.bv + l * P);
     for (int l = 0; l < n_scalar; ++l) vars.push_back(B.sv + l * P);
     for (int l = 0; l < n_other; ++l) vars.push_back(B.ov + l * P);
-    w.put<float>(299.0f);
-    for (int l = 0; l < n_var; ++l) w.put<int32_t>(2);  // double precision
-    w.put<int32_t>(0);                                  // no passive variables
-    w.put<int32_t>(0);                                  // no variable sharing
-    w.put<int32_t>(-1);                                 // no connectivity sharing
+    Writer z;
+    z.put<float>(299.0f);
+    for (int l = 0; l < n_var; ++l) z.put<int32_t>(2);  // double precision
+    z.put<int32_t>(0);                                  // no passive variables
+    z.put<int32_t>(0);                                  // no variable sharing
+    z.put<int32_t>(-1);                                 // no connectivity sharing
     for (const double *v : vars) {
       double lo = v[pidx(B.mx, B.my, B.ngg, -g, -g, -g)], hi = lo;
       for (int k = -g; k < B.mz + g; ++k)
@@ -110,33 +125,26 @@ extern "C" int cfk_write_flowfield(const char *path, const cfk_plt_block *blocks
             lo = std::min(lo, x);
             hi = std::max(hi, x);
           }
-      w.put<double>(lo);
-      w.put<double>(hi);
+      z.put<double>(lo);
+      z.put<double>(hi);
     }
-    for (const double *v : vars)
-      for (int k = -g; k < B.mz + g; ++k)
-        for (int j = -g; j < B.my + g; ++j)
-          for (int i = -g; i < B.mx + g; ++i) w.put<double>(v[pidx(B.mx, B.my, B.ngg, i, j, k)]);
+    ok = std::fwrite(z.buf.data(), 1, z.buf.size(), f) == z.buf.size();
+    for (size_t l = 0; ok && l < vars.size(); ++l) ok = write_window(f, vars[l], B, g);
   }
-  FILE *f = std::fopen(path, "wb");
-  if (!f) return report(err, err_len, std::string("cannot open ") + path + " for writing", CFK_ERR_IO);
-  const size_t n = std::fwrite(w.buf.data(), 1, w.buf.size(), f);
-  const bool ok = n == w.buf.size() && std::fclose(f) == 0;
+  ok = (std::fclose(f) == 0) && ok;
   if (!ok) return report(err, err_len, std::string("short write to ") + path, CFK_ERR_IO);
   return CFK_OK;
 }
 
 namespace {
 
+// Sequential reads from a FILE*; any short read clears ok.
 struct Reader {
-  const std::vector<unsigned char> &buf;
-  size_t at = 0;
+  FILE *f;
   bool ok = true;
   template <class T> T get() {
     T v{};
-    if (at + sizeof(T) > buf.size()) { ok = false; return v; }
-    std::memcpy(&v, buf.data() + at, sizeof(T));
-    at += sizeof(T);
+    if (std::fread(&v, sizeof(T), 1, f) != 1) ok = false;
     return v;
   }
   std::string str() {
@@ -148,9 +156,11 @@ struct Reader {
     }
     return s;
   }
-  void skip(size_t n) {
-    if (at + n > buf.size()) ok = false;
-    else at += n;
+  void skip(int64_t n) {
+    if (ok && std::fseek(f, (long)n, SEEK_CUR) != 0) ok = false;
+  }
+  void read(double *dst, size_t n) {
+    if (ok && std::fread(dst, sizeof(double), n, f) != n) ok = false;
   }
 };
 
@@ -182,14 +192,12 @@ extern "C" int cfk_read_flowfield(const char *path, const cfk_plt_target *blocks
   if (!path || !blocks || n_block < 1 || n_spec < 0) return report(err, err_len, "bad argument", CFK_ERR_ARG);
   FILE *f = std::fopen(path, "rb");
   if (!f) return report(err, err_len, std::string("cannot open ") + path, CFK_ERR_IO);
-  std::vector<unsigned char> buf;
-  unsigned char chunk[1 << 16];
-  for (size_t n; (n = std::fread(chunk, 1, sizeof chunk, f)) > 0;) buf.insert(buf.end(), chunk, chunk + n);
-  std::fclose(f);
-  Reader r{buf};
-  if (buf.size() < 16 || std::memcmp(buf.data(), "#!TDV1", 6) != 0)
+  struct Closer { FILE *f; ~Closer() { std::fclose(f); } } closer{f};
+  Reader r{f};
+  char magic[8] = {0};
+  if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, "#!TDV1", 6) != 0)
     return report(err, err_len, "not a Tecplot binary file", CFK_ERR_IO);
-  r.skip(16);  // magic number, byte order, file type
+  r.skip(8);   // byte order, file type
   r.str();     // title
   const int32_t n_var = r.get<int32_t>();
   if (!r.ok || n_var < 3 || n_var > 4096) return report(err, err_len, "bad variable count", CFK_ERR_IO);
@@ -231,16 +239,21 @@ extern "C" int cfk_read_flowfield(const char *path, const cfk_plt_target *blocks
     const int g = g_file[b];
     const int64_t P = plane_size(B.mx, B.my, B.mz, B.ngg);
     const int64_t N = (int64_t)dims[3 * b] * dims[3 * b + 1] * dims[3 * b + 2];
-    r.skip(4 + 4 * (size_t)n_var + 12 + 16 * (size_t)n_var);  // zone record, formats, flags, min/max pairs
-    for (int l = 0; l < n_var; ++l) {
-      if (label[l] < 0) { r.skip((size_t)N * 8); continue; }
+    r.skip(4 + 4 * (int64_t)n_var + 12 + 16 * (int64_t)n_var);  // zone record, formats, flags, min/max pairs
+    const size_t row = (size_t)(B.mx + 2 * g);
+    for (int l = 0; r.ok && l < n_var; ++l) {
+      if (label[l] < 0) { r.skip(N * 8); continue; }
       double *dst = label[l] < 6 ? B.bv + label[l] * P : B.sv + (label[l] - 6) * P;
       for (int k = -g; k < B.mz + g; ++k)
-        for (int j = -g; j < B.my + g; ++j)
-          for (int i = -g; i < B.mx + g; ++i) dst[pidx(B.mx, B.my, B.ngg, i, j, k)] = r.get<double>();
+        for (int j = -g; j < B.my + g; ++j) r.read(dst + pidx(B.mx, B.my, B.ngg, -g, j, k), row);
     }
     if (!r.ok) return report(err, err_len, "truncated data of zone " + std::to_string(b), CFK_ERR_IO);
   }
+  // fseek past the end of the file succeeds, so a file cut inside the
+  // skipped variables of the last zone shows only here
+  const long end_of_data = std::ftell(f);
+  if (end_of_data < 0 || std::fseek(f, 0, SEEK_END) != 0 || std::ftell(f) < end_of_data)
+    return report(err, err_len, "truncated data of zone " + std::to_string(n_block - 1), CFK_ERR_IO);
   if (solution_time) *solution_time = t;
   return CFK_OK;
 }

@@ -163,9 +163,15 @@ def test_bad_files_are_reported(tmp_path):
     with pytest.raises(cfk.CfkError, match="does not match block 0"):
         cfk.read_flowfield(path, targets[::-1])
     data = path.read_bytes()
-    (tmp_path / "short.plt").write_bytes(data[:-100])
+    B1 = blocks[1]
+    mach_plane = 8 * B1["mx"] * B1["my"] * B1["mz"]
+    (tmp_path / "short.plt").write_bytes(data[:-(mach_plane + 100)])   # cut inside the temperature plane
     with pytest.raises(cfk.CfkError, match="-5: truncated data of zone 1"):
         cfk.read_flowfield(tmp_path / "short.plt", targets)
+    # cut inside the last zone's trailing Mach plane, which the reader skips
+    (tmp_path / "short2.plt").write_bytes(data[:-8])
+    with pytest.raises(cfk.CfkError, match="-5: truncated data of zone 1"):
+        cfk.read_flowfield(tmp_path / "short2.plt", targets)
     (tmp_path / "other.plt").write_bytes(b"hello world, not tecplot")
     with pytest.raises(cfk.CfkError, match="not a Tecplot"):
         cfk.read_flowfield(tmp_path / "other.plt", targets)
