@@ -190,6 +190,8 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.c_char_p), i, _DP, ctypes.c_char_p, ctypes.c_size_t]),
             "cfk_register_inner_face": (i, [i, i, vp, vp, i, ctypes.POINTER(cfk_inner_face)]),
             "cfk_inner_communication": (i, [vp, vp, ctypes.POINTER(cfk_inner_face), vp]),
+            "cfk_read_inner_interface": (i, [ctypes.c_char_p, i, i, i, ctypes.POINTER(cfk_inner_face), i,
+                                             ctypes.POINTER(i), ctypes.c_char_p, ctypes.c_size_t]),
             "cfk_local_time_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step_graph": (i, [vp, _DP, vp]),
@@ -277,6 +279,22 @@ def read_flowfield(path, targets, species=()):
     if rc != 0:
         raise CfkError(f"cfk_read_flowfield: {rc}: {err.value.decode()}")
     return t.value
+
+
+def read_inner_interface(path, dim, ngg, n_block, max_faces=64):
+    """cfk_read_inner_interface: the registered inner faces of every block,
+    as a list per block."""
+    faces = (cfk_inner_face * max_faces)()
+    counts = (ctypes.c_int * n_block)()
+    err = ctypes.create_string_buffer(256)
+    rc = lib().cfk_read_inner_interface(str(path).encode(), dim, ngg, n_block, faces, max_faces, counts, err, 256)
+    if rc != 0:
+        raise CfkError(f"cfk_read_inner_interface: {rc}: {err.value.decode()}")
+    out, n = [], 0
+    for b in range(n_block):
+        out.append([faces[n + q] for q in range(counts[b])])
+        n += counts[b]
+    return out
 
 
 def make_param(p: dict, faces) -> cfk_param:

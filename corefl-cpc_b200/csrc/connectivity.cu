@@ -3,7 +3,12 @@
 // mesh's inner-interface records as InnerFace::register_boundary does
 // (reference src/Mesh.cpp:39-172).  The steps have to give the reference's
 // numbers exactly, since the communication kernel walks them.
+#include <cstdio>
 #include <cstdlib>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
 
 #include "corefl_b200.h"
 
@@ -105,5 +110,48 @@ extern "C" int cfk_register_inner_face(int dim, int ngg, const int src[6], const
   r.target_direction = it.side;
   r.target_block = target_block - 1;
   *out = r;
+  return CFK_OK;
+}
+
+// The mesh's inner-interface file (reference src/Mesh.cpp:927-958,
+// Mesh::read_inner_interface): a title line; the number of inner faces of
+// each block; a second title line; then per block, per face, two lines of
+// seven integers — this block's range and the target's range followed by the
+// target block's 1-based number (the first line's seventh integer is not
+// used).  Faces are registered in file order.
+extern "C" int cfk_read_inner_interface(const char *path, int dim, int ngg, int n_block, cfk_inner_face *faces,
+                                        int max_faces, int *n_per_block, char *err, size_t err_len) {
+  auto fail = [&](const std::string &m, int code) {
+    if (err && err_len) std::snprintf(err, err_len, "%s", m.c_str());
+    return code;
+  };
+  if (!path || n_block < 1 || !n_per_block || (max_faces > 0 && !faces)) return fail("bad argument", CFK_ERR_ARG);
+  std::ifstream in(path);
+  if (!in) return fail(std::string("cannot open ") + path, CFK_ERR_IO);
+  std::string line;
+  std::getline(in, line);
+  std::vector<int> count(n_block);
+  for (int b = 0; b < n_block; ++b)
+    if (!(in >> count[b]) || count[b] < 0) return fail("bad face count of block " + std::to_string(b), CFK_ERR_IO);
+  std::getline(in, line);  // rest of the counts line
+  std::getline(in, line);  // second title line
+  int n = 0;
+  for (int b = 0; b < n_block; ++b) {
+    for (int l = 0; l < count[b]; ++l) {
+      int a[7], t[7];
+      for (int *rec : {a, t}) {
+        if (!std::getline(in, line)) return fail("file ends inside block " + std::to_string(b), CFK_ERR_IO);
+        std::istringstream ls(line);
+        for (int q = 0; q < 7; ++q)
+          if (!(ls >> rec[q])) return fail("short record in block " + std::to_string(b), CFK_ERR_IO);
+      }
+      if (n >= max_faces) return fail("more than max_faces inner faces", CFK_ERR_ARG);
+      if (cfk_register_inner_face(dim, ngg, a, t, t[6], &faces[n]) != CFK_OK)
+        return fail("block " + std::to_string(b) + " face " + std::to_string(l) + ": record cannot be decoded",
+                    CFK_ERR_IO);
+      ++n;
+    }
+    n_per_block[b] = count[b];
+  }
   return CFK_OK;
 }

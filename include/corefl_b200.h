@@ -280,6 +280,12 @@ int cfk_read_flowfield(const char *path, const cfk_plt_target *blocks, int n_blo
  * axis or, in 3-D, without a marked tangential axis. */
 int cfk_register_inner_face(int dim, int ngg, const int src[6], const int tar[6], int target_block,
                             cfk_inner_face *out);
+/* Read the mesh's inner-interface file (input/boundary_condition/inner%4d.txt,
+ * reference src/Mesh.cpp:927-958) and register every face in it: faces[]
+ * receives them block by block in file order (at most max_faces), and
+ * n_per_block[b] how many belong to block b.  Host only. */
+int cfk_read_inner_interface(const char *path, int dim, int ngg, int n_block, cfk_inner_face *faces, int max_faces,
+                             int *n_per_block, char *err, size_t err_len);
 /* Replaces inner_communication<M> of data_communication for one inner face
  * (reference src/DataCommunication.cu:6-102): this block's ghost nodes behind
  * the face take the target block's primitive variables; on the face itself

@@ -226,3 +226,53 @@ def test_periodic_split_stays_finite_and_consistent():
     assert np.all(np.isfinite(a)) and np.all(np.isfinite(b))
     assert np.array_equal(a[inner][..., g + A.mx - 1], b[inner][..., g])      # the cut
     assert np.array_equal(a[inner][..., g], b[inner][..., g + B.mx - 1])      # the periodic seam
+
+
+def _inner_file(links, n_block):
+    """The mesh's inner-interface file for `links` in the layout of the
+    reference's reader: title, per-block face counts, title, record pairs."""
+    lines = ["inner faces", " ".join(str(sum(1 for b, *_ in links if b == k)) for k in range(n_block)), "records"]
+    for k in range(n_block):
+        for b, src, tar, tb in links:
+            if b == k:
+                lines.append(" ".join(map(str, src + [0])))
+                lines.append(" ".join(map(str, tar + [tb])))
+    return "\n".join(lines) + "\n"
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_inner_interface_file_registers_like_the_records(tmp_path, periodic):
+    whole = cases.sine_wave(n=25, ny=11, nz=9, scheme=52, viscous=False)
+    if not periodic:
+        whole = _outflow_i(whole)
+    A, B, links = cases.split_i(whole, 12)
+    path = tmp_path / "inner   0.txt"
+    path.write_text(_inner_file(links, 2))
+    per_block = cfk.read_inner_interface(path, 3, whole.ngg, 2)
+    for k in range(2):
+        want = [cfk.register_inner_face(3, whole.ngg, s, t, tb) for b, s, t, tb in links if b == k]
+        assert [bytes(f) for f in per_block[k]] == [bytes(f) for f in want]
+    assert len(per_block[0]) == (2 if periodic else 1)
+    # the same file for the 2-D tube
+    A2, B2, links2 = cases.split_i(cases.sod(64, 9, scheme=52), 30)
+    (tmp_path / "inner2.txt").write_text(_inner_file(links2, 2))
+    got = cfk.read_inner_interface(tmp_path / "inner2.txt", 2, 3, 2)
+    assert bytes(got[1][0]) == bytes(cfk.register_inner_face(2, 3, links2[1][1], links2[1][2], links2[1][3]))
+
+
+def test_inner_interface_file_errors(tmp_path):
+    whole = cases.sine_wave(n=25, ny=11, nz=9, scheme=52, viscous=False)
+    _, _, links = cases.split_i(whole, 12)
+    text = _inner_file(links, 2)
+    with pytest.raises(cfk.CfkError, match="-5: cannot open"):
+        cfk.read_inner_interface(tmp_path / "missing.txt", 3, 3, 2)
+    (tmp_path / "cut.txt").write_text("\n".join(text.splitlines()[:-1]) + "\n")
+    with pytest.raises(cfk.CfkError, match="file ends inside block 1"):
+        cfk.read_inner_interface(tmp_path / "cut.txt", 3, 3, 2)
+    (tmp_path / "f.txt").write_text(text)
+    with pytest.raises(cfk.CfkError, match="max_faces"):
+        cfk.read_inner_interface(tmp_path / "f.txt", 3, 3, 2, max_faces=3)
+    bad = text.replace("-1 -11 1 9", "1 11 1 9", 1)   # first record loses its marked axis
+    (tmp_path / "bad.txt").write_text(bad)
+    with pytest.raises(cfk.CfkError, match="cannot be decoded"):
+        cfk.read_inner_interface(tmp_path / "bad.txt", 3, 3, 2)
