@@ -118,11 +118,20 @@ std::string struct_string(const Struct &st, const char *k) {
   return std::string();
 }
 
+int struct_int(const Struct &st, const char *k, int dflt) {
+  auto it = st.find(k);
+  if (it == st.end()) return dflt;
+  if (auto p = std::get_if<int>(&it->second)) return *p;
+  return dflt;
+}
+
 // The wall condition of the boundary_conditions list (reference
 // src/BoundCond.cpp:480-528, Wall::Wall): thermal_type isothermal (default,
 // also for an unknown name, as there), adiabatic or equilibrium_radiation
 // (kept as 2, which cfk_create rejects); temperature defaults to 300 K.
-// Returns false when more than one wall struct is listed.
+// Returns false when more than one wall struct is listed, or when the wall
+// asks for blowing/suction fluctuations or shock blowing (problem set-ups
+// outside this path).
 bool read_wall(const Setup &s, cfk_wall &w, std::string &err) {
   w.thermal_type = 0;
   w.catalytic_type = 0;
@@ -137,6 +146,10 @@ bool read_wall(const Setup &s, cfk_wall &w, std::string &err) {
       err = "more than one wall condition in boundary_conditions; cfk_param carries one";
       return false;
     }
+    if (struct_int(it->second, "fluctuation_type", 0) != 0 || struct_int(it->second, "if_blow_shock_wave", 0) != 0) {
+      err = "wall " + name + ": wall fluctuations and shock blowing are not supported";
+      return false;
+    }
     const std::string t = struct_string(it->second, "thermal_type");
     w.thermal_type = t == "adiabatic" ? 1 : t == "equilibrium_radiation" ? 2 : 0;
     w.temperature = struct_real(it->second, "temperature", 300.0);
@@ -144,12 +157,6 @@ bool read_wall(const Setup &s, cfk_wall &w, std::string &err) {
   return true;
 }
 
-int struct_int(const Struct &st, const char *k, int dflt) {
-  auto it = st.find(k);
-  if (it == st.end()) return dflt;
-  if (auto p = std::get_if<int>(&it->second)) return *p;
-  return dflt;
-}
 
 // The inflow condition of the boundary_conditions list, air (reference
 // src/BoundCond.cpp:9-260, Inflow::Inflow for a constant inflow): the state

@@ -167,3 +167,28 @@ def test_wall_description_checked_before_device_use():
         assert corefl_b200.lib().cfk_create(ctypes.byref(p), ctypes.byref(h)) == -1, bad
     ok = corefl_b200.make_param({**base, "wall_thermal_type": 1, "wall_yk": [0.5, 0.5]}, faces)
     assert ok.wall.thermal_type == 1 and ok.faces[0].label == 2 and list(ok.wall.yk[:3]) == [0.5, 0.5, 0.0]
+
+
+def test_setup_wall_struct(tmp_path):
+    """The wall struct of setup.txt: thermal type and temperature are read;
+    wall fluctuations (a problem set-up outside this path) are reported
+    instead of being dropped silently."""
+    import corefl_b200
+
+    def param_of(text):
+        f = tmp_path / "setup.txt"
+        f.write_text(text)
+        p = corefl_b200.cfk_param()
+        err = ctypes.create_string_buffer(256)
+        rc = corefl_b200.lib().cfk_param_from_setup(str(f).encode(), ctypes.byref(p), err, 256)
+        return rc, p, err.value.decode()
+
+    head = "int inviscid_scheme = 72\narray string boundary_conditions {\n  wall\n}\n"
+    rc, p, _ = param_of(head + "struct wall {\n string type = wall\n int label = 2\n string thermal_type = adiabatic\n}\n")
+    assert rc == 0 and p.wall.thermal_type == 1
+    rc, p, _ = param_of(head + "struct wall {\n string type = wall\n string thermal_type = isothermal\n"
+                        " real temperature = 322\n}\n")
+    assert rc == 0 and p.wall.thermal_type == 0 and p.wall.temperature == 322.0
+    rc, _, err = param_of(head + "struct wall {\n string type = wall\n real temperature = 322\n"
+                          " int fluctuation_type = 1\n real fluctuation_intensity = 0.04\n}\n")
+    assert rc == -5 and "fluctuations" in err
