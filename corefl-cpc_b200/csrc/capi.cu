@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "ctx.cuh"
 
 namespace cfk {
@@ -51,7 +53,12 @@ using namespace cfk;
 using namespace cfk_detail;
 
 namespace {
-// Records the events of one phase around the launches issued in its scope.
+const char *const kPhaseName[CFK_NPHASE] = {"cfk inviscid flux", "cfk viscous flux", "cfk update",
+                                            "cfk boundary conditions", "cfk properties", "cfk time step"};
+
+// One phase of a step: an NVTX range named after it (visible to Nsight
+// Systems; inert when no tool is attached) and, with profiling on, CUDA
+// events around the launches issued in its scope.
 struct PhaseScope {
   cfk_ctx *c;
   int phase;
@@ -60,9 +67,11 @@ struct PhaseScope {
   int n0;
   cudaEvent_t a = nullptr;
   PhaseScope(cfk_ctx *c_, int ph, cudaStream_t s, int *n_) : c(c_), phase(ph), st(s), n(n_), n0(*n_) {
+    nvtxRangePushA(kPhaseName[ph]);
     if (c->profiling) { a = c->take_event(); cudaEventRecord(a, st); }
   }
   ~PhaseScope() {
+    nvtxRangePop();
     if (!c->profiling) return;
     cudaEvent_t b = c->take_event();
     cudaEventRecord(b, st);
