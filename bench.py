@@ -46,6 +46,27 @@ N_NODES = 257
 FLOPS_PER_FACE_WENO7_CH = 2980.0
 
 
+WENO_PROFILE = os.path.join(ROOT, "profiles", "weno_air_flux_diff_161.md")
+WENO_PROFILE_NODES = 161 ** 3
+
+
+def weno_traffic_per_launch(nodes):
+    """DRAM bytes per launch of the WENO sweep kernel: the mean of the
+    'DRAM read + write per launch' row (MB, one value per sweep) of the ncu
+    summary captured on a 161^3 block, scaled to `nodes` interior nodes (the
+    kernel reads each input about once, so its traffic grows with the
+    nodes).  Returns (bytes or None, description)."""
+    try:
+        with open(WENO_PROFILE) as f:
+            row = next(line for line in f if line.startswith("| DRAM read + write per launch"))
+        mb = [float(c.strip().split()[0]) for c in row.strip().strip("|").split("|")[1:]]
+        per_launch = sum(mb) / len(mb) * 1e6 * nodes / WENO_PROFILE_NODES
+        return per_launch, (f"ncu dram__bytes_read+write on 161^3 ({sum(mb) / len(mb):.0f} MB per sweep, "
+                            f"profiles/weno_air_flux_diff_161.md) scaled by nodes")
+    except (OSError, StopIteration, ValueError, IndexError):
+        return None, "no ncu summary"
+
+
 def max_over_ranks(x: float, dist, device) -> float:
     """The largest of each rank's x (one all-reduce); x itself without a process group."""
     if not dist:
@@ -472,13 +493,10 @@ def main():
     if args.scheme == 72:
         achieved = FLOPS_PER_FACE_WENO7_CH * faces_per_launch / (avg_launch_ms * 1e-3) / 1e12
         peak = cfk.measure_fp64_peak()
-        traffic = None
-        tf = os.path.join(ROOT, "profiles", "weno_air_traffic.json")
-        if os.path.exists(tf):
-            with open(tf) as f:
-                traffic = json.load(f).get("bytes_per_launch_257")
+        traffic, traffic_source = weno_traffic_per_launch(case.mx * case.my * case.mz)
         roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": traffic, "kernel": "weno_air_flux_diff<dir,7> (x/y/z sweeps)",
+                    "traffic": traffic, "traffic_source": traffic_source,
+                    "kernel": "weno_air_flux_diff<dir,7> (x/y/z sweeps)",
                     "peak_source": "measured live: cfk_measure_fp64_peak FMA-chain kernel",
                     "avg_launch_ms": avg_launch_ms, "flops_per_launch": FLOPS_PER_FACE_WENO7_CH * faces_per_launch}
     else:

@@ -71,3 +71,14 @@ def test_reference_arm_under_torchrun_prints_once():
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     assert json.loads(lines[0])["n_gpus"] == 2
+
+
+def test_weno_traffic_comes_from_the_ncu_summary():
+    """The roofline's traffic is the ncu DRAM figure of the committed 161^3
+    summary, scaled by interior nodes to the benchmark block."""
+    import bench
+
+    t161, src = bench.weno_traffic_per_launch(161 ** 3)
+    assert 6.9e8 < t161 < 7.3e8 and "161^3" in src
+    t257, _ = bench.weno_traffic_per_launch(257 ** 3)
+    assert abs(t257 / t161 - (257 / 161) ** 3) < 1e-12
