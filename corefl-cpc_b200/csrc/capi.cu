@@ -573,6 +573,7 @@ int cfk_set_tile_variants(cfk_ctx *c, const int *var) {
 
 int cfk_update_cv_and_bv_rk(cfk_ctx *c, double dt, int rk, void *stream) {
   NEED_ZONE(c);
+  if (int r = need_mech_for_mixture(c)) return r;
   if (rk < 0 || rk > 2) return fail(c, CFK_ERR_ARG, "rk must be 0, 1 or 2");
   CFK_CHECK(c, launch_update_rk(c->z, c->p, thermo_of(c), dt, nullptr, rk, c->d_err, S(stream)), "update_cv_and_bv_rk");
   c->launches += 1;
@@ -581,6 +582,7 @@ int cfk_update_cv_and_bv_rk(cfk_ctx *c, double dt, int rk, void *stream) {
 
 int cfk_update_physical_properties(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
+  if (int r = need_mech_for_mixture(c)) return r;
   CFK_CHECK(c, launch_update_properties(c->z, c->p, thermo_of(c), S(stream)), "update_physical_properties");
   c->launches += 1;
   return CFK_OK;
@@ -588,6 +590,7 @@ int cfk_update_physical_properties(cfk_ctx *c, void *stream) {
 
 int cfk_compute_cv_from_bv(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
+  if (int r = need_mech_for_mixture(c)) return r;
   CFK_CHECK(c, launch_cv_from_bv(c->z, c->p, thermo_of(c), S(stream)), "compute_cv_from_bv");
   c->launches += 1;
   return CFK_OK;
@@ -595,6 +598,7 @@ int cfk_compute_cv_from_bv(cfk_ctx *c, void *stream) {
 
 int cfk_apply_boundary_conditions(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
+  if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
   CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, S(stream), &n),
             "boundary conditions");
@@ -650,6 +654,7 @@ int cfk_inner_communication(cfk_ctx *c, cfk_ctx *t, const cfk_inner_face *f, voi
   NEED_ZONE(c);
   if (!t || !f) return fail(c, CFK_ERR_ARG, "inner_communication: null target or face");
   if (!t->bound) return fail(c, CFK_ERR_STATE, "inner_communication: target has no zone bound");
+  if (int r = need_mech_for_mixture(c)) return r;
   if (t->hp.device != c->hp.device) return fail(c, CFK_ERR_ARG, "inner_communication: blocks on different devices");
   if (t->z.d.ngg != c->z.d.ngg || (t->z.d.mz == 1) != (c->z.d.mz == 1) || t->p.n_var != c->p.n_var ||
       t->p.n_scalar != c->p.n_scalar || t->p.n_spec != c->p.n_spec)
@@ -663,6 +668,7 @@ int cfk_inner_communication(cfk_ctx *c, cfk_ctx *t, const cfk_inner_face *f, voi
 
 int cfk_local_time_step(cfk_ctx *c, double *dt_out, void *stream) {
   NEED_ZONE(c);
+  if (int r = need_mech_for_mixture(c)) return r;
   CFK_CHECK(c, launch_local_dt(c->z, c->p, thermo_of(c), c->d_dt_bits, S(stream)), "local_time_step");
   c->launches += 2;
   if (dt_out) {
