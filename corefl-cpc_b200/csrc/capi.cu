@@ -330,7 +330,6 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
     const size_t P = (size_t)z.d.plane(z.d.ngg);
     if (c->own_sensor_n < P) {
       if (c->own_sensor) cudaFree(c->own_sensor);
-  if (c->own_fvis8) cudaFree(c->own_fvis8);
       c->own_sensor = nullptr;
       c->own_sensor_n = 0;
       CFK_CHECK(c, cudaMalloc(&c->own_sensor, P * sizeof(double)), "shock sensor allocation");
