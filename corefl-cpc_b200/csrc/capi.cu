@@ -599,7 +599,8 @@ int cfk_apply_boundary_conditions(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
   if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
-  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, S(stream), &n),
+  CFK_CHECK(c, launch_boundary_conditions(c->z, c->p, thermo_of(c), c->hp.faces, c->hp.n_face, c->hp.wall,
+                                          c->hp.inflow, c->hp.outflow, S(stream), &n),
             "boundary conditions");
   c->launches += n;
   return CFK_OK;
@@ -722,7 +723,9 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_BC, st, &n);
-      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, st, &n), "boundary conditions");
+      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
+                                              c->hp.outflow, st, &n),
+                "boundary conditions");
     }
     {
       PhaseScope ps(c, CFK_PH_PROPS, st, &n);
@@ -771,7 +774,9 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
             "wu_reaction_step");
   ++n;
-  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, st, &n), "boundary conditions");
+  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
+                                          c->hp.outflow, st, &n),
+            "boundary conditions");
   CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
   ++n;
   // wu_RK_subStep (:564-634): SSP-RK3 over dt/2 on dq - Cn, no property update
@@ -779,11 +784,13 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order > 0)
-    CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
+      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
     CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;
-    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow, c->hp.outflow, st, &n), "boundary conditions");
+    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
+                                          c->hp.outflow, st, &n),
+            "boundary conditions");
   }
   c->launches += n;
   if (dt_used) *dt_used = dt;
