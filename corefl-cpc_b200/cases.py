@@ -290,44 +290,70 @@ def with_back_pressure(case: Case, p_back: float) -> Case:
     return dataclasses.replace(case, param=param, name=case.name + "_pback")
 
 
-def split_i(case: Case, h: int, periodic_i: bool | None = None):
-    """Two blocks cut from `case` along i, sharing the node plane i = h:
-    A holds nodes 0..h, B nodes h..mx-1.  Every padded array is sliced from
-    the whole block's, so both blocks carry exactly its metrics and state.
-    Returns (A, B, links) where links lists the inner faces as the mesh's
-    inner-interface records: (block, src, tar, target_block), block 0-based,
-    ranges and target_block 1-based as the reference's inner%4d.txt holds them.
-    The cut is an inner face; if the i faces of `case` are periodic
-    (periodic_i None: read from case.faces), A's i-min and B's i-max faces
-    become an inner face too, else they keep the case's i-face labels."""
+def split(case: Case, h: int, axis: int = 0, periodic: bool | None = None):
+    """Two blocks cut from `case` across `axis` (0 i, 1 j, 2 k), sharing the
+    node plane at index h: A holds nodes 0..h, B nodes h..m-1 along that
+    axis.  Every padded array is sliced from the whole block's, so both
+    blocks carry exactly its metrics and state.  Returns (A, B, links) where
+    links lists the inner faces as the mesh's inner-interface records:
+    (block, src, tar, target_block), block 0-based, ranges and target_block
+    1-based as the reference's inner%4d.txt holds them (in 3-D the lower
+    tangential axis is the marked one).  The cut is an inner face; if the
+    case's faces across `axis` are periodic (periodic None: read from
+    case.faces), A's min face and B's max face become an inner face too,
+    else they keep the case's labels."""
     g = case.ngg
-    if periodic_i is None:
-        periodic_i = any(f == 0 and lab == 8 for f, _, lab in case.faces)
+    m = [case.mx, case.my, case.mz]
+    if axis == 2 and case.mz == 1:
+        raise ValueError("a 2-D block cannot be cut along k")
+    if periodic is None:
+        periodic = any(f == axis and lab == 8 for f, _, lab in case.faces)
     shape = lambda a: a.reshape(a.shape[:-1] + (case.mz + 2 * g, case.my + 2 * g, case.mx + 2 * g))
+    pos = -1 - axis  # position of the axis in the padded (k, j, i) shape
 
     def cut(a, lo, hi):
         if a is None:
             return None
-        b = shape(a)[..., lo:hi + 2 * g + 1]
+        b = shape(a)
+        sl = [slice(None)] * b.ndim
+        sl[pos] = slice(lo, hi + 2 * g + 1)
+        b = b[tuple(sl)]
         return np.ascontiguousarray(b.reshape(a.shape[:-1] + (b.shape[-3] * b.shape[-2] * b.shape[-1],)))
 
     def block(lo, hi, keep):
-        faces = [fc for fc in case.faces if fc[0] != 0 or (not periodic_i and (fc[0], fc[1]) == keep)]
-        return dataclasses.replace(case, name=f"{case.name}_i{lo}-{hi}", mx=hi - lo + 1, metric=cut(case.metric, lo, hi),
-                                   jac=cut(case.jac, lo, hi), bv=cut(case.bv, lo, hi), sv=cut(case.sv, lo, hi),
-                                   faces=faces, x=cut(case.x, lo, hi))
+        faces = [fc for fc in case.faces if fc[0] != axis or (not periodic and (fc[0], fc[1]) == keep)]
+        ext = dict(zip(("mx", "my", "mz"), m))
+        ext["mx my mz".split()[axis]] = hi - lo + 1
+        return dataclasses.replace(case, name=f"{case.name}_{'ijk'[axis]}{lo}-{hi}", **ext,
+                                   metric=cut(case.metric, lo, hi), jac=cut(case.jac, lo, hi), bv=cut(case.bv, lo, hi),
+                                   sv=cut(case.sv, lo, hi), faces=faces, x=cut(case.x, lo, hi))
 
-    A = block(0, h, (0, -1))
-    B = block(h, case.mx - 1, (0, 1))
-    my, mz = case.my, case.mz
-    if case.mz == 1:
-        rng = lambda i: [i, i, 1, my, 1, 1]
-    else:
-        rng = lambda i: [i, i, -1, -my, 1, mz]
-    links = [(0, rng(A.mx), rng(1), 2), (1, rng(1), rng(A.mx), 1)]
-    if periodic_i:
-        links += [(0, rng(1), rng(B.mx), 2), (1, rng(B.mx), rng(1), 1)]
+    A = block(0, h, (axis, -1))
+    B = block(h, m[axis] - 1, (axis, 1))
+    two_d = case.mz == 1
+
+    def rng(v):
+        r = [0] * 6
+        tang = [a for a in range(3 if not two_d else 2) if a != axis]
+        for a in range(3):
+            if a == axis:
+                r[2 * a] = r[2 * a + 1] = v
+            elif two_d or a != tang[0]:
+                r[2 * a], r[2 * a + 1] = 1, m[a]
+            else:
+                r[2 * a], r[2 * a + 1] = -1, -m[a]
+        return r
+
+    na, nb = h + 1, m[axis] - h
+    links = [(0, rng(na), rng(1), 2), (1, rng(1), rng(na), 1)]
+    if periodic:
+        links += [(0, rng(1), rng(nb), 2), (1, rng(nb), rng(1), 1)]
     return A, B, links
+
+
+def split_i(case: Case, h: int, periodic_i: bool | None = None):
+    """split() across i (kept for the existing callers)."""
+    return split(case, h, 0, periodic_i)
 
 
 def _gas_constant(case: Case) -> np.ndarray:

@@ -276,3 +276,44 @@ def test_inner_interface_file_errors(tmp_path):
     (tmp_path / "bad.txt").write_text(bad)
     with pytest.raises(cfk.CfkError, match="cannot be decoded"):
         cfk.read_inner_interface(tmp_path / "bad.txt", 3, 3, 2)
+
+
+def _outflow_axis(case, axis):
+    return dataclasses.replace(case, faces=[(f, d, 6 if f == axis else lab) for f, d, lab in case.faces])
+
+
+def _split_vs_whole_axis(whole, h, axis, steps):
+    A, B, links = cases.split(whole, h, axis, periodic=False)
+    oz = pyoracle.OracleZone(whole)
+    oz.initialize()
+    mb = OracleBlocks([A, B], links)
+    mb.initialize()
+    g = whole.ngg
+    shp = lambda c: (-1, c.mz + 2 * g, c.my + 2 * g, c.mx + 2 * g)
+    worst = 0.0
+    for _ in range(steps):
+        assert oz.step() == pytest.approx(mb.step(), rel=1e-13)
+        W = oz["cv"].reshape(shp(whole))
+        scale = np.abs(W).max(axis=(1, 2, 3))
+        scale[1:4] = scale[1:4].max()
+        for blk, lo in ((A, 0), (B, h)):
+            arr = (mb.z[0] if blk is A else mb.z[1])["cv"].reshape(shp(blk))
+            inner = arr[:, g:g + blk.mz, g:g + blk.my, g:g + blk.mx]
+            sl = [slice(None), slice(g, g + whole.mz), slice(g, g + whole.my), slice(g, g + whole.mx)]
+            sl[3 - axis] = slice(g + lo, g + lo + (blk.mx, blk.my, blk.mz)[axis])
+            worst = max(worst, float((np.abs(inner - W[tuple(sl)]) / scale[:, None, None, None]).max()))
+    return worst
+
+
+@pytest.mark.parametrize("axis,h", [(1, 5), (2, 4)])
+def test_block_cut_across_j_or_k_steps_like_whole_block(axis, h):
+    """The cut across j (tangential axes i marked, k) and across k (i marked,
+    j): registration and communication for the other normal axes, over
+    whole RK3 steps."""
+    whole = _outflow_axis(cases.perturbed(cases.sine_wave(n=13, ny=12, nz=10, scheme=52, viscous=False), seed=4,
+                                          amp=0.05), axis)
+    assert _split_vs_whole_axis(whole, h, axis, 3) <= 1e-14
+
+
+def test_2d_tube_cut_across_j_steps_like_whole_tube():
+    assert _split_vs_whole_axis(cases.sod(40, 12, scheme=52), 6, 1, 4) <= 1e-14
