@@ -1288,6 +1288,73 @@ void orc_inner_communication(orc_zone *z, orc_zone *tz, const orc_param *p, cons
       }
 }
 
+static int unphysical(const double *v, const double *ll, const double *ul) {
+  for (int l = 0; l < 5; ++l)
+    if (isnan(v[l]) || v[l] < ll[l] || v[l] > ul[l]) return 1;
+  return 0;
+}
+
+int orc_limit_flow(orc_zone *z, const orc_param *p, const double ll[5], const double ul[5]) {
+  const int g = z->ngg;
+  const long sz = psz(z, g);
+  const long nn = (long)z->mx * z->my * z->mz;
+  double *snap = (double *)malloc(sizeof(double) * 5 * nn);
+  if (!snap) return -1;
+#define SNAP(i, j, k) (snap + 5 * (((long)(k) * z->my + (j)) * z->mx + (i)))
+  for (int k = 0; k < z->mz; ++k)
+    for (int j = 0; j < z->my; ++j)
+      for (int i = 0; i < z->mx; ++i)
+        for (int l = 0; l < 5; ++l) SNAP(i, j, k)[l] = z->bv[pidx(z, g, i, j, k) + l * sz];
+  int repaired = 0;
+  for (int k = 0; k < z->mz; ++k)
+    for (int j = 0; j < z->my; ++j)
+      for (int i = 0; i < z->mx; ++i) {
+        const double *var = SNAP(i, j, k);
+        if (!unphysical(var, ll, ul)) continue;
+        double upd[5] = {0, 0, 0, 0, 0};
+        int kn = 0;
+        for (int ka = -1; ka < 2; ++ka) {
+          const int k1 = k + ka;
+          if (k1 < 0 || k1 >= z->mz) continue;
+          for (int ja = -1; ja < 2; ++ja) {
+            const int j1 = j + ja;
+            if (j1 < 0 || j1 >= z->my) continue;
+            for (int ia = -1; ia < 2; ++ia) {
+              const int i1 = i + ia;
+              if (i1 < 0 || i1 >= z->mx) continue;
+              const double *nb = SNAP(i1, j1, k1);
+              if (unphysical(nb, ll, ul)) continue;
+              for (int l = 0; l < 5; ++l) upd[l] += nb[l];
+              ++kn;
+            }
+          }
+        }
+        if (kn > 0) {
+          const double kn_inv = 1.0 / kn;
+          for (int l = 0; l < 5; ++l) upd[l] *= kn_inv;
+        } else {
+          for (int l = 0; l < 5; ++l) {
+            upd[l] = var[l] > ll[l] ? var[l] : ll[l];
+            upd[l] = upd[l] < ul[l] ? upd[l] : ul[l];
+          }
+        }
+        const long id = pidx(z, g, i, j, k);
+        for (int l = 0; l < 5; ++l) z->bv[id + l * sz] = upd[l];
+        if (p->mech) {
+          double R = 0;
+          for (int l = 0; l < p->n_spec; ++l) R += z->sv[id + l * sz] * p->mech->gas_const[l];
+          z->bv[id + 5 * sz] = upd[4] / (upd[0] * R);
+        } else {
+          z->bv[id + 5 * sz] = upd[4] * MW_AIR / (upd[0] * R_U);
+        }
+        cv_from_bv_point(z, p, id);
+        ++repaired;
+      }
+#undef SNAP
+  free(snap);
+  return repaired;
+}
+
 /* eliminate_k_gradient (src/FieldOperation.cu:47-72) */
 void orc_eliminate_k_gradient(orc_zone *z, const orc_param *p) {
   const int g = z->ngg;

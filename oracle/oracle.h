@@ -126,6 +126,17 @@ int orc_register_inner_face(int dim, int ngg, const int src[6], const int tar[6]
  * with the target block tz (may be z itself). */
 void orc_inner_communication(orc_zone *z, orc_zone *tz, const orc_param *p, const orc_inner_face *f);
 
+/* limit_flow (src/TimeAdvanceFunc.cuh:117-230; limits src/DParameter.cu:333-357):
+ * interior nodes whose density, velocity or pressure is NaN or outside
+ * [ll, ul] take the average of the good nodes of their 3x3x3 neighbourhood
+ * inside the block (or their own values clamped to [ll, ul] when none is
+ * good), T from the state equation, cv recomputed.  Good and bad are judged
+ * on the state before the call, so the result does not depend on the order
+ * nodes are visited (the reference's single kernel reads neighbours that
+ * other threads may be rewriting; the two agree wherever no two bad nodes
+ * are neighbours).  Returns the number of nodes repaired. */
+int orc_limit_flow(orc_zone *z, const orc_param *p, const double ll[5], const double ul[5]);
+
 /* zone memory management (host, zero-filled) */
 int orc_zone_alloc(orc_zone *z, int mx, int my, int mz, int ngg, int n_var, int n_spec, int n_scalar);
 void orc_zone_free(orc_zone *z);

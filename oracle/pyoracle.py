@@ -179,6 +179,8 @@ def lib() -> ctypes.CDLL:
         L.orc_register_inner_face.restype = ctypes.c_int
         L.orc_inner_communication.argtypes = [zp, zp, pp, ctypes.POINTER(orc_inner_face)]
         L.orc_inner_communication.restype = None
+        L.orc_limit_flow.argtypes = [zp, pp, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_limit_flow.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -261,6 +263,12 @@ class OracleZone:
     def inner_communication(self, target: "OracleZone", face: orc_inner_face):
         self.L.orc_inner_communication(ctypes.byref(self.z), ctypes.byref(target.z), ctypes.byref(self.p),
                                        ctypes.byref(face))
+
+    def limit_flow(self, ll, ul) -> int:
+        """orc_limit_flow with the limits ll, ul of (rho, u, v, w, p)."""
+        lo = np.ascontiguousarray(ll, dtype=np.float64)
+        hi = np.ascontiguousarray(ul, dtype=np.float64)
+        return self.L.orc_limit_flow(ctypes.byref(self.z), ctypes.byref(self.p), lo.ctypes.data, hi.ctypes.data)
 
     def call(self, name, *args):
         return getattr(self.L, name)(ctypes.byref(self.z), ctypes.byref(self.p), *args)
