@@ -16,6 +16,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda.h>  // driver types for the context-id lookup (entry points resolved at run time)
+
 #include "cfk_common.cuh"
 
 namespace cfk {
@@ -87,16 +89,54 @@ __global__ void __launch_bounds__(1024) local_dt_static_pass2(const double *part
 }
 
 namespace {
-// Device address of g_dt_partials per device, looked up once per device with
-// that device current.  In host code the symbol itself is only a host-side
-// stand-in; kernels must be given this address.
+// Device address of g_dt_partials per device, looked up with that device
+// current.  In host code the symbol itself is only a host-side stand-in;
+// kernels must be given this address.  The lookup is kept together with the id
+// of the context it was made in: cudaDeviceReset destroys the context and the
+// module's copy of the array with it, and the context the runtime creates on
+// the next call has a new id, so the address is looked up again there.
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-double *g_scratch_addr[kMaxDevices] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id;
+  double *addr;
+};
+ScratchSlot g_scratch[kMaxDevices] = {};
 
+using CtxGetCurrentFn = CUresult(CUDAAPI *)(CUcontext *);
+using CtxGetIdFn = CUresult(CUDAAPI *)(CUcontext, unsigned long long *);
+
+// Id of the context current on the calling thread (unique over the process's
+// lifetime); 0 if the driver cannot report it, in which case every call looks
+// the address up afresh.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Called with `dev` current (the runtime has made its primary context current).
 int scratch_for_device(int dev, double **out, char *err, size_t err_len) {
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  const unsigned long long id = current_context_id();
+  ScratchSlot &slot = g_scratch[dev];
+  if (!slot.addr || id == 0 || slot.ctx_id != id) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_dt_partials);
     if (e != cudaSuccess || !p) {
@@ -104,11 +144,20 @@ int scratch_for_device(int dev, double **out, char *err, size_t err_len) {
                                         cudaGetErrorString(e));
       return CFK_ERR_CUDA;
     }
-    g_scratch_addr[dev] = static_cast<double *>(p);
+    slot.addr = static_cast<double *>(p);
+    slot.ctx_id = id;
   }
-  *out = g_scratch_addr[dev];
+  *out = slot.addr;
   return CFK_OK;
 }
+
+// Restores the calling thread's current device when the entry point returns.
+struct DeviceRestore {
+  int dev = -1;
+  ~DeviceRestore() {
+    if (dev >= 0) cudaSetDevice(dev);
+  }
+};
 }  // namespace
 
 }  // namespace cfk
@@ -137,7 +186,11 @@ extern "C" int cfk_local_time_step_static(const cfk_param *param, const cfk_zone
   if (!zone->metric || !zone->bv || (param->viscous_order > 0 && !zone->mul))
     return report(CFK_ERR_ARG, "metric and bv (and mul for viscous runs) are required");
   if (param->device < 0 || param->device >= kMaxDevices) return report(CFK_ERR_ARG, "device ordinal out of range");
-  cudaError_t e = cudaSetDevice(param->device);
+  DeviceRestore restore;
+  cudaError_t e = cudaGetDevice(&restore.dev);
+  if (e != cudaSuccess) return report(CFK_ERR_CUDA, cudaGetErrorString(e));
+  if (restore.dev == param->device) restore.dev = -1;  // already current: nothing to restore
+  e = cudaSetDevice(param->device);
   if (e != cudaSuccess) return report(CFK_ERR_CUDA, cudaGetErrorString(e));
   double *scratch = nullptr;
   const int rc = scratch_for_device(param->device, &scratch, err, err_len);

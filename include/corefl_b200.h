@@ -364,9 +364,11 @@ long long cfk_kernel_launches(const cfk_ctx *ctx);
  * partial minimum per 256-node row segment, ceil(mx/256)*my*mz <= 262144, i.e.
  * 2 MiB) is a file-scope device array that every GPU loading the library holds
  * until exit.  The first call on a device looks up that array's device address
- * (do it before any stream capture).  Calls share the scratch: calls that
- * overlap on the GPU race.  Air model only; larger zones are rejected with
- * CFK_ERR_ARG and a message in err. */
+ * (do it before any stream capture); after a cudaDeviceReset the next call
+ * looks it up again.  The call makes param->device current while it launches
+ * and restores the caller's current device before it returns.  Calls share
+ * the scratch: calls that overlap on the GPU race.  Air model only; larger
+ * zones are rejected with CFK_ERR_ARG and a message in err. */
 int cfk_local_time_step_static(const cfk_param *param, const cfk_zone *zone, double *dt_min_device, void *stream,
                                char *err, size_t err_len);
 

@@ -3,12 +3,14 @@
 Some callers cannot allocate device memory (a host building a CUDA graph, a
 memory-pool policy that forbids allocation after start-up, a framework that
 owns all device memory).  This entry point gives them the CFL step without a
-context: its scratch is a file-scope device array.  The test calls it through
+context: its scratch is a file-scope device array.  The tests call it through
 the C ABI twice in a row — on two different zones, so that scratch left over
-from the first call cannot leak into the second — and checks both results
-against the context entry point, with the tolerance of the other time-step
-test (1e-14 relative).  The device buffers here belong to the caller (torch);
-the entry point itself allocates nothing.
+from the first call cannot leak into the second — and check both results
+against the context entry point and against the CPU oracle's local and global
+time step, with the tolerance of the other time-step tests (1e-14 relative).
+The device buffers here belong to the caller (torch); the entry point itself
+allocates nothing, which the free-memory check after its first call on the
+device shows.
 """
 import ctypes
 
@@ -17,6 +19,7 @@ import pytest
 
 import cases
 import corefl_b200 as cfk
+import pyoracle
 from gpuzone import GpuZone
 
 pytestmark = pytest.mark.gpu
@@ -54,6 +57,38 @@ def test_static_local_time_step_matches_context_entry_point_twice():
         dt = _static_dt(gz, dt_dev)
         assert dt == pytest.approx(dt_ref, rel=1e-14)
         assert np.allclose(gz.get("dt_local"), dt_local_ref, rtol=1e-14, atol=0)
+
+
+def test_static_local_time_step_matches_oracle_twice_and_allocates_nothing():
+    """Both calls against the oracle's orc_local_time_step/orc_global_time_step
+    from the same state; device free memory is unchanged by calls after the
+    first (which may load the library's module and look up the scratch
+    address), and the caller's current device is the same afterwards."""
+    import torch
+
+    dt_dev = torch.zeros(1, dtype=torch.float64, device="cuda:0")
+    zones = []
+    for case in (cases.perturbed(cases.sine_wave(n=29, scheme=72, viscous=True), seed=13),
+                 cases.perturbed(cases.sod(96, 7, scheme=52), seed=14)):
+        oz = pyoracle.OracleZone(case)
+        oz.initialize()
+        gz = GpuZone(case)
+        gz.load_from(oz, keys=("cv", "bv", "mul"))
+        oz.call("orc_local_time_step")
+        dt_o = oz.L.orc_global_time_step(ctypes.byref(oz.z))
+        zones.append((gz, oz, dt_o))
+    _static_dt(zones[0][0], dt_dev)  # first call on this device: module load and address lookup
+    torch.cuda.synchronize()
+    dev_before = torch.cuda.current_device()
+    free_before = torch.cuda.mem_get_info()[0]
+    for gz, oz, dt_o in zones:
+        gz.t["dt_local"].zero_()
+        dt = _static_dt(gz, dt_dev)
+        assert dt == pytest.approx(dt_o, rel=1e-14)
+        assert np.allclose(gz.get("dt_local"), oz["dt_local"], rtol=1e-14, atol=0)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    assert torch.cuda.current_device() == dev_before
 
 
 def test_static_local_time_step_rejects_oversized_zone():
