@@ -337,8 +337,11 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
           if (rY[l] < 0) rY[l] = 0;
           sum += rY[l];
         }
+        // every partial density clipped: no composition to renormalise, so
+        // the node goes to the plain integrator instead of carrying 0/0
+        if (!(sum > 0)) reason = SG_NEWTON_FAILED;
         for (int l = 0; l < ns; ++l) {
-          Yn[l] = rY[l] / sum;
+          Yn[l] = sum > 0 ? rY[l] / sum : Y0[l];
           rY[l] = Yn[l] * qv[0];
         }
       }
@@ -711,16 +714,20 @@ __global__ void __launch_bounds__(128, 1) sg_train_kernel(const __grid_constant_
 }
 
 // Sum of the per-CTA partial gradients; optional export; Adam update of the
-// FP32 master weights and their BF16 core-matrix copy.
+// FP32 master weights and their BF16 core-matrix copy.  Once a training
+// kernel has flagged a tensor-core wait timeout (value 4 in err) its partials
+// are incomplete, so the update is skipped: the weights stay as they were
+// until the host reads the flag and reports the error.
 __global__ void sg_adam_kernel(float *master, float *m, float *v, const float *partials, int n_part, uint8_t *w16,
                                float lr, float b1, float b2, float eps, float bc1, float bc2, float *grad_out,
-                               int update) {
+                               int update, const int *err) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= kSgNParam) return;
   float g = 0.f;
   for (int p = 0; p < n_part; ++p) g += partials[(long long)p * kSgNParam + e];
   if (grad_out) grad_out[e] = g;
   if (!update) return;
+  if (err && (*(volatile const int *)err & 4)) return;
   const float mm = b1 * m[e] + (1.f - b1) * g;
   const float vv = b2 * v[e] + (1.f - b2) * g * g;
   m[e] = mm;
@@ -828,9 +835,9 @@ cudaError_t launch_sg_train(const float *X, const float *G, long long n, long lo
 
 cudaError_t launch_sg_adam(float *master, float *m, float *v, const float *partials, int n_part, uint8_t *w16,
                            float lr, float b1, float b2, float eps, float bc1, float bc2, float *grad_out, int update,
-                           cudaStream_t st) {
+                           const int *err, cudaStream_t st) {
   sg_adam_kernel<<<(kSgNParam + 255) / 256, 256, 0, st>>>(master, m, v, partials, n_part, w16, lr, b1, b2, eps, bc1,
-                                                          bc2, grad_out, update);
+                                                          bc2, grad_out, update, err);
   return cudaGetLastError();
 }
 

@@ -30,7 +30,7 @@ cudaError_t launch_sg_train(const float *X, const float *G, long long n, long lo
                             cudaStream_t st);
 cudaError_t launch_sg_adam(float *master, float *m, float *v, const float *partials, int n_part, uint8_t *w16,
                            float lr, float b1, float b2, float eps, float bc1, float bc2, float *grad_out, int update,
-                           cudaStream_t st);
+                           const int *err, cudaStream_t st);
 cudaError_t launch_sg_publish(const float *master, uint8_t *w16, cudaStream_t st);
 cudaError_t launch_sg_init(float *master, float *m, float *v, unsigned long long seed, cudaStream_t st);
 cudaError_t launch_wu_reaction_list(const Zone &z, const Param &p, const Mech *mc, const Mech &mc_host, double dt,
@@ -267,7 +267,7 @@ int cfk_surrogate_train(cfk_ctx *c, const float *X, const float *G, long long n,
       s->adam_t += 1;
       const float bc1 = 1.f - std::pow(b1, (float)s->adam_t), bc2 = 1.f - std::pow(b2, (float)s->adam_t);
       CFK_CHECK(c, launch_sg_adam(s->master, s->m, s->v, s->partials, n_ctas, s->w16, (float)lr, b1, b2, eps, bc1,
-                                  bc2, nullptr, 1, 0),
+                                  bc2, nullptr, 1, c->d_err, 0),
                 "surrogate adam");
       c->launches += 2;
     }
@@ -294,7 +294,7 @@ int cfk_surrogate_gradients(cfk_ctx *c, const float *X, const float *G, long lon
                                c->d_err, &n_ctas, 0),
             "surrogate gradients");
   CFK_CHECK(c, launch_sg_adam(s->master, s->m, s->v, s->partials, n_ctas, s->w16, 0.f, 0.9f, 0.999f, 1e-8f, 1.f, 1.f,
-                              grad_out, 0, 0),
+                              grad_out, 0, nullptr, 0),
             "gradient reduction");
   c->launches += 2;
   CFK_CHECK(c, cudaDeviceSynchronize(), "surrogate gradients");
