@@ -1,6 +1,6 @@
 """Builds the bundled mechanism tables (*.npz in this folder) from the
-Chemkin files that ship with the reference's examples (run where the
-reference is available at REFERENCE_ROOT):
+Chemkin files that ship with the reference's examples.
+Usage: python make_mechanisms.py <reference root>
 
 li2004.npz        example/constantVolumeReactor/input/chemistry/2004-Li-IntJ.Chem.Kinet.inp
                   (+ therm.dat, tran.dat): 9 species, 19 reactions after the
@@ -15,14 +15,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 import mechanism  # noqa: E402
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
-
 SOURCES = {
     "li2004": ("constantVolumeReactor", "2004-Li-IntJ.Chem.Kinet.inp"),
     "premix_h2_ar": ("reactiveShockTube", "H2_mech-PREMIX.inp"),
 }
 
 if __name__ == "__main__":
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: python make_mechanisms.py <reference root>")
+    REF = sys.argv[1]
     for name, (ex, mech) in SOURCES.items():
         d = os.path.join(REF, "example", ex, "input", "chemistry")
         m = mechanism.parse(os.path.join(d, mech), os.path.join(d, "therm.dat"), os.path.join(d, "tran.dat"))

@@ -1,5 +1,5 @@
 """Regenerates the golden fixtures in this folder from the reference's own
-example data (run in a checkout that has the reference at REFERENCE_ROOT).
+example data.  Usage: python make_golden.py <reference root>
 
 sod_exact.npz  — exact Riemann solution of the Sod problem at t = 0.2
                  (reference example/sodShockTube/exact.dat: x, u, rho, p).
@@ -14,7 +14,7 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = None  # the reference checkout, from the command line
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -40,7 +40,8 @@ def reactor():
 
 
 if __name__ == "__main__":
-    if not os.path.isdir(REF):
-        sys.exit(f"reference not found at {REF}")
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: python make_golden.py <reference root>")
+    REF = sys.argv[1]
     sod_exact()
     reactor()
