@@ -86,3 +86,37 @@ def rel_err(a: np.ndarray, b: np.ndarray, momentum=(1, 2, 3)) -> float:
 def interior_planes(case, arr: np.ndarray) -> np.ndarray:
     """Interior nodes of every plane of a padded (n, P) array, as (n, N)."""
     return np.stack([case.interior(arr[l]).reshape(-1) for l in range(arr.shape[0])])
+
+
+def pointwise_rel_err(a: np.ndarray, b: np.ndarray, n_spec: int = 0) -> float:
+    """Pointwise relative difference of conserved-variable stacks (n, N),
+    maximised over nodes and variables: density and total energy |a - b| / |b|
+    at each node; each momentum component |a_l - b_l| / max(|rho V|, rho c) at
+    each node, with the node's own momentum magnitude, or, where the flow is
+    slower than sound, the acoustic momentum rho c (ideal gas, gamma = 1.4,
+    from the node's density, energy and momentum) — a component that is zero
+    up to round-off, like v in a 1-D problem, has no relative error of its own;
+    the partial densities |a_l - b_l| / rho (mass-fraction units).  For
+    mixtures (n_spec > 0), whose energy includes formation enthalpies, the
+    momentum floor is 1e-8 of the largest momentum magnitude instead of rho c."""
+    a = np.atleast_2d(a)
+    b = np.atleast_2d(b)
+    worst = 0.0
+    for l in (0, 4):
+        if l < b.shape[0]:
+            worst = max(worst, float((np.abs(a[l] - b[l]) / np.abs(b[l])).max()))
+    if b.shape[0] >= 5:
+        mag2 = b[1] ** 2 + b[2] ** 2 + b[3] ** 2
+        mag = np.sqrt(mag2)
+        if n_spec == 0:
+            p = 0.4 * (b[4] - 0.5 * mag2 / b[0])
+            floor = np.sqrt(np.maximum(1.4 * p * b[0], 0.0))
+        else:
+            floor = 1e-8 * max(float(mag.max()), 1e-300)
+        den = np.maximum(np.maximum(mag, floor), 1e-300)
+        for l in (1, 2, 3):
+            worst = max(worst, float((np.abs(a[l] - b[l]) / den).max()))
+    for l in range(5, 5 + n_spec):
+        if l < b.shape[0]:
+            worst = max(worst, float((np.abs(a[l] - b[l]) / np.abs(b[0])).max()))
+    return worst

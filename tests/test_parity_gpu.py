@@ -2,8 +2,9 @@
 
 Bar: per-variable relative difference max|gpu - oracle| / max|oracle| of the
 conserved variables <= 1e-12 after every RK3 step (the three momentum planes
-share the largest momentum magnitude as their scale); the CFL time step
-agrees to 1e-13.  Inputs are seeded; sizes are small enough for the oracle to
+share the largest momentum magnitude as their scale), and the pointwise
+relative difference (per node; gpuzone.pointwise_rel_err) <= 1e-12 as well;
+the CFL time step agrees to 1e-13.  Inputs are seeded; sizes are small enough for the oracle to
 finish in seconds.
 """
 import numpy as np
@@ -11,7 +12,7 @@ import pytest
 
 import cases
 import pyoracle
-from gpuzone import GpuZone, interior_planes, rel_err
+from gpuzone import GpuZone, interior_planes, pointwise_rel_err, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -35,9 +36,12 @@ def _lockstep(case, n_steps, graph=False, tol=TOL, drift_tol=1e-10, tiles=None):
         dt_o = oz.step()
         dt_g = gz.ctx.rk3_step(graph=graph)
         assert dt_g == pytest.approx(dt_o, rel=1e-13), f"dt differs at step {s}"
-        e = rel_err(interior_planes(case, gz.get("cv")), interior_planes(case, oz["cv"]))
+        g, o = interior_planes(case, gz.get("cv")), interior_planes(case, oz["cv"])
+        e = rel_err(g, o)
         worst = max(worst, e)
         assert e <= tol, f"step {s}: conserved-variable relative difference {e:.3e} > {tol:g}"
+        ep = pointwise_rel_err(g, o)
+        assert ep <= tol, f"step {s}: pointwise relative difference {ep:.3e} > {tol:g}"
     # the padded arrays (ghosts filled by the BCs) agree as well
     assert rel_err(gz.get("cv"), oz["cv"]) <= tol
     assert rel_err(gz.get("bv"), oz["bv"]) <= tol
