@@ -6,11 +6,12 @@ Jacobian and the nine metric terms in the reference's VectorField3D layout
 (rho, u, v, w, p, T) and the settings of the run.
 
 Grid metrics follow Block::compute_jac_metric (reference
-src/Mesh.cpp:244-300): second-order central differences of the coordinates,
-J = det(d(x,y,z)/d(xi,eta,zeta)) and grad(xi) etc. from the cofactors.  Ghost
-coordinates are point reflections through the boundary node (reference
-src/Mesh.cpp:1020-1076), with z(k) = k for 2-D blocks; one extra reflected
-layer lets the central differences reach the outermost ghost node.
+src/Mesh.cpp:244-533): second-order central differences of the coordinates,
+J = det(d(x,y,z)/d(xi,eta,zeta)) and grad(xi) etc. from the cofactors, on the
+reference's ghost grid (src/Mesh.cpp:1014-1080): face ghosts are point
+reflections through the boundary node, with z(k) = z(0) + k for 2-D blocks,
+and edge and corner ghosts stay 0, so the metrics of the ghost nodes next to
+them are the reference's own.
 """
 from __future__ import annotations
 
@@ -60,37 +61,69 @@ class Case:
         return a.reshape(self.shape())[g:g + self.mz, g:g + self.my, g:g + self.mx]
 
 
-def _reflect_extend(c: np.ndarray, ext: int, axis: int, two_d_k: bool = False) -> np.ndarray:
-    """Extend a coordinate array by `ext` ghost layers on both sides of `axis`
-    by point reflection through the boundary node."""
-    n = c.shape[axis]
-    if two_d_k:
-        return c
-    lo = [2 * np.take(c, [0], axis=axis) - np.take(c, [q], axis=axis) for q in range(ext, 0, -1)]
-    hi = [2 * np.take(c, [n - 1], axis=axis) - np.take(c, [n - 1 - q], axis=axis) for q in range(1, ext + 1)]
-    return np.concatenate(lo + [c] + hi, axis=axis)
-
-
-def metrics(x: np.ndarray, y: np.ndarray, z: np.ndarray, ngg: int):
-    """Jacobian and metric on the padded grid from interior node coordinates
-    indexed [k, j, i].  Returns (jac (P,), metric (9, P), xg (P,))."""
-    mz, my, mx = x.shape
+def ghost_grid(x: np.ndarray, y: np.ndarray, z: np.ndarray, ngg: int):
+    """Coordinate arrays [k, j, i] with ngg + 1 ghost layers, filled as the
+    reference's Mesh::init_ghost_grid does (reference src/Mesh.cpp:1014-1162):
+    face ghosts (outside the block across one face) are point reflections
+    through the boundary node, x(-q) = 2 x(0) - x(q); for 2-D blocks the
+    k-ghosts copy the node with z(k) = z(0) + k; then edges and corners by the
+    parallelogram rule in three passes — the (i, j) edges of the k-planes of
+    the block, the (i, k) edges of its j-planes, and the (j, k) edges and the
+    corners for every i — e.g. x(-i, -j, k) = x(-i, 0, k) + x(0, -j, k) - x(0, 0, k)."""
     e = ngg + 1
-    coords = []
-    for c in (x, y, z):
-        c = _reflect_extend(c, e, 2)
-        c = _reflect_extend(c, e, 1)
-        if mz > 1:
-            c = _reflect_extend(c, e, 0)
-        coords.append(c)
-    X, Y, Z = coords
-    if mz == 1:
-        # 2-D block: z(k) = z(0) + k (reference src/Mesh.cpp:1066-1077)
-        ks = np.arange(-e, e + 1, dtype=np.float64)
-        X = np.repeat(X, 2 * e + 1, axis=0)
-        Y = np.repeat(Y, 2 * e + 1, axis=0)
-        Z = np.repeat(Z, 2 * e + 1, axis=0) + ks[:, None, None]
+    mz, my, mx = x.shape
+    two_d = mz == 1
+    out = []
+    for n, c in enumerate((x, y, z)):
+        a = np.zeros((mz + 2 * e, my + 2 * e, mx + 2 * e))
+        I, J, K = slice(e, e + mx), slice(e, e + my), slice(e, e + mz)
+        a[K, J, I] = c
+        for q in range(1, e + 1):
+            a[K, J, e - q] = 2 * c[:, :, 0] - c[:, :, q]
+            a[K, J, e + mx - 1 + q] = 2 * c[:, :, mx - 1] - c[:, :, mx - 1 - q]
+            a[K, e - q, I] = 2 * c[:, 0, :] - c[:, q, :]
+            a[K, e + my - 1 + q, I] = 2 * c[:, my - 1, :] - c[:, my - 1 - q, :]
+            if two_d:
+                a[e - q, J, I] = c[0] + (-q) if n == 2 else c[0]
+                a[e + q, J, I] = c[0] + q if n == 2 else c[0]
+            else:
+                a[e - q, J, I] = 2 * c[0] - c[q]
+                a[e + mz - 1 + q, J, I] = 2 * c[mz - 1] - c[mz - 1 - q]
+        lo = lambda m, q: e - q  # noqa: E731  index of node -q
+        hi = lambda m, q: e + m - 1 + q  # noqa: E731  index of node m - 1 + q
+        i0, i1, j0, j1, k0, k1 = e, e + mx - 1, e, e + my - 1, e, e + mz - 1
+        # pass 1: (i, j) edges for k in [0, mz)
+        for qi in range(1, e + 1):
+            for qj in range(1, e + 1):
+                for (ii, iref), (jj, jref) in (((lo(mx, qi), i0), (lo(my, qj), j0)),
+                                               ((hi(mx, qi), i1), (hi(my, qj), j1)),
+                                               ((lo(mx, qi), i0), (hi(my, qj), j1)),
+                                               ((hi(mx, qi), i1), (lo(my, qj), j0))):
+                    a[K, jj, ii] = a[K, jref, ii] + a[K, jj, iref] - a[K, jref, iref]
+        # pass 2: (i, k) edges for j in [0, my)
+        for qi in range(1, e + 1):
+            for qk in range(1, e + 1):
+                for (ii, iref), (kk, kref) in (((lo(mx, qi), i0), (lo(mz, qk), k0)),
+                                               ((hi(mx, qi), i1), (hi(mz, qk), k1)),
+                                               ((lo(mx, qi), i0), (hi(mz, qk), k1)),
+                                               ((hi(mx, qi), i1), (lo(mz, qk), k0))):
+                    a[kk, J, ii] = a[kref, J, ii] + a[kk, J, iref] - a[kref, J, iref]
+        # pass 3: (j, k) edges and corners for every i
+        for qj in range(1, e + 1):
+            for qk in range(1, e + 1):
+                for (jj, jref), (kk, kref) in (((lo(my, qj), j0), (lo(mz, qk), k0)),
+                                               ((hi(my, qj), j1), (hi(mz, qk), k1)),
+                                               ((lo(my, qj), j0), (hi(mz, qk), k1)),
+                                               ((hi(my, qj), j1), (lo(mz, qk), k0))):
+                    a[kk, jj, :] = a[kk, jref, :] + a[kref, jj, :] - a[kref, jref, :]
+        out.append(a)
+    return out
 
+
+def _jac_metric_formula(X, Y, Z):
+    """J and the nine metric terms at every node of the (n-2)-shaped inner
+    part of coordinate arrays [k, j, i], in the reference's arithmetic order
+    (reference src/Mesh.cpp:250-298)."""
     def d(a, axis):
         sl_p = [slice(1, -1)] * 3
         sl_m = [slice(1, -1)] * 3
@@ -102,22 +135,84 @@ def metrics(x: np.ndarray, y: np.ndarray, z: np.ndarray, ngg: int):
     dxd1, dyd1, dzd1 = d(X, 2), d(Y, 2), d(Z, 2)
     dxd2, dyd2, dzd2 = d(X, 1), d(Y, 1), d(Z, 1)
     dxd3, dyd3, dzd3 = d(X, 0), d(Y, 0), d(Z, 0)
-    jac = (dxd1 * dyd2 * dzd3 + dxd2 * dyd3 * dzd1 + dxd3 * dyd1 * dzd2 - dxd1 * dyd3 * dzd2 -
-           dxd2 * dyd1 * dzd3 - dxd3 * dyd2 * dzd1)
-    if np.any(jac <= 0):
+    with np.errstate(divide="ignore", invalid="ignore"):
+        jac = (dxd1 * dyd2 * dzd3 + dxd2 * dyd3 * dzd1 + dxd3 * dyd1 * dzd2 - dxd1 * dyd3 * dzd2 -
+               dxd2 * dyd1 * dzd3 - dxd3 * dyd2 * dzd1)
+        m = np.empty((9,) + jac.shape)
+        m[0] = (dyd2 * dzd3 - dyd3 * dzd2) / jac
+        m[1] = (dxd3 * dzd2 - dxd2 * dzd3) / jac
+        m[2] = (dxd2 * dyd3 - dxd3 * dyd2) / jac
+        m[3] = (dyd3 * dzd1 - dyd1 * dzd3) / jac
+        m[4] = (dxd1 * dzd3 - dxd3 * dzd1) / jac
+        m[5] = (dxd3 * dyd1 - dxd1 * dyd3) / jac
+        m[6] = (dyd1 * dzd2 - dyd2 * dzd1) / jac
+        m[7] = (dxd2 * dzd1 - dxd1 * dzd2) / jac
+        m[8] = (dxd1 * dyd2 - dxd2 * dyd1) / jac
+    return jac, m
+
+
+def metrics(x: np.ndarray, y: np.ndarray, z: np.ndarray, ngg: int):
+    """Jacobian and metric on the padded grid from interior node coordinates
+    indexed [k, j, i], as the reference's Block::compute_jac_metric leaves
+    them (reference src/Mesh.cpp:244-533) on the ghost grid of ghost_grid():
+    the central-difference formula at every padded node, then, in the
+    reference's sweep order (the k-ghost planes of the face interior outwards
+    from k = 0 and from k = mz - 1, the j-ghost planes with edges, the i-ghost
+    planes with edges and corners), a node whose Jacobian is not positive
+    takes the metric and Jacobian of its neighbour one plane inwards.  A
+    non-positive Jacobian inside the block is an error (the reference stops).
+    Returns (jac (P,), metric (9, P), xg (P,) the padded x coordinates)."""
+    mz, my, mx = x.shape
+    two_d = mz == 1
+    X, Y, Z = ghost_grid(x, y, z, ngg)
+    jac_f, met_f = _jac_metric_formula(X, Y, Z)  # shape (mz + 2 ngg, my + 2 ngg, mx + 2 ngg)
+    g = ngg
+    jac = np.zeros_like(jac_f)
+    met = np.zeros_like(met_f)
+
+    def put(sel_k, sel_j, sel_i):
+        jac[sel_k, sel_j, sel_i] = jac_f[sel_k, sel_j, sel_i]
+        met[:, sel_k, sel_j, sel_i] = met_f[:, sel_k, sel_j, sel_i]
+
+    def fix(axis, p, q, sel_a, sel_b):
+        """Plane p along `axis` over the ranges sel_a, sel_b of the other two
+        axes (in k, j, i order); non-positive Jacobians take plane q's values."""
+        idx = [None, None, None]
+        others = [a for a in (0, 1, 2) if a != axis]
+        idx[axis] = p
+        idx[others[0]], idx[others[1]] = sel_a, sel_b
+        src = list(idx)
+        src[axis] = q
+        t = tuple(idx)
+        put(*t)
+        bad = ~(jac[t] > 0)
+        if bad.any():
+            jac[t] = np.where(bad, jac[tuple(src)], jac[t])
+            met[(slice(None),) + t] = np.where(bad[None], met[(slice(None),) + tuple(src)], met[(slice(None),) + t])
+
+    ii = slice(g + 1, g + mx - 1)
+    jj = slice(g + 1, g + my - 1)
+    # block 0: i in [1, mx-1), j in [1, my-1), k in [1, mz-1) (k = 0 for 2-D)
+    kk = slice(g, g + 1) if two_d else slice(g + 1, g + mz - 1)
+    put(kk, jj, ii)
+    if np.any(~(jac[kk, jj, ii] > 0)):
         raise ValueError("non-positive Jacobian in the generated grid")
-    m = np.empty((9,) + jac.shape)
-    m[0] = (dyd2 * dzd3 - dyd3 * dzd2) / jac
-    m[1] = (dxd3 * dzd2 - dxd2 * dzd3) / jac
-    m[2] = (dxd2 * dyd3 - dxd3 * dyd2) / jac
-    m[3] = (dyd3 * dzd1 - dyd1 * dzd3) / jac
-    m[4] = (dxd1 * dzd3 - dxd3 * dzd1) / jac
-    m[5] = (dxd3 * dyd1 - dxd1 * dyd3) / jac
-    m[6] = (dyd1 * dzd2 - dyd2 * dzd1) / jac
-    m[7] = (dxd2 * dzd1 - dxd1 * dzd2) / jac
-    m[8] = (dxd1 * dyd2 - dxd2 * dyd1) / jac
+    all_k = slice(0, mz + 2 * g)
+    all_j = slice(0, my + 2 * g)
+    for k in range(0, -g - 1, -1):  # block 1: k = 0 .. -ngg
+        fix(0, g + k, g + k + 1, jj, ii)
+    for k in range(mz - 1, mz + g):  # block 2: k = mz-1 .. mz+ngg-1
+        fix(0, g + k, g + k - 1, jj, ii)
+    for j in range(0, -g - 1, -1):  # block 3: j = 0 .. -ngg, all k
+        fix(1, g + j, g + j + 1, all_k, ii)
+    for j in range(my - 1, my + g):  # block 4
+        fix(1, g + j, g + j - 1, all_k, ii)
+    for i in range(0, -g - 1, -1):  # block 5: i = 0 .. -ngg, all j, k
+        fix(2, g + i, g + i + 1, all_k, all_j)
+    for i in range(mx - 1, mx + g):  # block 6
+        fix(2, g + i, g + i - 1, all_k, all_j)
     xg = X[1:-1, 1:-1, 1:-1]
-    return jac.reshape(-1).copy(), m.reshape(9, -1).copy(), xg.reshape(-1).copy()
+    return jac.reshape(-1).copy(), met.reshape(9, -1).copy(), xg.reshape(-1).copy()
 
 
 def _air_param(**kw) -> dict:

@@ -88,7 +88,7 @@ def interior_planes(case, arr: np.ndarray) -> np.ndarray:
     return np.stack([case.interior(arr[l]).reshape(-1) for l in range(arr.shape[0])])
 
 
-def pointwise_rel_err(a: np.ndarray, b: np.ndarray, n_spec: int = 0) -> float:
+def pointwise_rel_err(a: np.ndarray, b: np.ndarray, n_spec: int = 0, p: np.ndarray | None = None) -> float:
     """Pointwise relative difference of conserved-variable stacks (n, N),
     maximised over nodes and variables: density and total energy |a - b| / |b|
     at each node; each momentum component |a_l - b_l| / max(|rho V|, rho c) at
@@ -98,7 +98,9 @@ def pointwise_rel_err(a: np.ndarray, b: np.ndarray, n_spec: int = 0) -> float:
     up to round-off, like v in a 1-D problem, has no relative error of its own;
     the partial densities |a_l - b_l| / rho (mass-fraction units).  For
     mixtures (n_spec > 0), whose energy includes formation enthalpies, the
-    momentum floor is 1e-8 of the largest momentum magnitude instead of rho c."""
+    momentum floor is 1e-8 of the largest momentum magnitude instead of rho c,
+    unless the node pressures p of the reference state are given: then the
+    floor is sqrt(p rho), a lower bound of rho c for any gas (gamma >= 1)."""
     a = np.atleast_2d(a)
     b = np.atleast_2d(b)
     worst = 0.0
@@ -108,9 +110,11 @@ def pointwise_rel_err(a: np.ndarray, b: np.ndarray, n_spec: int = 0) -> float:
     if b.shape[0] >= 5:
         mag2 = b[1] ** 2 + b[2] ** 2 + b[3] ** 2
         mag = np.sqrt(mag2)
-        if n_spec == 0:
-            p = 0.4 * (b[4] - 0.5 * mag2 / b[0])
-            floor = np.sqrt(np.maximum(1.4 * p * b[0], 0.0))
+        if p is not None:
+            floor = np.sqrt(np.maximum(np.asarray(p) * b[0], 0.0))
+        elif n_spec == 0:
+            p_air = 0.4 * (b[4] - 0.5 * mag2 / b[0])
+            floor = np.sqrt(np.maximum(1.4 * p_air * b[0], 0.0))
         else:
             floor = 1e-8 * max(float(mag.max()), 1e-300)
         den = np.maximum(np.maximum(mag, floor), 1e-300)
