@@ -41,6 +41,7 @@ class Case:
     faces: list  # [(face, direction, label)]
     x: np.ndarray | None = None  # (P,) node x, for checks against exact solutions
     mech: object = None  # mechanism.Mechanism for the mixture model
+    xyz: tuple | None = None  # interior node coordinates (x, y, z), each [k, j, i]
 
     @property
     def P(self) -> int:
@@ -274,7 +275,7 @@ def sod(nx: int = 400, ny: int = 7, scheme: int = 52, cfl: float = 0.5, reconstr
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref,
                        viscous_order=viscous_order)
     faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
-    return Case("sod", nx, ny, 1, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg)
+    return Case("sod", nx, ny, 1, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg, xyz=(x, y, z))
 
 
 def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float = 0.05, reynolds: float = 1000.0,
@@ -316,7 +317,8 @@ def sine_wave(n: int = 257, scheme: int = 72, viscous: bool = True, amp: float =
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref,
                        fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
     faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]
-    return Case("sine_wave", n, ny, nz, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg)
+    return Case("sine_wave", n, ny, nz, ngg, metric, jac, bv, np.zeros((0, P)), param, faces, x=xg,
+                xyz=(x, y, z))
 
 
 def perturbed(case: Case, seed: int = 0, amp: float = 1e-3) -> Case:
@@ -582,7 +584,7 @@ def mix_tube(mech, nx: int = 200, ny: int = 7, scheme: int = 52, reacting: bool 
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
                        viscous_order=viscous_order)
     faces = [(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)]
-    return Case("mix_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m)
+    return Case("mix_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m, xyz=(x, y, z))
 
 
 def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int | None = None,
@@ -627,4 +629,107 @@ def mix_wave(mech, n: int = 17, scheme: int = 72, viscous: bool = True, ny: int 
                        weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
                        fixed_dt=1 if dt is not None else 0, dt=dt or 0.0)
     faces = [(0, -1, 8), (0, 1, 8), (1, -1, 8), (1, 1, 8), (2, -1, 8), (2, 1, 8)]
-    return Case("mix_wave", n, ny, nz, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m)
+    return Case("mix_wave", n, ny, nz, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m,
+                xyz=(x, Y3 * length, Z3 * length))
+
+
+def mixture_enthalpy(mech, T: float, Y: np.ndarray) -> float:
+    """Specific enthalpy (J/kg) of a mixture from the NASA-7 polynomials,
+    h_k = R_u/W_k T (a0 + a1 T/2 + a2 T^2/3 + a3 T^3/4 + a4 T^4/5 + a5/T)."""
+    h = 0.0
+    for k in range(mech.n_spec):
+        a = mech.low[k] if T < mech.t_mid[k] else mech.high[k]
+        hk = T * (a[0] + T * (a[1] / 2 + T * (a[2] / 3 + T * (a[3] / 4 + T * a[4] / 5)))) + a[5]
+        h += Y[k] * R_U / mech.mw[k] * hk
+    return h
+
+
+def mixture_cp(mech, T: float, Y: np.ndarray) -> float:
+    cp = 0.0
+    for k in range(mech.n_spec):
+        a = mech.low[k] if T < mech.t_mid[k] else mech.high[k]
+        cp += Y[k] * R_U / mech.mw[k] * (a[0] + T * (a[1] + T * (a[2] + T * (a[3] + T * a[4]))))
+    return cp
+
+
+def reflected_shock_states(mech, Y: np.ndarray, T1: float, p1: float, mach: float):
+    """Frozen-chemistry Rankine-Hugoniot states of a shock of Mach `mach`
+    (against the frozen sound speed) running into gas at rest (T1, p1, Y) and
+    of its reflection from a closed end: returns dicts for state 2 (behind the
+    incident shock, lab velocity u towards the end wall) and state 5 (behind
+    the reflected shock, at rest), each with rho, u, p, T, and the reflected
+    shock's speed."""
+    from scipy.optimize import fsolve
+
+    R = R_U * float(np.sum(Y / mech.mw))
+    cp1 = mixture_cp(mech, T1, Y)
+    c1 = math.sqrt(cp1 / (cp1 - R) * R * T1)
+    rho1 = p1 / (R * T1)
+    W = mach * c1
+    h1 = mixture_enthalpy(mech, T1, Y)
+
+    def incident(x):
+        T2, r = x  # r = rho2 / rho1
+        w2 = W / r
+        p2 = rho1 * r * R * T2
+        return [(p1 + rho1 * W * W - p2 - rho1 * r * w2 * w2) / p1,
+                (h1 + 0.5 * W * W - mixture_enthalpy(mech, T2, Y) - 0.5 * w2 * w2) / h1 if h1 else 0.0]
+
+    T2, r2 = fsolve(incident, [2.0 * T1, 3.0], xtol=1e-12)
+    rho2, u2 = rho1 * r2, W * (1 - 1 / r2)
+    p2 = rho2 * R * T2
+    h2 = mixture_enthalpy(mech, T2, Y)
+
+    def reflected(x):
+        T5, r, Wr = x  # r = rho5 / rho2
+        wa, wb = u2 + Wr, Wr
+        p5 = rho2 * r * R * T5
+        return [(rho2 * wa - rho2 * r * wb) / (rho2 * u2),
+                (p2 + rho2 * wa * wa - p5 - rho2 * r * wb * wb) / p2,
+                (h2 + 0.5 * wa * wa - mixture_enthalpy(mech, T5, Y) - 0.5 * wb * wb) / abs(h2)]
+
+    T5, r5, Wr = fsolve(reflected, [1.7 * T2, 2.5, 0.5 * u2], xtol=1e-12)
+    rho5 = rho2 * r5
+    return (dict(rho=rho2, u=u2, p=rho2 * R * T2, T=T2), dict(rho=rho5, u=0.0, p=rho5 * R * T5, T=T5),
+            dict(incident_speed=W, reflected_speed=Wr, c1=c1))
+
+
+def reflected_shock_tube(mech, nx: int = 2048, ny: int = 512, length: float = 0.1, height: float = 0.025,
+                         stretch: float = 1.02, mach: float = 2.2, T1: float = 300.0, p1: float = 0.1 * 101325.0,
+                         x_shock: float | None = None, scheme: int = 52, viscous_order: int = 2) -> Case:
+    """Reflected-shock ignition: stoichiometric H2-O2 diluted by 70 % Ar (2 : 1 : 7
+    by mole) at (T1, p1), hit by an incident shock of Mach `mach`, as the gas
+    just after the shock has reflected from the closed end x = length: state 5
+    (at rest, hot) for x >= x_shock, state 2 (towards the wall) elsewhere,
+    from frozen Rankine-Hugoniot jumps (reflected_shock_states).  2-D block of
+    nx x ny nodes, uniform in x, stretched in y from the no-slip wall y = 0 by
+    the ratio `stretch` per cell; faces: x = 0 outflow, x = length adiabatic
+    no-slip wall (the end wall), y = 0 adiabatic no-slip wall, y = height
+    symmetry.  WENO5 characteristic (52) with mixture-averaged viscous fluxes;
+    the mechanism's reactions are kept."""
+    X = np.zeros(mech.n_spec)
+    X[mech.index("H2")], X[mech.index("O2")], X[mech.index("AR")] = 2.0, 1.0, 7.0
+    Y = mole_to_mass(mech, X / X.sum())
+    s2, s5, _ = reflected_shock_states(mech, Y, T1, p1, mach)
+    ngg = ghost_layers(scheme, viscous_order)
+    xs = np.linspace(0.0, length, nx)
+    widths = stretch ** np.arange(ny - 1)
+    ys = np.concatenate([[0.0], np.cumsum(widths)]) * (height / widths.sum())
+    x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
+    y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
+    z = np.zeros_like(x)
+    jac, metric, xg = metrics(x, y, z, ngg)
+    P = jac.size
+    x_shock = 0.9 * length if x_shock is None else x_shock
+    hot = xg >= x_shock
+    bv = np.zeros((6, P))
+    for l, key in ((0, "rho"), (1, "u"), (4, "p"), (5, "T")):
+        bv[l] = np.where(hot, s5[key], s2[key])
+    sv = np.repeat(Y[:, None], P, axis=1)
+    rho_ref, v_ref = s2["rho"], abs(s2["u"])
+    param = _mix_param(mech, dim=2, inviscid_scheme=scheme, reconstruction=2, cfl=0.5, viscous_order=viscous_order,
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=mech.n_reac,
+                       wall_thermal_type=1, wall_temperature=s5["T"], wall_catalytic_type=0)
+    faces = [(0, -1, 6), (0, 1, 2), (1, -1, 2), (1, 1, 3)]
+    return Case("reflected_shock_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=mech,
+                xyz=(x, y, z))

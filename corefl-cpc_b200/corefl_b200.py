@@ -63,6 +63,7 @@ class cfk_param(ctypes.Structure):
         ("v_ref", ctypes.c_double), ("rho_ref", ctypes.c_double), ("sensor_threshold", ctypes.c_double),
         ("device", ctypes.c_int), ("shock_sensor", ctypes.c_int), ("sensor_eps", ctypes.c_double),
         ("wall", cfk_wall), ("inflow", cfk_inflow), ("outflow", cfk_outflow),
+        ("limit_flow", ctypes.c_int), ("limit_ll", ctypes.c_double * 5), ("limit_ul", ctypes.c_double * 5),
     ]
 
 
@@ -181,6 +182,7 @@ def lib() -> ctypes.CDLL:
             "cfk_set_tile_variants": (i, [vp, ctypes.POINTER(i)]),
             "cfk_update_cv_and_bv_rk": (i, [vp, d, i, vp]),
             "cfk_update_physical_properties": (i, [vp, vp]),
+            "cfk_limit_flow": (i, [vp, ctypes.POINTER(ctypes.c_longlong), vp]),
             "cfk_compute_cv_from_bv": (i, [vp, vp]),
             "cfk_apply_boundary_conditions": (i, [vp, vp]),
             "cfk_eliminate_k_gradient": (i, [vp, vp]),
@@ -196,6 +198,9 @@ def lib() -> ctypes.CDLL:
             "cfk_rk3_step": (i, [vp, _DP, vp]),
             "cfk_rk3_step_graph": (i, [vp, _DP, vp]),
             "cfk_wu_splitting_step": (i, [vp, i, _DP, vp]),
+            "cfk_wu_splitting_step_record": (i, [vp, i, vp, vp, _DP, vp]),
+            "cfk_wu_splitting_step_surrogate": (i, [vp, ctypes.POINTER(cfk_surrogate_gate), i,
+                                                    ctypes.POINTER(cfk_surrogate_stats), _DP, vp]),
             "cfk_memcpy_h2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
             "cfk_memcpy_d2h": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
             "cfk_memcpy_d2d": (i, [vp, vp, vp, ctypes.c_size_t, vp]),
@@ -312,6 +317,8 @@ def make_param(p: dict, faces) -> cfk_param:
             setattr(cp.inflow, k[7:], v)
         elif k.startswith("outflow_"):
             setattr(cp.outflow, k[8:], v)
+        elif k in ("limit_ll", "limit_ul"):
+            setattr(cp, k, (ctypes.c_double * 5)(*v))
         elif k in dict(cfk_param._fields_):
             setattr(cp, k, v)
     cp.n_face = len(faces)
@@ -454,6 +461,12 @@ class Context:
     def update_rk(self, dt, rk, stream=None):
         self._ck(self.L.cfk_update_cv_and_bv_rk(self.h, dt, rk, stream), "update")
 
+    def limit_flow(self, stream=None) -> int:
+        """cfk_limit_flow: repairs the out-of-bounds nodes; returns their number."""
+        n = ctypes.c_longlong()
+        self._ck(self.L.cfk_limit_flow(self.h, ctypes.byref(n), stream), "limit_flow")
+        return n.value
+
     def properties(self, stream=None):
         self._ck(self.L.cfk_update_physical_properties(self.h, stream), "properties")
 
@@ -484,6 +497,24 @@ class Context:
         dt = ctypes.c_double(0.0)
         self._ck(self.L.cfk_wu_splitting_step(self.h, schedule, ctypes.byref(dt), stream), "wu_splitting_step")
         return dt.value
+
+    def wu_splitting_step_record(self, X_ptr, G_ptr, schedule=1, stream=None) -> float:
+        """cfk_wu_splitting_step_record: a plain Wu step that also writes one
+        training row per node into the device float arrays at X_ptr, G_ptr."""
+        dt = ctypes.c_double(0.0)
+        self._ck(self.L.cfk_wu_splitting_step_record(self.h, schedule, X_ptr, G_ptr, ctypes.byref(dt), stream),
+                 "wu_splitting_step_record")
+        return dt.value
+
+    def wu_splitting_step_surrogate(self, gate, step_index=0, want_stats=False, stream=None):
+        """cfk_wu_splitting_step_surrogate: returns (dt, stats or None)."""
+        dt = ctypes.c_double(0.0)
+        st = cfk_surrogate_stats() if want_stats else None
+        self._ck(self.L.cfk_wu_splitting_step_surrogate(self.h, ctypes.byref(gate), step_index,
+                                                        ctypes.byref(st) if st is not None else None,
+                                                        ctypes.byref(dt), stream), "wu_splitting_step_surrogate")
+        stats = {n: getattr(st, n) for n, _ in cfk_surrogate_stats._fields_} if st is not None else None
+        return dt.value, stats
 
     def sync(self, stream=None):
         self._ck(self.L.cfk_stream_sync(self.h, stream), "sync")

@@ -34,6 +34,8 @@ cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, c
 cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
                             cudaStream_t st, bool with_reaction = true);
+cudaError_t launch_limit_flow(const Zone &z, const Param &p, const Thermo *th, unsigned char *bad,
+                              unsigned long long *n_fixed, cudaStream_t st);
 cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces,
                                        int n_face, const cfk_wall &wall, const cfk_inflow &inflow,
                                        const cfk_outflow &outflow, cudaStream_t st, int *n_launch);
@@ -253,6 +255,11 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
   p.chem_advance_method = param->chem_advance_method;
   p.shock_sensor = param->shock_sensor; p.sensor_eps = param->sensor_eps;
   p.sensor_threshold = param->sensor_threshold;
+  p.limit_flow = param->limit_flow;
+  for (int l = 0; l < 5; ++l) {
+    p.limit_ll[l] = param->limit_ll[l];
+    p.limit_ul[l] = param->limit_ul[l];
+  }
   e = cudaMalloc(&c->d_dt_bits, 64);
   if (e != cudaSuccess) { delete c; return CFK_ERR_CUDA; }
   c->d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(c->d_dt_bits) + 8);
@@ -274,6 +281,7 @@ int cfk_destroy(cfk_ctx *c) {
   for (void *ptr : c->owned) cudaFree(ptr);
   if (c->own_sensor) cudaFree(c->own_sensor);
   if (c->own_fvis8) cudaFree(c->own_fvis8);
+  if (c->own_limit) cudaFree(c->own_limit);
   cudaFree(c->d_dt_bits);
   cudaFree(c->d_mech);
   delete c;
@@ -281,6 +289,23 @@ int cfk_destroy(cfk_ctx *c) {
 }
 
 const char *cfk_last_error(const cfk_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+// limit_flow's flag per interior node, owned by the context.
+static int ensure_limit_flags(cfk_ctx *c) {
+  const size_t n = (size_t)c->z.d.plane(0);
+  if (c->own_limit_n >= n) return CFK_OK;
+  if (c->own_limit) cudaFree(c->own_limit);
+  c->own_limit = nullptr;
+  c->own_limit_n = 0;
+  CFK_CHECK(c, cudaMalloc(&c->own_limit, n), "limit_flow flag allocation");
+  c->own_limit_n = n;
+  return CFK_OK;
+}
+
+// Device counter of the nodes limit_flow repaired (in the context's scratch line).
+static unsigned long long *limit_counter(cfk_ctx *c) {
+  return reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(c->d_dt_bits) + 24);
+}
 
 int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   if (!c || !zn) return CFK_ERR_ARG;
@@ -337,6 +362,9 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
     }
     CFK_CHECK(c, cudaMemset(c->own_sensor, 0, P * sizeof(double)), "shock sensor reset");
     z.shock_sensor = c->own_sensor;
+  }
+  if (c->p.limit_flow) {
+    if (int r = ensure_limit_flags(c)) return r;
   }
   c->bound = true;
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
@@ -579,6 +607,23 @@ int cfk_update_cv_and_bv_rk(cfk_ctx *c, double dt, int rk, void *stream) {
   return CFK_OK;
 }
 
+int cfk_limit_flow(cfk_ctx *c, long long *n_repaired, void *stream) {
+  NEED_ZONE(c);
+  if (int r = need_mech_for_mixture(c)) return r;
+  if (int r = ensure_limit_flags(c)) return r;
+  cudaStream_t st = S(stream);
+  CFK_CHECK(c, cudaMemsetAsync(limit_counter(c), 0, sizeof(unsigned long long), st), "limit_flow counter");
+  CFK_CHECK(c, launch_limit_flow(c->z, c->p, thermo_of(c), c->own_limit, limit_counter(c), st), "limit_flow");
+  c->launches += 2;
+  if (n_repaired) {
+    unsigned long long v = 0;
+    CFK_CHECK(c, cudaMemcpyAsync(&v, limit_counter(c), sizeof v, cudaMemcpyDeviceToHost, st), "limit_flow count");
+    CFK_CHECK(c, cudaStreamSynchronize(st), "limit_flow sync");
+    *n_repaired = (long long)v;
+  }
+  return CFK_OK;
+}
+
 int cfk_update_physical_properties(cfk_ctx *c, void *stream) {
   NEED_ZONE(c);
   if (int r = need_mech_for_mixture(c)) return r;
@@ -720,6 +765,11 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
       PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
       CFK_CHECK(c, launch_update_rk(z, p, th, c->hp.dt, dt_dev, rk, c->d_err, st), "update");
       ++n;
+      if (p.limit_flow) {
+        // limit_flow<M> after the update (reference src/RK.cuh:163-164)
+        CFK_CHECK(c, launch_limit_flow(z, p, th, c->own_limit, limit_counter(c), st), "limit_flow");
+        n += 2;
+      }
     }
     {
       PhaseScope ps(c, CFK_PH_BC, st, &n);
@@ -740,7 +790,43 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
 // One step of Wu's splitting (the loop body of wu_splitting, reference
 // src/StrangSplitting.cu:683-861).  With the CFL step the dt is read back to
 // the host once (the reaction kernels take it by value).
+// The reaction sub-step of a Wu step: the plain integrator (schedule 0/1),
+// optionally bracketed by the surrogate's training-row snapshot and record,
+// or the gated surrogate step.
+struct WuReaction {
+  int mode = 0;  // 0 plain, 1 plain with training rows, 2 surrogate
+  float *X = nullptr, *G = nullptr;
+  const cfk_surrogate_gate *gate = nullptr;
+  int step_index = 0;
+  cfk_surrogate_stats *stats = nullptr;
+};
+
+static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *dt_used, void *stream);
+
 int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *stream) {
+  return wu_splitting(c, schedule, WuReaction{}, dt_used, stream);
+}
+
+int cfk_wu_splitting_step_record(cfk_ctx *c, int schedule, float *X, float *G, double *dt_used, void *stream) {
+  if (!X || !G) return fail(c, CFK_ERR_ARG, "recording needs X and G");
+  WuReaction rx;
+  rx.mode = 1;
+  rx.X = X;
+  rx.G = G;
+  return wu_splitting(c, schedule, rx, dt_used, stream);
+}
+
+int cfk_wu_splitting_step_surrogate(cfk_ctx *c, const cfk_surrogate_gate *gate, int step_index,
+                                    cfk_surrogate_stats *stats, double *dt_used, void *stream) {
+  WuReaction rx;
+  rx.mode = 2;
+  rx.gate = gate;
+  rx.step_index = step_index;
+  rx.stats = stats;
+  return wu_splitting(c, 1, rx, dt_used, stream);
+}
+
+static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *dt_used, void *stream) {
   NEED_ZONE(c);
   if (c->hp.inviscid_scheme == 0) return fail(c, CFK_ERR_STATE, "inviscid_scheme 0 contexts have no transport step");
   if (!c->have_mech || c->hp.n_reac == 0) return fail(c, CFK_ERR_STATE, "no reacting mechanism loaded");
@@ -770,10 +856,22 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
   CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
   CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "Cn copy");
   // wu_reaction_subStep (:475-502)
-  unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
-  CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
-            "wu_reaction_step");
-  ++n;
+  if (rx.mode == 2) {
+    c->launches += n;
+    n = 0;
+    if (int r = cfk_surrogate_reaction_step(c, dt, rx.gate, rx.step_index, rx.stats, stream)) return r;
+  } else {
+    if (rx.mode == 1) {
+      if (int r = cfk_surrogate_record(c, 0, dt, nullptr, nullptr, stream)) return r;
+    }
+    unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
+    CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
+              "wu_reaction_step");
+    ++n;
+    if (rx.mode == 1) {
+      if (int r = cfk_surrogate_record(c, 1, dt, rx.X, rx.G, stream)) return r;
+    }
+  }
   CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
                                           c->hp.outflow, st, &n),
             "boundary conditions");
@@ -788,6 +886,11 @@ int cfk_wu_splitting_step(cfk_ctx *c, int schedule, double *dt_used, void *strea
     CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
     CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
     ++n;
+    if (p.limit_flow) {
+      // limit_flow<M> after the update (reference src/StrangSplitting.cu:602-604)
+      CFK_CHECK(c, launch_limit_flow(z, p, th, c->own_limit, limit_counter(c), st), "limit_flow");
+      n += 2;
+    }
     CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
                                           c->hp.outflow, st, &n),
             "boundary conditions");

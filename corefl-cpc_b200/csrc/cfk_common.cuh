@@ -55,6 +55,8 @@ struct Param {
   double weno_eps_scale, v_ref, rho_ref;
   int shock_sensor;                 // 0 modified Ducros, 1 modified Jameson, 2 density/pressure jump
   double sensor_eps, sensor_threshold;
+  int limit_flow;                   // limit_flow after every stage update
+  double limit_ll[5], limit_ul[5];  // bounds of rho, u, v, w, p
 };
 
 }  // namespace cfk

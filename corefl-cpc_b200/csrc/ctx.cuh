@@ -26,6 +26,8 @@ struct cfk_ctx {
   size_t own_sensor_n = 0;
   double *own_fvis8 = nullptr;   // node viscous fluxes of the 8th-order scheme
   size_t own_fvis8_n = 0;
+  unsigned char *own_limit = nullptr;  // limit_flow: out-of-bounds flag per interior node
+  size_t own_limit_n = 0;
   Mech *d_mech = nullptr;
   Mech h_mech{};  // host copy, passed by value to the kernels that read it from the constant bank
   bool have_mech = false;

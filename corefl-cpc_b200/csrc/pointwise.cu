@@ -129,6 +129,79 @@ __global__ void cv_from_bv_kernel(Zone z, Param p, const Thermo *th) {
 }
 
 // ---------------------------------------------------------------------------
+// limit_flow (reference src/TimeAdvanceFunc.cuh:117-220) in two passes, so
+// that every decision is taken on the values before the call: the first marks
+// the interior nodes whose density, velocity or pressure is NaN or outside the
+// bounds; the second replaces each marked node's rho, u, v, w, p by the mean
+// over the unmarked nodes of its 3 x 3 x 3 interior neighbourhood (k, j, i
+// loops from -1 to 1, the reference's order), or clamps them to the bounds
+// when there is none, then sets T from the state equation and cv from bv.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool out_of_bounds(const double *bv, int64_t id, int64_t sz, const Param &p) {
+  for (int l = 0; l < 5; ++l) {
+    const double v = bv[id + l * sz];
+    if (isnan(v) || v < p.limit_ll[l] || v > p.limit_ul[l]) return true;
+  }
+  return false;
+}
+
+__global__ void limit_flow_mark_kernel(Zone z, Param p, unsigned char *bad) {
+  const Dims d = z.d;
+  int i, j;
+  if (!flat_ij(d.mx, d.my, i, j)) return;
+  const int k = blockIdx.y;
+  const int64_t sz = d.plane(d.ngg);
+  bad[((int64_t)k * d.my + j) * d.mx + i] = out_of_bounds(z.bv, d.idx(d.ngg, i, j, k), sz, p) ? 1 : 0;
+}
+
+template <bool MIX>
+__global__ void limit_flow_fix_kernel(Zone z, Param p, const Thermo *th, const unsigned char *bad,
+                                      unsigned long long *n_fixed) {
+  const Dims d = z.d;
+  int i, j;
+  if (!flat_ij(d.mx, d.my, i, j)) return;
+  const int k = blockIdx.y;
+  if (!bad[((int64_t)k * d.my + j) * d.mx + i]) return;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
+  double upd[5] = {0, 0, 0, 0, 0};
+  int kn = 0;
+  for (int ka = -1; ka < 2; ++ka) {
+    const int k1 = k + ka;
+    if (k1 < 0 || k1 >= d.mz) continue;
+    for (int ja = -1; ja < 2; ++ja) {
+      const int j1 = j + ja;
+      if (j1 < 0 || j1 >= d.my) continue;
+      for (int ia = -1; ia < 2; ++ia) {
+        const int i1 = i + ia;
+        if (i1 < 0 || i1 >= d.mx) continue;
+        if (bad[((int64_t)k1 * d.my + j1) * d.mx + i1]) continue;
+        const int64_t n1 = d.idx(g, i1, j1, k1);
+        for (int l = 0; l < 5; ++l) upd[l] += z.bv[n1 + l * sz];
+        ++kn;
+      }
+    }
+  }
+  if (kn > 0) {
+    const double kn_inv = 1.0 / kn;
+    for (int l = 0; l < 5; ++l) upd[l] *= kn_inv;
+  } else {
+    // fmax(NaN, ll) = ll, as the reference's max(var, ll) gives
+    for (int l = 0; l < 5; ++l) upd[l] = fmin(fmax(z.bv[id + l * sz], p.limit_ll[l]), p.limit_ul[l]);
+  }
+  for (int l = 0; l < 5; ++l) z.bv[id + l * sz] = upd[l];
+  if (MIX) {
+    double R = 0;
+    for (int l = 0; l < p.n_spec; ++l) R += z.sv[id + l * sz] * th->gas_const[l];
+    z.bv[id + 5 * sz] = upd[4] / (upd[0] * R);
+  } else {
+    z.bv[id + 5 * sz] = upd[4] * kMwAir / (upd[0] * kRu);
+  }
+  cv_from_bv_point<MIX>(z, p, th, id);
+  atomicAdd(n_fixed, 1ull);
+}
+
+// ---------------------------------------------------------------------------
 // update_physical_properties (reference src/FieldOperation.cuh:86-120) over
 // the padded block.  The mixture branch also computes the mixture-averaged
 // transport properties (reference src/Transport.cu:43-165).
@@ -677,6 +750,14 @@ cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, do
   return cudaGetLastError();
 }
 
+cudaError_t launch_limit_flow(const Zone &z, const Param &p, const Thermo *th, unsigned char *bad,
+                              unsigned long long *n_fixed, cudaStream_t st) {
+  limit_flow_mark_kernel<<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, bad);
+  if (p.n_spec > 0) limit_flow_fix_kernel<true><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, bad, n_fixed);
+  else limit_flow_fix_kernel<false><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, bad, n_fixed);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st) {
   if (p.n_spec > 0) cv_from_bv_kernel<true><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
   else cv_from_bv_kernel<false><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
@@ -699,7 +780,12 @@ cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, uns
   return cudaGetLastError();
 }
 
-static FaceGeom make_face(const Dims &d, const cfk_face &f) {
+// A face's node range: its tangential extent widened by ngg ghosts only with
+// the 2nd-order viscous scheme, as the reference registers its boundaries
+// (src/Mesh.cpp:14-31, 637: need_extend_boundary = viscous_order == 2); for a
+// 2-D block the k range is then [-ngg, ngg], else [0, 0].
+static FaceGeom make_face(const Dims &d, const cfk_face &f, int viscous_order) {
+  const int g = viscous_order == 2 ? d.ngg : 0;
   FaceGeom fg;
   fg.face = f.face;
   fg.direction = f.direction;
@@ -709,11 +795,11 @@ static FaceGeom make_face(const Dims &d, const cfk_face &f) {
       fg.lo[a] = f.direction < 0 ? 0 : m[a] - 1;
       fg.n[a] = 1;
     } else {
-      fg.lo[a] = -d.ngg;
-      fg.n[a] = m[a] + 2 * d.ngg;
+      fg.lo[a] = -g;
+      fg.n[a] = m[a] + 2 * g;
     }
   }
-  if (d.mz == 1) { fg.lo[2] = -d.ngg; fg.n[2] = 2 * d.ngg + 1; }
+  if (d.mz == 1) { fg.lo[2] = -g; fg.n[2] = 2 * g + 1; }
   return fg;
 }
 
@@ -725,7 +811,7 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
   for (int o = 0; o < 5; ++o) {
     for (int n = 0; n < n_face; ++n) {
       if (faces[n].label != order[o]) continue;
-      const FaceGeom fg = make_face(z.d, faces[n]);
+      const FaceGeom fg = make_face(z.d, faces[n], p.viscous_order);
       const bool split = order[o] != 5;  // the inflow kernel keeps a face node's line in one thread
       const int cnt = fg.n[0] * fg.n[1] * fg.n[2] * (split && fg.face == 0 ? z.d.ngg + 1 : 1);
       const int blocks = (cnt + 127) / 128;

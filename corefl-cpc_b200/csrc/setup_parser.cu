@@ -282,6 +282,13 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
   p.shock_sensor = get(s.ints, "shock_sensor", 0);
   p.sensor_eps = get(s.reals, "shockSensor_epsilon", -1.0);
   const int species = get(s.ints, "species", 0);
+  // hardCodedMech > 0 selects the reference's hard-coded H2/air kinetics
+  // (src/FiniteRateChem.cu:19-358, src/StrangSplitting.cu:423-473, 479-484),
+  // whose arithmetic order differs from the table-driven kinetics this
+  // library implements: rejected rather than silently replaced
+  if (const int hc = get(s.ints, "hardCodedMech", 0); hc != 0)
+    return report("hardCodedMech = " + std::to_string(hc) +
+                  ": the hard-coded kinetics are not implemented; use the mechanism tables (hardCodedMech = 0)");
   if (species != 0) return report("species != 0 needs a mechanism; pass n_spec/n_scalar explicitly");
   p.n_spec = 0;
   p.n_scalar = 0;
@@ -291,6 +298,7 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
   const std::string ref = get(s.strings, "reference_state", std::string());
   p.rho_ref = 1.0;
   p.v_ref = 1.0;
+  double p_inf = 1.0;
   auto it = s.structs.find(ref);
   if (it != s.structs.end()) {
     const Struct &st = it->second;
@@ -303,10 +311,24 @@ extern "C" int cfk_param_from_setup(const char *setup_path, cfk_param *out, char
     if (mach < 0) mach = velocity / c;
     else velocity = mach * c;
     if (density < 0) density = pressure * mw / (R_u * temperature);
+    if (pressure < 0) pressure = density * temperature * R_u / mw;
     p.rho_ref = density;
     p.v_ref = std::fabs(velocity) < 1 ? c : velocity;
+    p_inf = pressure;
   }
   p.weno_eps_scale = p.rho_ref * p.v_ref * p.rho_ref * p.v_ref;
+  // limit_flow and its bounds from the reference state: rho_inf, v_inf (the
+  // speed of sound below 1 m/s) and p_inf (reference src/DParameter.cu:333-349,
+  // src/BoundCond.cpp:276-290)
+  p.limit_flow = get(s.bools, "limit_flow", false);
+  p.limit_ll[0] = 1e-6 * p.rho_ref;
+  p.limit_ul[0] = 1e+3 * p.rho_ref;
+  for (int l = 1; l < 4; ++l) {
+    p.limit_ll[l] = -1000 * p.v_ref;
+    p.limit_ul[l] = 1000 * p.v_ref;
+  }
+  p.limit_ll[4] = 1e-6 * p_inf;
+  p.limit_ul[4] = 1e+3 * p_inf;
   if (!read_wall(s, p.wall, err)) return report(err);
   if (!read_inflow(s, p.inflow, err)) return report(err);
   if (!read_outflow(s, p.outflow, err)) return report(err);

@@ -128,6 +128,11 @@ typedef struct cfk_param {
   cfk_wall wall;           /* read for faces labelled 2 */
   cfk_inflow inflow;       /* read for faces labelled 5 */
   cfk_outflow outflow;     /* read for faces labelled 6 */
+  int limit_flow;          /* 1: limit_flow after every stage update (reference src/RK.cuh:163-164,
+                              src/StrangSplitting.cu:602-604); needs the bounds below */
+  double limit_ll[5];      /* lower bounds of rho, u, v, w, p (reference src/DParameter.cu:333-349:
+                              1e-6 rho_inf, -1000 v_inf, 1e-6 p_inf) */
+  double limit_ul[5];      /* upper bounds (1e3 rho_inf, 1000 v_inf, 1e3 p_inf) */
 } cfk_param;
 
 /* Device pointers of one block, field for field the arrays of the reference's
@@ -218,6 +223,18 @@ int cfk_set_tile_variants(cfk_ctx *ctx, const int *var);
 /* SSP-RK3 stage update of cv and bv/sv.  Replaces update_cv_and_bv_rk<M>
  * (reference src/RK.cuh:224-281). */
 int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);
+/* Replaces limit_flow<M> (reference src/TimeAdvanceFunc.cuh:117-220), with the
+ * bounds param->limit_ll / limit_ul: every interior node whose density,
+ * velocity or pressure is NaN or outside the bounds takes the mean of the
+ * in-bounds nodes of its 3x3x3 neighbourhood (clamped to the bounds when there
+ * is none), its temperature from the state equation and its cv from bv.  All
+ * decisions are taken on the values before the call (the reference reads
+ * neighbours while other threads rewrite them).  *n_repaired (may be NULL)
+ * receives the number of repaired nodes; it synchronises the stream.  The
+ * first call on a context whose param has limit_flow = 0 allocates one byte
+ * per node; RK3 and Wu steps call it after each stage update when
+ * limit_flow = 1. */
+int cfk_limit_flow(cfk_ctx *ctx, long long *n_repaired, void *stream);
 /* Replaces update_physical_properties<M> (reference src/FieldOperation.cuh:86-120). */
 int cfk_update_physical_properties(cfk_ctx *ctx, void *stream);
 /* Replaces compute_cv_from_bv<M> (reference src/FieldOperation.cuh:39-64). */
@@ -417,10 +434,11 @@ typedef struct cfk_surrogate_stats {
  * the element mass fractions per species (a_ek W_e / W_k) used by the
  * conservation projection; n_elem <= 4. */
 int cfk_surrogate_init(cfk_ctx *ctx, unsigned long long seed, int n_elem, const double *elem_mu);
-/* Training data from the plain integrator: phase 0 before a reaction step
- * snapshots (T, p, Y) of every node; phase 1 after it writes one row per node
- * (node order i fastest) of raw features X[.][12] and targets G[.][11]
- * (device float arrays). */
+/* Training data from the plain integrator: phase 0 before a reaction step of
+ * length dt snapshots every node's state (where the zone has a transport term
+ * Cn, the states it alone reaches at the middle and the end of the step);
+ * phase 1 after it writes one row per node (node order i fastest) of raw
+ * features X[.][12] and targets G[.][11] (device float arrays). */
 int cfk_surrogate_record(cfk_ctx *ctx, int phase, double dt, float *X, float *G, void *stream);
 /* Standardisation from n rows of (X, G) on the device; the output scales
  * are the median |g_j| of a strided sample of the rows. */
@@ -456,6 +474,23 @@ int cfk_surrogate_default_gate(cfk_surrogate_gate *gate);
  * call synchronise the stream and report the counts. */
 int cfk_surrogate_reaction_step(cfk_ctx *ctx, double dt, const cfk_surrogate_gate *gate, int step_index,
                                 cfk_surrogate_stats *stats, void *stream);
+/* cfk_wu_splitting_step whose reaction sub-step (the plain integrator with
+ * the frozen transport term Cn, reference src/StrangSplitting.cu:475-502)
+ * also writes one training row per node, as cfk_surrogate_record does around
+ * a reactor step: the features are read at the state the frozen transport
+ * term alone reaches half-way through the sub-step, the targets are the
+ * changes from the state it reaches at the end.  X, G: device float arrays
+ * of mx*my*mz rows.  Needs cfk_surrogate_init. */
+int cfk_wu_splitting_step_record(cfk_ctx *ctx, int schedule, float *X, float *G, double *dt_used, void *stream);
+/* cfk_wu_splitting_step with the gated surrogate as its reaction sub-step:
+ * each node's change is predicted from its mid-sub-step transported state
+ * and applied to its end-of-sub-step transported state (with Cn = 0 both are
+ * the node's own state, as in cfk_surrogate_reaction_step); nodes the gate
+ * or the judge send to the plain integrator integrate with the frozen Cn.
+ * The transport half-steps are those of the plain step.  stats as in
+ * cfk_surrogate_reaction_step. */
+int cfk_wu_splitting_step_surrogate(cfk_ctx *ctx, const cfk_surrogate_gate *gate, int step_index,
+                                    cfk_surrogate_stats *stats, double *dt_used, void *stream);
 
 /* ---- measurement ------------------------------------------------------ */
 /* Phases of a step timed with CUDA events when profiling is on (plain steps

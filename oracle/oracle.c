@@ -827,11 +827,12 @@ double orc_global_time_step(const orc_zone *z) {
 /* no-slip wall (src/BoundCond.cu:2761-3031), inflow (src/BoundCond.cu:2190) */
 /* applied per label in the reference's priority order                       */
 /* (src/BoundCond.cu:3489-3619): outflow, inflow, symmetry, wall, periodic.  */
-/* Each face covers its tangential range widened by ngg ghosts               */
-/* (src/Mesh.cpp:14-31).                                                     */
+/* Each face covers its tangential range, widened by ngg ghosts only when    */
+/* viscous_order == 2 (src/Mesh.cpp:14-31, 637: need_extend_boundary); for  */
+/* a 2-D block the k range is then [-ngg, ngg], else [0, 0].                 */
 /* ------------------------------------------------------------------------ */
-static void face_range(const orc_zone *z, const orc_face *f, int lo[3], int hi[3]) {
-  const int g = z->ngg;
+static void face_range(const orc_zone *z, const orc_param *p, const orc_face *f, int lo[3], int hi[3]) {
+  const int g = p->viscous_order == 2 ? z->ngg : 0;
   const int m[3] = {z->mx, z->my, z->mz};
   for (int d = 0; d < 3; ++d) {
     if (d == f->face) {
@@ -848,7 +849,7 @@ static void apply_outflow_face(orc_zone *z, const orc_param *p, const orc_face *
   const int g = z->ngg;
   const long sz = psz(z, g);
   int lo[3], hi[3];
-  face_range(z, f, lo, hi);
+  face_range(z, p, f, lo, hi);
   const long s = pstride(z, g, f->face) * f->direction;
   const int ns = p->mech ? p->n_spec : 0;
   double *bv = z->bv, *sv = z->sv;
@@ -944,7 +945,7 @@ static void apply_periodic_face(orc_zone *z, const orc_param *p, const orc_face 
   const int g = z->ngg;
   const long sz = psz(z, g);
   int lo[3], hi[3];
-  face_range(z, f, lo, hi);
+  face_range(z, p, f, lo, hi);
   const int m[3] = {z->mx, z->my, z->mz};
   const long sd = pstride(z, g, f->face);
   const long s = sd * f->direction;
@@ -988,7 +989,7 @@ static void apply_wall_face(orc_zone *z, const orc_param *p, const orc_face *f) 
   const int g = z->ngg;
   const long sz = psz(z, g);
   int lo[3], hi[3];
-  face_range(z, f, lo, hi);
+  face_range(z, p, f, lo, hi);
   const long s = pstride(z, g, f->face) * f->direction;
   const int ns = p->mech ? p->n_spec : 0;
   const int catalytic = ns > 0 && p->wall_catalytic_type == 1;
@@ -1052,7 +1053,7 @@ static void apply_inflow_face(orc_zone *z, const orc_param *p, const orc_face *f
   const int g = z->ngg;
   const long sz = psz(z, g);
   int lo[3], hi[3];
-  face_range(z, f, lo, hi);
+  face_range(z, p, f, lo, hi);
   const long s = pstride(z, g, f->face) * f->direction;
   const int mix = p->mech != NULL;
   double *bv = z->bv, *sv = z->sv;
@@ -1134,7 +1135,7 @@ static void apply_symmetry_face(orc_zone *z, const orc_param *p, const orc_face 
   const int g = z->ngg;
   const long sz = psz(z, g);
   int lo[3], hi[3];
-  face_range(z, f, lo, hi);
+  face_range(z, p, f, lo, hi);
   const long s = pstride(z, g, f->face) * f->direction;
   const int mf = 3 * f->face;
   for (int k = lo[2]; k <= hi[2]; ++k)
@@ -1403,6 +1404,7 @@ double orc_wu_splitting_step(orc_zone *z, const orc_param *p, double dt_fixed) {
     orc_compute_viscous_flux(z, p);
     orc_compute_inviscid_flux(z, p);
     orc_update_cv_and_bv_rk_wu(z, p, 0.5 * dt, rk);
+    if (p->limit_flow) orc_limit_flow(z, p, p->limit_ll, p->limit_ul);
     orc_apply_boundary_conditions(z, p);
     if (z->mz == 1) orc_eliminate_k_gradient(z, p);
   }
@@ -1426,6 +1428,7 @@ double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed) {
     if (p->mech && p->n_reac > 0) orc_finite_rate_chemistry(z, p);
     orc_compute_inviscid_flux(z, p);
     orc_update_cv_and_bv_rk(z, p, dt, rk);
+    if (p->limit_flow) orc_limit_flow(z, p, p->limit_ll, p->limit_ul);
     orc_apply_boundary_conditions(z, p);
     if (z->mz == 1) orc_eliminate_k_gradient(z, p);
     orc_update_physical_properties(z, p);

@@ -104,6 +104,10 @@ typedef struct {
   /* outflow faces (src/BoundCond.h:125-134): if_backPressure, backPressure */
   int outflow_back_pressure_on;
   double outflow_back_pressure;
+  /* limit_flow after each stage update (src/RK.cuh:163-164,
+   * src/StrangSplitting.cu:602-604) with the bounds of rho, u, v, w, p */
+  int limit_flow;
+  double limit_ll[5], limit_ul[5];
 } orc_param;
 
 /* A face shared by two blocks of a multi-block mesh, as InnerFace holds it

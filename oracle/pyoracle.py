@@ -46,6 +46,7 @@ class orc_param(ctypes.Structure):
         ("inflow_v", ctypes.c_double), ("inflow_w", ctypes.c_double), ("inflow_pressure", ctypes.c_double),
         ("inflow_temperature", ctypes.c_double), ("inflow_mw", ctypes.c_double), ("inflow_sv", ctypes.c_double * 20),
         ("outflow_back_pressure_on", ctypes.c_int), ("outflow_back_pressure", ctypes.c_double),
+        ("limit_flow", ctypes.c_int), ("limit_ll", ctypes.c_double * 5), ("limit_ul", ctypes.c_double * 5),
     ]
 
 
@@ -218,7 +219,7 @@ class OracleZone:
             setattr(self.z, k, _ptr(a))
         self.p = orc_param()
         for k, v in c.param.items():
-            if k in ("wall_yk", "inflow_sv"):
+            if k in ("wall_yk", "inflow_sv", "limit_ll", "limit_ul"):
                 arr = getattr(self.p, k)
                 for l, y in enumerate(v):
                     arr[l] = y

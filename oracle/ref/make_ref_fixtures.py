@@ -112,6 +112,10 @@ def setup_txt(spec: Spec) -> str:
         ]
     else:
         out += ["int species = 0", "int reaction = 0"]
+    if float(p.get("sensor_threshold", 0.0)) > 1e-10:
+        out += [f"int shock_sensor = {int(p['shock_sensor'])}",
+                f"real shockSensor_threshold = {float(p['sensor_threshold'])!r}",
+                f"real shockSensor_epsilon = {float(p['sensor_eps'])!r}"]
     labels = sorted({lab for _, _, lab in c.faces})
     names = {6: "outflow", 8: "periodic", 2: "wall", 5: "inflow", 3: "symmetry"}
     bc_names = [names[lab] for lab in labels]
@@ -123,20 +127,44 @@ def setup_txt(spec: Spec) -> str:
     out.append("}")
     text = "\n".join(out) + "\n"
     for lab, n in zip(labels, bc_names):
-        text += _struct(n, {"type": n, "label": int(lab)})
+        text += _struct(n, bc_entries(c, n, int(lab)))
     text += spec.reference_state
     text += spec.setup_extra
     return text
 
 
+def bc_entries(c, name: str, label: int) -> dict:
+    """The setup.txt struct of one boundary condition from the case settings
+    (reference src/BoundCond.cpp:9-120 Inflow, :480-528 Wall, :597-618 Outflow)."""
+    p = c.param
+    e = {"type": name, "label": label}
+    if name == "wall":
+        e["thermal_type"] = "adiabatic" if int(p.get("wall_thermal_type", 0)) == 1 else "isothermal"
+        e["temperature"] = float(p.get("wall_temperature", 300.0))
+        if c.mech is not None and int(p.get("wall_catalytic_type", 0)) == 1:
+            e["catalytic_type"] = 1
+            for k, y in enumerate(p["wall_yk"]):
+                e[c.mech.species[k]] = float(y)
+    elif name == "inflow":
+        u, v, w = (float(p[k]) for k in ("inflow_u", "inflow_v", "inflow_w"))
+        if v != 0.0 or w != 0.0 or u <= 0.0:
+            raise ValueError("inflow fixtures use a velocity along +x (the reference scales a direction by |V|)")
+        e.update(density=float(p["inflow_density"]), velocity=u, pressure=float(p["inflow_pressure"]),
+                 u=1.0, v=0.0, w=0.0, inflow_sub=int(p.get("inflow_subsonic", 0)))
+        if c.mech is not None:
+            for k, y in enumerate(p["inflow_sv"]):
+                e[c.mech.species[k]] = float(y)
+    elif name == "outflow" and int(p.get("outflow_back_pressure_on", 0)) == 1:
+        e.update(if_backPressure=1, backPressure=float(p["outflow_back_pressure"]))
+    return e
+
+
 def write_grid(spec: Spec, d: str):
     c = spec.case
     mx, my, mz = spec.block_shape or (c.mx, c.my, c.mz)
-    # interior node coordinates [k, j, i], attached by the spec builders below
-    xyz = spec.case.__dict__.get("_xyz")
-    if xyz is None:
-        raise ValueError(f"{spec.name}: interior coordinates not attached")
-    x, y, z = xyz
+    if c.xyz is None:
+        raise ValueError(f"{spec.name}: the case carries no node coordinates")
+    x, y, z = c.xyz
     with open(os.path.join(d, "input", "grid", "grid   0.grd"), "w") as f:
         f.write("1\n")
         f.write(f"{mx} {my} {mz}\n")
@@ -233,57 +261,115 @@ def collect(spec: Spec, d: str) -> dict:
     return res
 
 
-def _attach_xyz(case, x, y, z):
-    case.__dict__["_xyz"] = (x, y, z)
-    return case
+def _air_state(name, rho, u, p):
+    return _struct(name, {"type": "inflow", "label": 5, "density": rho, "velocity": abs(u), "pressure": p,
+                          "u": 1.0 if u >= 0 else -1.0, "v": 0.0, "w": 0.0})
+
+
+def _ref(name):
+    return f"string default_init = {name}\nstring reference_state = {name}\n"
+
+
+def _sod_ref():
+    return (_struct("left", {"type": "inflow", "label": 5, "density": 1.0, "velocity": 0.0, "pressure": 1.0}) +
+            _struct("right", {"type": "inflow", "label": 5, "density": 0.125, "velocity": 0.0, "pressure": 0.1}) +
+            _ref("left") + "int groups_init = 2\n" +
+            _struct("init_cond_0", {"x0": 0.5, "x1": 1.5, "y0": -10.0, "y1": 10.0, "z0": -2.0, "z1": 2.0,
+                                    "name": "right"}))
 
 
 def _sod():
     c = cases.sod(400, 7, scheme=52, cfl=0.5)
-    xs = np.linspace(0.0, 1.0, 400)
-    ys = np.arange(7) * 0.01
-    x = np.broadcast_to(xs[None, None, :], (1, 7, 400)).copy()
-    y = np.broadcast_to(ys[None, :, None], (1, 7, 400)).copy()
-    _attach_xyz(c, x, y, np.zeros_like(x))
-    ref = (_struct("left", {"type": "inflow", "label": 5, "density": 1.0, "velocity": 0.0, "pressure": 1.0}) +
-           _struct("right", {"type": "inflow", "label": 5, "density": 0.125, "velocity": 0.0, "pressure": 0.1}) +
-           "string default_init = left\nstring reference_state = left\nint groups_init = 2\n" +
-           _struct("init_cond_0", {"x0": 0.5, "x1": 1.5, "y0": -10.0, "y1": 10.0, "z0": -2.0, "z1": 2.0,
-                                   "name": "right"}))
-    return Spec("sod_400x7_weno5", c, "rk3", 20, override_init=False, reference_state=ref)
+    return Spec("sod_400x7_weno5", c, "rk3", 20, override_init=False, reference_state=_sod_ref())
+
+
+def _sod_scheme(scheme, recon, steps=10):
+    c = cases.sod(200, 7, scheme=scheme, reconstruction=recon, cfl=0.5)
+    return Spec(f"sod_200x7_s{scheme}_r{recon}", c, "rk3", steps, override_init=False, reference_state=_sod_ref())
+
+
+def _sod_hybrid():
+    c = cases.sod(200, 7, scheme=52, cfl=0.5)
+    c.param.update(sensor_threshold=0.02, shock_sensor=1, sensor_eps=-1.0)
+    return Spec("sod_200x7_hybrid_jameson", c, "rk3", 10, override_init=False, reference_state=_sod_ref())
+
+
+def _sine_ref():
+    return _air_state("freestream", 1.0, 1.0, 1.0 / cases.GAMMA_AIR) + _ref("freestream")
 
 
 def _sine(n=21):
     c = cases.perturbed(cases.sine_wave(n=n, scheme=72, viscous=True), seed=7)
-    # the builder's coordinates, recomputed the same way
-    p0 = 1.0 / cases.GAMMA_AIR
-    T0 = p0 * cases.MW_AIR / (1.0 * cases.R_U)
-    mu0 = 1.7894e-5 * (T0 / 288.16) ** 1.5 * (288.16 + 110) / (T0 + 110)
-    L = 1000.0 * mu0
-    g = np.linspace(0.0, 1.0, n)
-    Z3, Y3, X3 = np.meshgrid(g, g, g, indexing="ij")
-    x = (X3 + 0.05 * np.sin(2 * np.pi * Y3) * np.sin(2 * np.pi * Z3)) * L
-    _attach_xyz(c, x, Y3 * L, Z3 * L)
-    ref = (_struct("freestream", {"type": "inflow", "label": 5, "density": 1.0, "velocity": 1.0,
-                                  "pressure": p0, "u": 1.0, "v": 0.0, "w": 0.0}) +
-           "string default_init = freestream\nstring reference_state = freestream\n")
-    return Spec(f"sine_{n}_weno7_visc", c, "rk3", 4, reference_state=ref)
+    return Spec(f"sine_{n}_weno7_visc", c, "rk3", 4, reference_state=_sine_ref())
+
+
+def _sine_visc8():
+    c = cases.perturbed(cases.sine_wave(n=15, ny=13, nz=11, scheme=72, viscous_order=8), seed=9, amp=1e-2)
+    return Spec("sine_15x13x11_weno7_visc8", c, "rk3", 3, reference_state=_sine_ref())
+
+
+def _channel_walls():
+    base = cases.perturbed(cases.sine_wave(n=17, ny=13, nz=9, scheme=52, viscous=True), seed=5, amp=2e-2)
+    c = cases.with_walls(base, thermal_type=0)
+    return Spec("channel_17x13x9_walls_weno5_visc", c, "rk3", 3, reference_state=_sine_ref())
+
+
+# The boundary-condition runs use a fixed step: the reference's grid minimum
+# of the CFL step (global_time_step / min_of_arr, src/TimeAdvanceFunc.cu:102-152)
+# lets blocks overwrite the partial minima other blocks are still reading and
+# returns before the barrier in partly filled blocks; on these 576-node tubes
+# its own run gave dt = 0 on the first step.
+def _duct_inflow():
+    base = cases.sod(64, 9, scheme=52, cfl=0.5)
+    c = cases.with_inflow(base, rho=1.1, u=2.0, p=0.8, subsonic=0)
+    c.param.update(fixed_dt=1, dt=2e-3)
+    # the inflow boundary's own struct is the reference state
+    return Spec("duct_64x9_supersonic_inflow_fixed_dt", c, "rk3", 10, reference_state=_ref("inflow"))
+
+
+def _duct_subsonic_back_pressure():
+    base = cases.sod(64, 9, scheme=52, cfl=0.5)
+    c = cases.with_back_pressure(cases.with_inflow(base, rho=1.1, u=0.5, p=0.8, subsonic=1), 0.7)
+    c.param.update(fixed_dt=1, dt=2e-3)
+    return Spec("duct_64x9_subsonic_inflow_back_pressure_fixed_dt", c, "rk3", 10, reference_state=_ref("inflow"))
+
+
+def _tube_back_pressure():
+    c = cases.with_back_pressure(cases.sod(64, 9, scheme=52, cfl=0.5), 0.5)
+    c.param.update(fixed_dt=1, dt=2e-3)
+    return Spec("tube_64x9_back_pressure_fixed_dt", c, "rk3", 10, override_init=False, reference_state=_sod_ref())
+
+
+TUBE_LEFT_Y = {"H2": 0.012772428, "O2": 0.101362139, "AR": 0.885865433}
+
+
+def _tube_ref():
+    return (_struct("left", dict({"type": "inflow", "label": 5, "density": 0.18075, "velocity": 0.0,
+                                  "pressure": 35594.0, "u": 1.0, "v": 0.0, "w": 0.0}, **TUBE_LEFT_Y)) + _ref("left"))
 
 
 def _tube():
-    mech = mechanism.load("premix_h2_ar")
-    nx, ny, length = 64, 7, 0.1
-    c = cases.mix_tube(mech, nx, ny, scheme=52, reacting=True)
-    xs = np.linspace(0.0, length, nx)
-    ys = np.arange(ny) * length / 100.0
-    x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
-    y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
-    _attach_xyz(c, x, y, np.zeros_like(x))
-    Y = {"H2": 0.012772428, "O2": 0.101362139, "AR": 0.885865433}
-    ref = (_struct("left", dict({"type": "inflow", "label": 5, "density": 0.18075, "velocity": 0.0,
-                                 "pressure": 35594.0, "u": 1.0, "v": 0.0, "w": 0.0}, **Y)) +
-           "string default_init = left\nstring reference_state = left\n")
-    return Spec("tube_h2o2ar_wu", c, "wu", 5, mech_name="premix_h2_ar", reference_state=ref)
+    c = cases.mix_tube(mechanism.load("premix_h2_ar"), 64, 7, scheme=52, reacting=True)
+    return Spec("tube_h2o2ar_wu", c, "wu", 5, mech_name="premix_h2_ar", reference_state=_tube_ref())
+
+
+def _mix_tube_roe():
+    c = cases.mix_tube(mechanism.load("premix_h2_ar"), 64, 7, scheme=2, reconstruction=2)
+    return Spec("mixtube_64x7_roe_muscl", c, "rk3", 8, mech_name="premix_h2_ar", reference_state=_tube_ref())
+
+
+def _mix_wave(reacting):
+    mech = mechanism.load("li2004")
+    if reacting:
+        c = cases.mix_wave(mech, 13, ny=11, nz=9, scheme=72, reacting=True, T0=1400.0)
+        name = "mixwave_13x11x9_weno7_visc_reacting"
+    else:
+        c = cases.mix_wave(mech, 13, ny=11, nz=9, scheme=72)
+        name = "mixwave_13x11x9_weno7_visc"
+    Y = {mech.species[k]: float(c.sv[k, 0]) for k in range(mech.n_spec)}
+    ref = _struct("stream", dict({"type": "inflow", "label": 5, "density": float(c.bv[0, 0]), "velocity": 50.0,
+                                  "pressure": 101325.0, "u": 1.0, "v": 0.0, "w": 0.0}, **Y)) + _ref("stream")
+    return Spec(name, c, "rk3", 2, mech_name="li2004", reference_state=ref)
 
 
 def _reactors(n_side=32, steps=10, dt=1e-7):
@@ -291,7 +377,7 @@ def _reactors(n_side=32, steps=10, dt=1e-7):
     n = n_side * n_side
     base = cases.reactor_batch(mech, n, seed=2024)
     # the same reactors as an n_side x n_side 2-D block with the ghost layers
-    # of the reference's default inviscid scheme for a reacting mixture run
+    # of the reference's WENO5 scheme
     ngg = cases.ghost_layers(52)
     shape = (1 + 2 * ngg, n_side + 2 * ngg, n_side + 2 * ngg)
 
@@ -303,24 +389,42 @@ def _reactors(n_side=32, steps=10, dt=1e-7):
     P = shape[0] * shape[1] * shape[2]
     metric = np.zeros((9, P))
     metric[0] = metric[4] = metric[8] = 1.0
-    c = dataclasses.replace(base, mx=n_side, my=n_side, mz=1, ngg=ngg, bv=bv, sv=sv, metric=metric,
-                            jac=np.ones(P), faces=[(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)])
-    c.param.update(inviscid_scheme=52, fixed_dt=1, dt=dt)
     xs = np.arange(n_side, dtype=np.float64)
     x = np.broadcast_to(xs[None, None, :], (1, n_side, n_side)).copy()
     y = np.broadcast_to(xs[None, :, None], (1, n_side, n_side)).copy()
-    _attach_xyz(c, x, y, np.zeros_like(x))
+    c = dataclasses.replace(base, mx=n_side, my=n_side, mz=1, ngg=ngg, bv=bv, sv=sv, metric=metric,
+                            jac=np.ones(P), faces=[(0, -1, 6), (0, 1, 6), (1, -1, 6), (1, 1, 6)],
+                            xyz=(x, y, np.zeros_like(x)), param=dict(base.param, inviscid_scheme=52, fixed_dt=1,
+                                                                     dt=dt))
     X = np.zeros(mech.n_spec)
     X[mech.index("H2")], X[mech.index("O2")], X[mech.index("N2")] = 2.0, 1.0, 3.76
     Yd = cases.mole_to_mass(mech, X / X.sum())
     st = {"type": "inflow", "label": 5, "density": 1.0, "velocity": 0.0, "pressure": 101325.0,
           "u": 1.0, "v": 0.0, "w": 0.0}
     st.update({mech.species[k]: float(Yd[k]) for k in range(mech.n_spec)})
-    ref = _struct("still", st) + "string default_init = still\nstring reference_state = still\n"
-    return Spec("reactors_li2004_1024", c, "react", steps, react_dt=dt, mech_name="li2004", reference_state=ref)
+    return Spec("reactors_li2004_1024", c, "react", steps, react_dt=dt, mech_name="li2004",
+                reference_state=_struct("still", st) + _ref("still"))
 
 
-SPECS = {"sod": _sod, "sine": _sine, "tube": _tube, "reactors": _reactors}
+SPECS = {
+    "sod": _sod,
+    "sine": _sine,
+    "tube": _tube,
+    "reactors": _reactors,
+    "sod_roe": lambda: _sod_scheme(2, 2),
+    "sod_ausm_nnd2": lambda: _sod_scheme(3, 3),
+    "sod_hllc_first": lambda: _sod_scheme(4, 1),
+    "sod_hybrid": _sod_hybrid,
+    "sine_visc8": _sine_visc8,
+    "channel_walls": _channel_walls,
+    "duct_inflow": _duct_inflow,
+    "back_pressure": _tube_back_pressure,
+    "duct_subsonic": _duct_subsonic_back_pressure,
+    "mixtube_roe": _mix_tube_roe,
+    "mixwave": lambda: _mix_wave(False),
+    "mixwave_reacting": lambda: _mix_wave(True),
+}
+
 
 
 def main():

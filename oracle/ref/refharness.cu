@@ -13,6 +13,9 @@
 //
 //   refharness <case dir> rk3 <steps>   SSP-RK3 steps   (src/RK.cuh:84-216)
 //   refharness <case dir> wu  <steps>   Wu splitting    (src/StrangSplitting.cu:683-861)
+//   refharness <case dir> visc 0        one compute_viscous_flux into a zeroed
+//        dq from the initialised state (src/ViscousScheme.cu:7-73): writes
+//        out/visc_dq.bin and the flux arrays out/visc_{f,g,h}.bin
 //   refharness <case dir> react <steps> <dt>
 //        reaction steps only: wu_reaction_step with Cn = 0 on every node
 //        (src/StrangSplitting.cu:373-421, constant-volume reactors)
@@ -256,6 +259,22 @@ template<MixtureModel M> struct Run {
     return dt;
   }
 
+  // One viscous-flux evaluation (compute_viscous_flux, src/ViscousScheme.cu:7-73)
+  // into a zeroed dq, from the initialised state: dq and the node/face flux
+  // arrays it leaves behind.
+  void viscous_once() {
+    cfd::DZone &z = zone();
+    const size_t nq = static_cast<size_t>(z.dq.size()) * n_var * sizeof(real);
+    const size_t nf = static_cast<size_t>(z.fFlux.size()) * n_var * sizeof(real);
+    cudaMemset(z.dq.data(), 0, nq);
+    cfd::compute_viscous_flux<M>(mesh, driver.field, driver.param, parameter);
+    check("compute_viscous_flux");
+    write_device("out/visc_dq.bin", z.dq.data(), nq);
+    write_device("out/visc_f.bin", z.fFlux.data(), nf);
+    write_device("out/visc_g.bin", z.gFlux.data(), nf);
+    write_device("out/visc_h.bin", z.hFlux.data(), nf);
+  }
+
   // Reaction only, Cn = 0: a batch of constant-volume reactors.
   real react_step(real dt) {
     cfd::DZone &z = zone();
@@ -274,6 +293,10 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
   r.dump_grid();
   r.dump_param();
   r.dump_state(0);
+  if (mode == "visc") {
+    r.viscous_once();
+    return 0;
+  }
   for (int s = 1; s <= steps; ++s) {
     real dt = 0;
     if (mode == "rk3")
@@ -293,13 +316,13 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
 
 int main(int argc, char *argv[]) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react <steps> [dt]\n");
+    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react|visc <steps> [dt]\n");
     return 2;
   }
   const std::string mode = argv[2];
   const int steps = std::atoi(argv[3]);
   const double react_dt = argc > 4 ? std::atof(argv[4]) : 0.0;
-  if (mode != "rk3" && mode != "wu" && mode != "react") {
+  if (mode != "rk3" && mode != "wu" && mode != "react" && mode != "visc") {
     std::fprintf(stderr, "refharness: unknown mode %s\n", mode.c_str());
     return 2;
   }

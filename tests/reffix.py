@@ -40,16 +40,17 @@ def generator():
     return _gen
 
 
-FIXTURES = {  # generator spec name -> fixture file
-    "sod": "ref_sod_400x7_weno5.npz",
-    "sine": "ref_sine_21_weno7_visc.npz",
-    "tube": "ref_tube_h2o2ar_wu.npz",
-    "reactors": "ref_reactors_li2004_1024.npz",
-}
+def names():
+    """The recorded runs, by the generator's spec key."""
+    return list(generator().SPECS)
+
+
+def fixture_path(name):
+    return os.path.join(GOLDEN, f"ref_{generator().SPECS[name]().name}.npz")
 
 
 def load(name):
-    with np.load(os.path.join(GOLDEN, FIXTURES[name])) as z:
+    with np.load(fixture_path(name)) as z:
         return {k: z[k] for k in z.files}
 
 

@@ -5,6 +5,7 @@ good nodes of their 3x3x3 neighbourhood, or their own values clamped to the
 limits when no neighbour is good; T follows from the state equation and cv
 from the new state.  Good and bad are judged on the state before the call."""
 import numpy as np
+import pytest
 
 import cases
 import pyoracle
@@ -93,3 +94,51 @@ def test_physical_state_is_left_alone():
     before = oz["bv"].copy(), oz["cv"].copy()
     assert oz.limit_flow(ll, ul) == 0
     assert np.array_equal(oz["bv"], before[0]) and np.array_equal(oz["cv"], before[1])
+
+
+def test_setup_reader_takes_limit_flow_and_its_bounds(tmp_path):
+    """limit_flow and the bounds the reference derives from its reference
+    state (src/DParameter.cu:333-349): rho 1e-6..1e3 rho_inf, velocity
+    +-1000 v_inf (the speed of sound when |v_inf| < 1), p 1e-6..1e3 p_inf."""
+    import ctypes
+
+    import corefl_b200
+
+    setup = tmp_path / "setup.txt"
+    setup.write_text("bool limit_flow = 1\nstring reference_state = free\n"
+                     "struct free {\n  string type = inflow\n  int label = 5\n  real density = 1.2\n"
+                     "  real velocity = 0.5\n  real pressure = 1e5\n}\n")
+    p = corefl_b200.cfk_param()
+    err = ctypes.create_string_buffer(256)
+    assert corefl_b200.lib().cfk_param_from_setup(str(setup).encode(), ctypes.byref(p), err, 256) == 0
+    assert p.limit_flow == 1
+    T = 1e5 * 28.9647 / (1.2 * 8314.462618)
+    c = (1.4 * 8314.462618 / 28.9647 * T) ** 0.5
+    assert list(p.limit_ll) == pytest.approx([1.2e-6, -1000 * c, -1000 * c, -1000 * c, 0.1], rel=1e-15)
+    assert list(p.limit_ul) == pytest.approx([1.2e3, 1000 * c, 1000 * c, 1000 * c, 1e8], rel=1e-15)
+    setup.write_text("int hardCodedMech = 1\n")
+    rc = corefl_b200.lib().cfk_param_from_setup(str(setup).encode(), ctypes.byref(p), err, 256)
+    assert rc != 0 and b"hardCodedMech" in err.value
+
+
+def test_oracle_rk3_step_applies_limit_flow():
+    """With limit_flow set, the oracle's stage loop repairs a density spike
+    above the bound in every stage: after one step no interior density
+    exceeds it, while the same step without limit_flow leaves it there."""
+    base = cases.sod(48, 7, scheme=52)
+    v = base.param["v_ref"]
+    ll, ul = [1e-6, -1000 * v, -1000 * v, -1000 * v, 1e-6], [2.0, 1000 * v, 1000 * v, 1000 * v, 1e3]
+    bv = base.bv.copy()
+    g = base.ngg
+    B = bv.reshape(6, base.mz + 2 * g, base.my + 2 * g, base.mx + 2 * g)
+    B[0, g, g + 3, g + 10] = 4.0
+    B[5] = B[4] / (B[0] * R_AIR)
+    out = {}
+    for on in (0, 1):
+        case = base.__class__(**{**base.__dict__, "bv": bv.copy(),
+                                 "param": dict(base.param, limit_flow=on, limit_ll=ll, limit_ul=ul)})
+        oz = pyoracle.OracleZone(case)
+        oz.initialize()
+        oz.step()
+        out[on] = case.interior(oz["bv"][0]).max()
+    assert out[1] <= 2.0 < out[0]

@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-@pytest.mark.parametrize("name", list(reffix.FIXTURES))
+@pytest.mark.parametrize("name", reffix.names())
 def test_library_replays_reference_run(name):
     reports = reffix.replay(reffix.GpuReplay(name))
     for r in reports:
