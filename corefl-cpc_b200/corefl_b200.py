@@ -186,6 +186,9 @@ def lib() -> ctypes.CDLL:
             "cfk_compute_cv_from_bv": (i, [vp, vp]),
             "cfk_apply_boundary_conditions": (i, [vp, vp]),
             "cfk_eliminate_k_gradient": (i, [vp, vp]),
+            "cfk_halo_size": (i, [vp, i, ctypes.POINTER(ctypes.c_longlong)]),
+            "cfk_halo_pack": (i, [vp, i, i, vp, vp]),
+            "cfk_halo_assign": (i, [vp, i, i, vp, vp]),
             "cfk_write_flowfield": (i, [ctypes.c_char_p, ctypes.POINTER(cfk_plt_block), i, i,
                                         ctypes.POINTER(ctypes.c_char_p), i, i, d, ctypes.c_char_p, ctypes.c_size_t]),
             "cfk_read_flowfield": (i, [ctypes.c_char_p, ctypes.POINTER(cfk_plt_target), i,
@@ -475,6 +478,18 @@ class Context:
 
     def eliminate_k_gradient(self, stream=None):
         self._ck(self.L.cfk_eliminate_k_gradient(self.h, stream), "eliminate_k_gradient")
+
+    def halo_size(self, face) -> int:
+        """cfk_halo_size: doubles in the halo buffer of a block face on axis `face`."""
+        n = ctypes.c_longlong()
+        self._ck(self.L.cfk_halo_size(self.h, face, ctypes.byref(n)), "halo_size")
+        return n.value
+
+    def halo_pack(self, face, direction, buf_ptr, stream=None):
+        self._ck(self.L.cfk_halo_pack(self.h, face, direction, buf_ptr, stream), "halo_pack")
+
+    def halo_assign(self, face, direction, buf_ptr, stream=None):
+        self._ck(self.L.cfk_halo_assign(self.h, face, direction, buf_ptr, stream), "halo_assign")
 
     def inner_communication(self, target: "Context", face: cfk_inner_face, stream=None):
         self._ck(self.L.cfk_inner_communication(self.h, target.h, ctypes.byref(face), stream), "inner_communication")

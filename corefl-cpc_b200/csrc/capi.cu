@@ -40,6 +40,10 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
                                        int n_face, const cfk_wall &wall, const cfk_inflow &inflow,
                                        const cfk_outflow &outflow, cudaStream_t st, int *n_launch);
 cudaError_t launch_finite_rate_chemistry(const Zone &z, const Mech *mc, cudaStream_t st);
+long long halo_doubles(const Dims &d, const Param &p, int face);
+cudaError_t launch_halo_pack(const Zone &z, const Param &p, int face, int direction, double *buf, cudaStream_t st);
+cudaError_t launch_halo_assign(const Zone &z, const Param &p, const Thermo *th, int face, int direction,
+                               const double *buf, cudaStream_t st);
 cudaError_t launch_eliminate_k_gradient(const Zone &z, const Param &p, cudaStream_t st);
 cudaError_t launch_inner_communication(const Zone &z, const Zone &tz, const Param &p, const Thermo *th,
                                        const cfk_inner_face &f, cudaStream_t st);
@@ -621,6 +625,40 @@ int cfk_limit_flow(cfk_ctx *c, long long *n_repaired, void *stream) {
     CFK_CHECK(c, cudaStreamSynchronize(st), "limit_flow sync");
     *n_repaired = (long long)v;
   }
+  return CFK_OK;
+}
+
+static int halo_face_ok(cfk_ctx *c, int face, int direction) {
+  if (face < 0 || face > 2 || (direction != -1 && direction != 1))
+    return fail(c, CFK_ERR_ARG, "face must be 0, 1 or 2 and direction -1 or +1");
+  if (face == 2 && c->z.d.mz == 1) return fail(c, CFK_ERR_ARG, "a 2-D block has no k faces to share");
+  return CFK_OK;
+}
+
+int cfk_halo_size(cfk_ctx *c, int face, long long *n_doubles) {
+  NEED_ZONE(c);
+  if (int r = halo_face_ok(c, face, -1)) return r;
+  if (!n_doubles) return fail(c, CFK_ERR_ARG, "n_doubles is NULL");
+  *n_doubles = halo_doubles(c->z.d, c->p, face);
+  return CFK_OK;
+}
+
+int cfk_halo_pack(cfk_ctx *c, int face, int direction, double *buf, void *stream) {
+  NEED_ZONE(c);
+  if (int r = halo_face_ok(c, face, direction)) return r;
+  if (!buf) return fail(c, CFK_ERR_ARG, "buf is NULL");
+  CFK_CHECK(c, launch_halo_pack(c->z, c->p, face, direction, buf, S(stream)), "halo pack");
+  c->launches += 1;
+  return CFK_OK;
+}
+
+int cfk_halo_assign(cfk_ctx *c, int face, int direction, const double *buf, void *stream) {
+  NEED_ZONE(c);
+  if (int r = halo_face_ok(c, face, direction)) return r;
+  if (int r = need_mech_for_mixture(c)) return r;
+  if (!buf) return fail(c, CFK_ERR_ARG, "buf is NULL");
+  CFK_CHECK(c, launch_halo_assign(c->z, c->p, thermo_of(c), face, direction, buf, S(stream)), "halo assign");
+  c->launches += 1;
   return CFK_OK;
 }
 

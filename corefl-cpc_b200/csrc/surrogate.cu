@@ -261,7 +261,10 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
     const int q = t * 128 + row;
     const bool valid = q < a.n_nodes;
     int64_t id = 0, iq = 0;
-    double T0 = 0, p0 = 0, Y0[kMaxSpec];
+    // Y0: composition the predicted change applies to; Te, qe: temperature and
+    // conserved variables it starts from (the node's own, or with the frozen
+    // transport term Cn the state that term alone reaches by the step's end)
+    double T0 = 0, p0 = 0, Y0[kMaxSpec], Te = 0, qe[5] = {0, 0, 0, 0, 0};
     int reason = valid ? 0 : -1;
     float x[kSgIn];
     if (valid) {
@@ -271,8 +274,43 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
       T0 = a.z.bv[id + 5 * szp];
       p0 = a.z.bv[id + 4 * szp];
       for (int l = 0; l < kMaxSpec; ++l) Y0[l] = l < ns ? a.z.sv[id + l * szp] : 0.0;
+#pragma unroll
+      for (int l = 0; l < 5; ++l) qe[l] = a.z.cv[id + l * szp];
+      Te = T0;
+      double Tf = T0, pf = p0, Yf[kMaxSpec];
+      for (int l = 0; l < kMaxSpec; ++l) Yf[l] = Y0[l];
+      if (a.z.Cn) {
+        // features at the mid-step state of the frozen transport, the change
+        // applied to its end-of-step state
+        double q0[5], rY0[kMaxSpec], cq[5], crY[kMaxSpec], qm[5];
+        const double s = a.dt / a.z.jac[id];
+#pragma unroll
+        for (int l = 0; l < 5; ++l) {
+          q0[l] = qe[l];
+          cq[l] = a.z.Cn[iq + l * szq] * s;
+        }
+        bool moved = false;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) moved |= cq[l] != 0.0;
+        for (int l = 0; l < ns; ++l) {
+          rY0[l] = a.z.cv[id + (5 + l) * szp];
+          crY[l] = a.z.Cn[iq + (5 + l) * szq] * s;
+          moved |= crY[l] != 0.0;
+        }
+        // a node the transport term leaves unchanged keeps its own state
+        if (moved) {
+          bool ok = sg_transported(th, ns, q0, rY0, cq, crY, 0.5, T0, qm, Yf, Tf, pf);
+          double pe = 0;
+          ok = ok && sg_transported(th, ns, q0, rY0, cq, crY, 1.0, Tf, qe, Y0, Te, pe);
+          if (!ok) {
+            reason = SG_NEWTON_FAILED;
+            Tf = T0;
+            pf = p0;
+          }
+        }
+      }
       double f[kSgIn];
-      sg_raw_features(T0, p0, Y0, ns, a.dt, f);
+      sg_raw_features(Tf, pf, Yf, ns, a.dt, f);
       bool ood = false;
       for (int c = 0; c < kSgIn; ++c) {
         const double dev = f[c] - (double)a.nrm.in_mean[c];
@@ -324,37 +362,18 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
       const bool projected = sg_project(a.proj, ns, Z0, Yn);
       double qv[5], rY[kMaxSpec];
 #pragma unroll
-      for (int l = 0; l < 5; ++l) qv[l] = a.z.cv[id + l * szp];
+      for (int l = 0; l < 5; ++l) qv[l] = qe[l];
       for (int l = 0; l < ns; ++l) rY[l] = qv[0] * Yn[l];
-      if (a.z.Cn) {
-        // transport source over the step, added after the reaction change
-        const double s = a.dt / a.z.jac[id];
-#pragma unroll
-        for (int l = 0; l < 5; ++l) qv[l] += a.z.Cn[iq + l * szq] * s;
-        double sum = 0;
-        for (int l = 0; l < ns; ++l) {
-          rY[l] += a.z.Cn[iq + (5 + l) * szq] * s;
-          if (rY[l] < 0) rY[l] = 0;
-          sum += rY[l];
-        }
-        // every partial density clipped: no composition to renormalise, so
-        // the node goes to the plain integrator instead of carrying 0/0
-        if (!(sum > 0)) reason = SG_NEWTON_FAILED;
-        for (int l = 0; l < ns; ++l) {
-          Yn[l] = sum > 0 ? rY[l] / sum : Y0[l];
-          rY[l] = Yn[l] * qv[0];
-        }
-      }
       const double rinv = 1.0 / qv[0];
       const double u = qv[1] * rinv, v = qv[2] * rinv, w = qv[3] * rinv;
-      double guess = T0 + rr[9];
-      guess = fmin(fmax(guess, fmax(T0 - 500.0, 200.0)), T0 + 3000.0);
+      double guess = Te + rr[9];
+      guess = fmin(fmax(guess, fmax(Te - 500.0, 200.0)), Te + 3000.0);
       Tn = guess;
       double pn = 0;
       const bool ok = projected && temperature_newton(th, ns, Yn, qv[4], qv[0], u * u + v * v + w * w, Tn, pn);
       if (!ok) reason = SG_NEWTON_FAILED;
-      else if (fabs(Tn - T0) > a.gate.dT_max) reason = SG_IGNITION;
-      else if (fabs(T0 + rr[9] - Tn) > a.gate.dT_consistency) reason = SG_CONSISTENCY;
+      else if (fabs(Tn - Te) > a.gate.dT_max) reason = SG_IGNITION;
+      else if (fabs(Te + rr[9] - Tn) > a.gate.dT_consistency) reason = SG_CONSISTENCY;
       judged = reason == 0 && a.gate.judge_stride > 0 &&
                ((unsigned)q + (unsigned)a.gate.judge_salt) % (unsigned)a.gate.judge_stride == 0;
       if (reason == 0 && !judged) {
@@ -437,16 +456,55 @@ __global__ void sg_judge_kernel(Zone z, int ns, const SgJudge *judge, const unsi
 // Training data: a snapshot of (T, p, Y) before a plain reaction step, then
 // the raw features and targets after it.
 // ---------------------------------------------------------------------------
-__global__ void sg_snapshot_kernel(Zone z, int ns, int n_nodes, double *snap) {
+// Training rows from the plain integrator.  Before its step: the state the
+// features are read at and the state the change applies to (sg_transported:
+// the node's own without a transport term, else the frozen transport term's
+// mid-step and end-of-step states), 21 doubles per node: T, p, Y[9] of the
+// first, T, Y[9] of the second.  After it: one row of raw features and
+// targets per node, the targets the changes from the second state.
+constexpr int kSnap = 21;
+
+__global__ void sg_snapshot_kernel(Zone z, const Thermo *th, int n_nodes, double dt, double *snap) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_nodes) return;
   const Dims d = z.d;
+  const int ns = th->n_spec;
   const int i = q % d.mx, r = q / d.mx, j = r % d.my, k = r / d.my;
   const int64_t id = d.idx(d.ngg, i, j, k), szp = d.plane(d.ngg);
-  double *s = snap + (int64_t)q * 11;
-  s[0] = z.bv[id + 5 * szp];
-  s[1] = z.bv[id + 4 * szp];
-  for (int l = 0; l < kMaxSpec; ++l) s[2 + l] = l < ns ? z.sv[id + l * szp] : 0.0;
+  double *s = snap + (int64_t)q * kSnap;
+  double T0 = z.bv[id + 5 * szp], p0 = z.bv[id + 4 * szp], Y0[kMaxSpec];
+  for (int l = 0; l < kMaxSpec; ++l) Y0[l] = l < ns ? z.sv[id + l * szp] : 0.0;
+  double Tf = T0, pf = p0, Yf[kMaxSpec], Te = T0, Ye[kMaxSpec];
+  for (int l = 0; l < kMaxSpec; ++l) Yf[l] = Ye[l] = Y0[l];
+  if (z.Cn) {
+    const int64_t iq = d.idx(0, i, j, k), szq = d.plane(0);
+    double q0[5], rY0[kMaxSpec], cq[5], crY[kMaxSpec], qt[5], pe = 0;
+    const double sc = dt / z.jac[id];
+    bool moved = false;
+    for (int l = 0; l < 5; ++l) {
+      q0[l] = z.cv[id + l * szp];
+      cq[l] = z.Cn[iq + l * szq] * sc;
+      moved |= cq[l] != 0.0;
+    }
+    for (int l = 0; l < ns; ++l) {
+      rY0[l] = z.cv[id + (5 + l) * szp];
+      crY[l] = z.Cn[iq + (5 + l) * szq] * sc;
+      moved |= crY[l] != 0.0;
+    }
+    if (moved && !(sg_transported(th, ns, q0, rY0, cq, crY, 0.5, T0, qt, Yf, Tf, pf) &&
+          sg_transported(th, ns, q0, rY0, cq, crY, 1.0, Tf, qt, Ye, Te, pe))) {
+      // no transported state: the row falls back to the node's own (a
+      // training sample of the reaction alone)
+      Tf = Te = T0;
+      pf = p0;
+      for (int l = 0; l < kMaxSpec; ++l) Yf[l] = Ye[l] = Y0[l];
+    }
+  }
+  s[0] = Tf;
+  s[1] = pf;
+  for (int l = 0; l < kMaxSpec; ++l) s[2 + l] = Yf[l];
+  s[11] = Te;
+  for (int l = 0; l < kMaxSpec; ++l) s[12 + l] = Ye[l];
 }
 
 __global__ void sg_record_kernel(Zone z, int ns, int n_nodes, const double *snap, double dt, float *X, float *G) {
@@ -455,14 +513,14 @@ __global__ void sg_record_kernel(Zone z, int ns, int n_nodes, const double *snap
   const Dims d = z.d;
   const int i = q % d.mx, r = q / d.mx, j = r % d.my, k = r / d.my;
   const int64_t id = d.idx(d.ngg, i, j, k), szp = d.plane(d.ngg);
-  const double *s = snap + (int64_t)q * 11;
+  const double *s = snap + (int64_t)q * kSnap;
   double f[kSgIn];
   sg_raw_features(s[0], s[1], s + 2, ns, dt, f);
   for (int c = 0; c < kSgIn; ++c) X[(int64_t)q * kSgIn + c] = (float)f[c];
   float *gq = G + (int64_t)q * kSgOut;
   for (int l = 0; l < kMaxSpec; ++l)
-    gq[l] = l < ns ? (float)(sg_boxcox(z.sv[id + l * szp]) - sg_boxcox(s[2 + l])) : 0.f;
-  gq[9] = (float)(z.bv[id + 5 * szp] - s[0]);
+    gq[l] = l < ns ? (float)(sg_boxcox(z.sv[id + l * szp]) - sg_boxcox(s[12 + l])) : 0.f;
+  gq[9] = (float)(z.bv[id + 5 * szp] - s[11]);
   gq[10] = (float)log(fmin(fmax(z.reaction_timeScale[id], 1e-20), 1e6));
 }
 
@@ -795,9 +853,9 @@ cudaError_t launch_sg_judge(const Zone &z, int ns, const SgJudge *judge, const u
   return cudaGetLastError();
 }
 
-cudaError_t launch_sg_snapshot(const Zone &z, int ns, double *snap, cudaStream_t st) {
+cudaError_t launch_sg_snapshot(const Zone &z, const Thermo *th, double dt, double *snap, cudaStream_t st) {
   const int n = z.d.mx * z.d.my * z.d.mz;
-  sg_snapshot_kernel<<<(n + 127) / 128, 128, 0, st>>>(z, ns, n, snap);
+  sg_snapshot_kernel<<<(n + 127) / 128, 128, 0, st>>>(z, th, n, dt, snap);
   return cudaGetLastError();
 }
 

@@ -110,6 +110,34 @@ __host__ __device__ inline void sg_raw_features(double T, double p, const double
   f[11] = log(dt);
 }
 
+// The state a node reaches when the frozen transport term of Wu's splitting
+// acts alone for the fraction f of the reaction step: conserved variables
+// q = q0 + f cq (cq = Cn dt / J over the whole step), partial densities
+// rY0 + f crY clipped at 0 and scaled to the new density, Y = rY / rho, and T,
+// p from the energy by the Newton iteration (T_guess to start).  Returns
+// false when no partial density is left or the iteration fails.  Inside a
+// flow the surrogate reads its features at f = 1/2 (the mid-step state the
+// frozen transport passes through) and applies its predicted change to the
+// f = 1 state; with Cn = 0 both are the node's own state.
+__device__ inline bool sg_transported(const Thermo *th, int ns, const double *q0, const double *rY0, const double *cq,
+                                      const double *crY, double f, double T_guess, double *q, double *Y, double &T,
+                                      double &p) {
+#pragma unroll
+  for (int l = 0; l < 5; ++l) q[l] = q0[l] + f * cq[l];
+  double sum = 0;
+  for (int l = 0; l < ns; ++l) {
+    Y[l] = fmax(rY0[l] + f * crY[l], 0.0);
+    sum += Y[l];
+  }
+  if (!(sum > 0) || !(q[0] > 0)) return false;
+  for (int l = 0; l < ns; ++l) Y[l] /= sum;
+  for (int l = ns; l < kMaxSpec; ++l) Y[l] = 0.0;
+  const double rinv = 1.0 / q[0];
+  const double u = q[1] * rinv, v = q[2] * rinv, w = q[3] * rinv;
+  T = T_guess;
+  return temperature_newton(th, ns, Y, q[4], q[0], u * u + v * v + w * w, T, p);
+}
+
 // Weighted least-squares projection of Y onto {mu Y = Z0, Y >= 0}: the
 // correction of species k is proportional to (Y_k + 1e-12), so trace species
 // move least; species driven negative are clipped to 0 and frozen, and the

@@ -20,7 +20,7 @@ cudaError_t launch_sg_step(const Zone &z, const Mech *mc, const uint8_t *w16, co
                            cudaStream_t st);
 cudaError_t launch_sg_judge(const Zone &z, int ns, const SgJudge *judge, const unsigned *judge_count,
                             const SgGate &gate, unsigned short *revert, SgCounters *cnt, int n_sm, cudaStream_t st);
-cudaError_t launch_sg_snapshot(const Zone &z, int ns, double *snap, cudaStream_t st);
+cudaError_t launch_sg_snapshot(const Zone &z, const Thermo *th, double dt, double *snap, cudaStream_t st);
 cudaError_t launch_sg_record(const Zone &z, int ns, const double *snap, double dt, float *X, float *G, cudaStream_t st);
 cudaError_t launch_sg_colstats(const float *X, const float *G, long long n, const float *scales, double *acc,
                                unsigned *mm, int n_sm, cudaStream_t st);
@@ -83,7 +83,7 @@ cudaError_t ensure_nodes(Surrogate *s, long long n) {
   if ((e = cudaMalloc(&s->judge, n * sizeof(SgJudge))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&s->revert, n * sizeof(unsigned short))) != cudaSuccess) return e;
   if ((e = cudaMemset(s->revert, 0, n * sizeof(unsigned short))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&s->snap, n * 11 * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&s->snap, n * 21 * sizeof(double))) != cudaSuccess) return e;
   s->cap = n;
   return cudaSuccess;
 }
@@ -155,10 +155,11 @@ int cfk_surrogate_record(cfk_ctx *c, int phase, double dt, float *X, float *G, v
   if (r) return r;
   Surrogate *s = c->sg;
   CFK_CHECK(c, ensure_nodes(s, zone_nodes(c)), "surrogate node buffers");
+  if (!(dt > 0)) return fail(c, CFK_ERR_ARG, "record needs dt > 0");
   if (phase == 0) {
-    CFK_CHECK(c, launch_sg_snapshot(c->z, c->hp.n_spec, s->snap, S(stream)), "surrogate snapshot");
+    CFK_CHECK(c, launch_sg_snapshot(c->z, &c->d_mech->th, dt, s->snap, S(stream)), "surrogate snapshot");
   } else if (phase == 1) {
-    if (!X || !G || !(dt > 0)) return fail(c, CFK_ERR_ARG, "record needs X, G and dt > 0");
+    if (!X || !G) return fail(c, CFK_ERR_ARG, "record needs X and G");
     CFK_CHECK(c, launch_sg_record(c->z, c->hp.n_spec, s->snap, dt, X, G, S(stream)), "surrogate record");
   } else {
     return fail(c, CFK_ERR_ARG, "phase must be 0 (before the step) or 1 (after it)");

@@ -50,3 +50,24 @@ def ignition_metrics(dt: float, T0: np.ndarray, T: np.ndarray):
     dT = np.diff(np.vstack([np.asarray(T0)[None, :], T]), axis=0)
     k = np.argmax(dT, axis=0)
     return (k + 0.5) * dt, T.max(axis=0), dT.max(axis=0)
+
+
+def record_flow(ctx: "cf.Context", n_nodes: int, steps: int, torch, every: int = 1, schedule: int = 1,
+                device: str = "cuda:0"):
+    """Run `steps` plain Wu-splitting steps of the bound flow zone and record
+    one (features, targets) row per node of the reaction sub-step for every
+    `every`-th step (cfk_wu_splitting_step_record: features at the frozen
+    transport term's mid-step state, targets from its end state).  Returns
+    device tensors X (rows, 12), G (rows, 11) and the step sizes."""
+    n_rec = (steps + every - 1) // every
+    X = torch.empty((n_rec * n_nodes, cf.SG_NIN), dtype=torch.float32, device=device)
+    G = torch.empty((n_rec * n_nodes, cf.SG_NOUT), dtype=torch.float32, device=device)
+    dts, r = [], 0
+    for s in range(steps):
+        if s % every == 0:
+            dts.append(ctx.wu_splitting_step_record(X[r * n_nodes].data_ptr(), G[r * n_nodes].data_ptr(), schedule))
+            r += 1
+        else:
+            dts.append(ctx.wu_splitting_step(schedule))
+    ctx.sync()
+    return X, G, np.array(dts)

@@ -235,6 +235,23 @@ int cfk_update_cv_and_bv_rk(cfk_ctx *ctx, double dt, int rk, void *stream);
  * per node; RK3 and Wu steps call it after each stage update when
  * limit_flow = 1. */
 int cfk_limit_flow(cfk_ctx *ctx, long long *n_repaired, void *stream);
+/* Halo of a block face shared with a block on another rank: the reference's
+ * parallel faces (src/Mesh.cpp:964-995, parallel_communication
+ * src/DataCommunication.cu:105-208).  face 0/1/2 and direction -1 (min
+ * side) / +1 (max side) name a whole block face over the block's own
+ * tangential nodes.  cfk_halo_pack replaces setup_data_to_be_sent (:270-307):
+ * it writes, per face node (first tangential axis fastest), the face node and
+ * the ngg nodes inside it, each as the 6 basic variables and the n_scalar
+ * scalars, into the device buffer buf of cfk_halo_size doubles.
+ * cfk_halo_assign replaces assign_data_received (:210-266): from the
+ * neighbour's packed buffer it averages the shared face nodes (copies theirs
+ * where ours has |V| > 1e-15 and theirs not; leaves ours where ours is at
+ * rest), fills the ngg ghost layers from the neighbour's inner layers and
+ * sets cv from bv there.  Moving the buffers between ranks is the caller's
+ * (NCCL, MPI, a peer copy); the face's own boundary condition is none. */
+int cfk_halo_size(cfk_ctx *ctx, int face, long long *n_doubles);
+int cfk_halo_pack(cfk_ctx *ctx, int face, int direction, double *buf, void *stream);
+int cfk_halo_assign(cfk_ctx *ctx, int face, int direction, const double *buf, void *stream);
 /* Replaces update_physical_properties<M> (reference src/FieldOperation.cuh:86-120). */
 int cfk_update_physical_properties(cfk_ctx *ctx, void *stream);
 /* Replaces compute_cv_from_bv<M> (reference src/FieldOperation.cuh:39-64). */

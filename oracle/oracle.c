@@ -1435,3 +1435,77 @@ double orc_rk3_step(orc_zone *z, const orc_param *p, double dt_fixed) {
   }
   return dt;
 }
+
+/* Halo of a block face shared with another rank's block: setup_data_to_be_sent
+ * and assign_data_received (src/DataCommunication.cu:210-307) over a whole
+ * block face (face 0/1/2, direction -1/+1), tangential nodes of the block
+ * only.  Buffer per face node t (first tangential axis fastest), layer q =
+ * 0..ngg (q-th node inwards), 6 basic variables then n_scalar scalars. */
+static void halo_geom(const orc_zone *z, int face, int direction, int *a, int *b, int *na, int *nb, int *f0) {
+  const int m[3] = {z->mx, z->my, z->mz};
+  *a = face == 0 ? 1 : 0;
+  *b = face == 2 ? 1 : 2;
+  *na = m[*a];
+  *nb = m[*b];
+  *f0 = direction < 0 ? 0 : m[face] - 1;
+}
+
+long orc_halo_size(const orc_zone *z, const orc_param *p, int face) {
+  int a, b, na, nb, f0;
+  halo_geom(z, face, -1, &a, &b, &na, &nb, &f0);
+  return (long)na * nb * (z->ngg + 1) * (6 + p->n_scalar);
+}
+
+void orc_halo_pack(const orc_zone *z, const orc_param *p, int face, int direction, double *buf) {
+  int a, b, na, nb, f0;
+  halo_geom(z, face, direction, &a, &b, &na, &nb, &f0);
+  const int g = z->ngg, nt = 6 + p->n_scalar;
+  const long sz = psz(z, g);
+  for (int t = 0; t < na * nb; ++t)
+    for (int q = 0; q <= g; ++q) {
+      int idx[3];
+      idx[a] = t % na;
+      idx[b] = t / na;
+      idx[face] = f0 - q * direction;
+      const long id = pidx(z, g, idx[0], idx[1], idx[2]);
+      double *o = buf + ((long)t * (g + 1) + q) * nt;
+      for (int l = 0; l < 6; ++l) o[l] = z->bv[id + l * sz];
+      for (int l = 0; l < p->n_scalar; ++l) o[6 + l] = z->sv[id + l * sz];
+    }
+}
+
+void orc_halo_assign(orc_zone *z, const orc_param *p, int face, int direction, const double *buf) {
+  int a, b, na, nb, f0;
+  halo_geom(z, face, direction, &a, &b, &na, &nb, &f0);
+  const int g = z->ngg, nt = 6 + p->n_scalar;
+  const long sz = psz(z, g);
+  for (int t = 0; t < na * nb; ++t) {
+    const double *in = buf + (long)t * (g + 1) * nt;
+    int idx[3];
+    idx[a] = t % na;
+    idx[b] = t / na;
+    idx[face] = f0;
+    long id = pidx(z, g, idx[0], idx[1], idx[2]);
+    const double *bv = z->bv;
+    const double u_this = sqrt(bv[id + sz] * bv[id + sz] + bv[id + 2 * sz] * bv[id + 2 * sz] +
+                               bv[id + 3 * sz] * bv[id + 3 * sz]);
+    if (fabs(u_this) > 1e-15) {
+      if (sqrt(in[1] * in[1] + in[2] * in[2] + in[3] * in[3]) < 1e-15) {
+        for (int l = 0; l < 6; ++l) z->bv[id + l * sz] = in[l];
+        for (int l = 0; l < p->n_scalar; ++l) z->sv[id + l * sz] = in[6 + l];
+      } else {
+        for (int l = 0; l < 6; ++l) z->bv[id + l * sz] = 0.5 * (z->bv[id + l * sz] + in[l]);
+        for (int l = 0; l < p->n_scalar; ++l) z->sv[id + l * sz] = 0.5 * (z->sv[id + l * sz] + in[6 + l]);
+      }
+      cv_from_bv_point(z, p, id);
+    }
+    for (int q = 1; q <= g; ++q) {
+      idx[face] = f0 + q * direction;
+      id = pidx(z, g, idx[0], idx[1], idx[2]);
+      const double *v = in + q * nt;
+      for (int l = 0; l < 6; ++l) z->bv[id + l * sz] = v[l];
+      for (int l = 0; l < p->n_scalar; ++l) z->sv[id + l * sz] = v[6 + l];
+      cv_from_bv_point(z, p, id);
+    }
+  }
+}

@@ -140,6 +140,10 @@ void orc_inner_communication(orc_zone *z, orc_zone *tz, const orc_param *p, cons
  * other threads may be rewriting; the two agree wherever no two bad nodes
  * are neighbours).  Returns the number of nodes repaired. */
 int orc_limit_flow(orc_zone *z, const orc_param *p, const double ll[5], const double ul[5]);
+/* halo of a block face shared with another rank's block (src/DataCommunication.cu:210-307) */
+long orc_halo_size(const orc_zone *z, const orc_param *p, int face);
+void orc_halo_pack(const orc_zone *z, const orc_param *p, int face, int direction, double *buf);
+void orc_halo_assign(orc_zone *z, const orc_param *p, int face, int direction, const double *buf);
 
 /* zone memory management (host, zero-filled) */
 int orc_zone_alloc(orc_zone *z, int mx, int my, int mz, int ngg, int n_var, int n_spec, int n_scalar);

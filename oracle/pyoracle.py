@@ -182,6 +182,12 @@ def lib() -> ctypes.CDLL:
         L.orc_inner_communication.restype = None
         L.orc_limit_flow.argtypes = [zp, pp, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_limit_flow.restype = ctypes.c_int
+        L.orc_halo_size.argtypes = [zp, pp, ctypes.c_int]
+        L.orc_halo_size.restype = ctypes.c_long
+        L.orc_halo_pack.argtypes = [zp, pp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        L.orc_halo_pack.restype = None
+        L.orc_halo_assign.argtypes = [zp, pp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        L.orc_halo_assign.restype = None
         _lib = L
     return _lib
 
@@ -270,6 +276,16 @@ class OracleZone:
         lo = np.ascontiguousarray(ll, dtype=np.float64)
         hi = np.ascontiguousarray(ul, dtype=np.float64)
         return self.L.orc_limit_flow(ctypes.byref(self.z), ctypes.byref(self.p), lo.ctypes.data, hi.ctypes.data)
+
+    def halo_pack(self, face, direction) -> np.ndarray:
+        """orc_halo_pack: the face's packed halo (float64 numpy array)."""
+        buf = np.empty(self.L.orc_halo_size(ctypes.byref(self.z), ctypes.byref(self.p), face))
+        self.L.orc_halo_pack(ctypes.byref(self.z), ctypes.byref(self.p), face, direction, buf.ctypes.data)
+        return buf
+
+    def halo_assign(self, face, direction, buf: np.ndarray):
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        self.L.orc_halo_assign(ctypes.byref(self.z), ctypes.byref(self.p), face, direction, buf.ctypes.data)
 
     def call(self, name, *args):
         return getattr(self.L, name)(ctypes.byref(self.z), ctypes.byref(self.p), *args)
