@@ -145,41 +145,63 @@ def _upload(ctx, zone, case):
     ctx.sync()
 
 
-def cpu_baseline_sample(scheme: int, reconstruction: int, target_s: float = 15.0, n: int = 49):
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_sample(scheme: int, reconstruction: int, steps: int = 3, warm: int = 1, n: int = N_NODES,
+                        case=None):
     """The oracle (the reference's algorithm restated in C, OpenMP on all host
-    threads) on a bounded sample of the workload: the same wave and settings
-    on an n^3 block, stepped until ~target_s of CPU work."""
+    threads, built with -march=native for this host) on the workload itself:
+    the n^3 wave (the benchmark block by default), `warm` untimed RK3 steps,
+    then `steps` steps each timed on its own; the value is the median
+    per-step rate (with the spread)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle  # test/baseline infrastructure only
 
-    case = cases.sine_wave(n=n, scheme=scheme, viscous=True, cfl=0.5, reconstruction=reconstruction)
+    native = pyoracle.use_native_build() if pyoracle._lib is None else pyoracle.LIB_PATH.endswith("_native/liboracle.so")
+    if case is None:
+        case = cases.sine_wave(n=n, scheme=scheme, viscous=True, cfl=0.5, reconstruction=reconstruction)
     z = pyoracle.OracleZone(case)
     z.initialize()
-    z.step()  # warm
-    steps, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < target_s:
+    for _ in range(warm):
         z.step()
-        steps += 1
-    el = time.perf_counter() - t0
-    return {"value": case.N * steps / el, "unit": UNIT, "cores": int(pyoracle.lib().orc_num_threads()),
-            "kind": "port", "sample": f"{n}^3-node block of the same wave, WENO7-ch + viscous, {steps} RK3 steps "
-                                      f"in {el:.1f} s", "steps": steps, "seconds": el}
+    per = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        z.step()
+        per.append(time.perf_counter() - t0)
+    rates = sorted(case.N / t for t in per)
+    med = float(np.median(rates))
+    del z
+    return {"value": med, "unit": UNIT, "cores": int(pyoracle.lib().orc_num_threads()), "kind": "port",
+            "sample": f"{case.mx}x{case.my}x{case.mz}-node block of the workload, WENO{scheme // 10 if scheme > 10 else ''}"
+                      f"{'-ch' if scheme > 10 else ''} + viscous, median of {steps} RK3 steps after {warm} untimed "
+                      f"(per-step rates {rates[0]:.3e}..{rates[-1]:.3e}); {'-march=native' if native else 'portable x86-64-v3'} "
+                      f"build on {_cpu_model()}",
+            "steps": steps, "seconds": float(sum(per)), "spread": [rates[0], rates[-1]], "cpu": _cpu_model()}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    # bounded sample per step, sized so that the whole run stays within minutes
-    total = max(args.steps + args.warmup, 1)
-    per = max(3.0, min(20.0, 150.0 / total))
-    res = cpu_baseline_sample(args.scheme, args.reconstruction, target_s=per * args.steps)
+    # each timed step is one RK3 step of the full workload on the host
+    res = cpu_baseline_sample(args.scheme, args.reconstruction, steps=max(args.steps, 1),
+                              warm=min(max(args.warmup, 0), 1), n=args.n)
     line = {
         "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / max(res["steps"], 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": "3-D viscous sine wave, curvilinear periodic block, WENO7-ch + 2nd-order viscous, "
-                               "SSP-RK3 CFL 0.5", "nodes": f"{N_NODES}^3 (sampled on the host: 49^3)"},
+                               "SSP-RK3 CFL 0.5", "nodes": f"{args.n}^3"},
         "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -383,13 +405,242 @@ def surrogate_bench(args, local):
     return out
 
 
+def _flow_ctx(mech, case, local, seed):
+    """A context holding the flow block `case` (mixture, reacting), with the
+    start-of-run sequence applied and the surrogate initialised."""
+    import corefl_b200 as cfk
+    param = dict(case.param)
+    param["device"] = local
+    ctx = cfk.Context(param, case.faces)
+    zone = ctx.alloc_zone(case.mx, case.my, case.mz)
+    ctx.set_mechanism(mech)
+    for fld, arr in (("bv", case.bv), ("sv", case.sv), ("jac", case.jac), ("metric", case.metric)):
+        a = np.ascontiguousarray(arr)
+        ctx.h2d(getattr(zone, fld), a.ctypes.data, a.nbytes)
+    ctx.properties()
+    ctx.boundary_conditions()
+    ctx.properties()
+    ctx.cv_from_bv()
+    ctx.surrogate_init(seed, mech.element_mass_fractions())
+    ctx.sync()
+    return ctx, zone
+
+
+def _interior_plane(ctx, zone, case, field, l):
+    """Plane l of a padded zone array, interior nodes, as a host array."""
+    a = np.empty(case.P)
+    ctx.d2h(a.ctypes.data, getattr(zone, field) + l * case.P * 8, case.P * 8)
+    return case.interior(a)
+
+
+def surrogate_flow_bench(args, local):
+    """The chemistry surrogate inside the reacting flow step (Wu's splitting
+    with the reaction sub-step replaced by the gated network), on reflected-
+    shock tubes of stoichiometric H2-O2 with 70 % Ar (PREMIX 9 species / 19
+    reactions, WENO5-ch + mixture-averaged viscous fluxes, adiabatic walls).
+
+    1. ignition window (a small tube, Mach 2.6, reflected state ~1400 K): the
+       plain run through ignition records one row per node per step
+       (cfk_wu_splitting_step_record); the network is trained on the rows; the
+       gated surrogate run repeats the window; ignition delay (largest rise of
+       the domain's peak T) and peak T of both, fraction of node-steps on the
+       network, whole-window device time of each.
+    2. the 2048 x 512 tube (wall-normal stretching 1.02, Mach 2.2 incident
+       shock into 0.1 atm / 300 K): K plain and K gated surrogate steps from the
+       same start with the network of 1.; reacting cell-updates/s of each
+       (cells x steps / device time), the reaction sub-step's share, the
+       fallback fraction, and the mean T and Y_OH differences after K steps."""
+    import torch
+    import mechanism
+    import surrogate as sg
+
+    mech = mechanism.load("premix_h2_ar")
+    dev = f"cuda:{local}"
+    out = {"mechanism": "PREMIX H2/O2/Ar 9s/19r", "dtype": "bf16 network, fp32 accumulate; fp64 rest"}
+    # 1. ignition window
+    nx, ny, W = args.sflow_ign_nx, args.sflow_ign_ny, args.sflow_ign_steps
+    small = cases.reflected_shock_tube(mech, nx, ny, length=0.02, height=0.004, mach=2.6)
+    n = small.N
+    traces, rows = {}, None
+    for mode in ("plain", "surrogate"):
+        ctx, zone = _flow_ctx(mech, small, local, 7)
+        if mode == "plain":
+            X = torch.empty((W * n, sg.cf.SG_NIN), dtype=torch.float32, device=dev)
+            G = torch.empty((W * n, sg.cf.SG_NOUT), dtype=torch.float32, device=dev)
+        else:
+            ctx.surrogate_set_params(weights, norm)
+            gate = ctx.surrogate_default_gate()
+        Tpad = torch.empty(small.P, dtype=torch.float64, device=dev)
+        Tint = Tpad.view(small.shape())[small.ngg:small.ngg + 1, small.ngg:small.ngg + ny, small.ngg:small.ngg + nx]
+        peak = torch.empty(W, dtype=torch.float64, device=dev)
+        t, now, stats = [], 0.0, []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for s_ in range(W):
+            if mode == "plain":
+                dt = ctx.wu_splitting_step_record(X[s_ * n].data_ptr(), G[s_ * n].data_ptr())
+            else:
+                dt, st = ctx.wu_splitting_step_surrogate(gate, s_, want_stats=(s_ % 20 == 19))
+                if st:
+                    stats.append(st)
+            now += dt
+            t.append(now)
+            ctx.d2d(Tpad.data_ptr(), zone.bv + 5 * small.P * 8, small.P * 8)
+            peak[s_] = Tint.max()
+        e1.record()
+        torch.cuda.synchronize()
+        traces[mode] = (np.array(t), peak.cpu().numpy(), e0.elapsed_time(e1), stats)
+        if mode == "plain":
+            t0 = time.time()
+            losses = sg.fit(ctx, X, G, epochs=args.sflow_epochs, batch=8192, lr0=2e-3, lr1=1e-5, seed=3)
+            torch.cuda.synchronize()
+            weights, norm = ctx.surrogate_get_params()
+            out["training"] = {"rows": W * n, "epochs": args.sflow_epochs, "train_s": time.time() - t0,
+                               "loss_first": losses[0], "loss_last": losses[-1]}
+            del X, G
+        ctx.close()
+
+    def ignition(tr):
+        tt, pk = tr[0], tr[1]
+        rise = np.diff(np.concatenate([[pk[0]], pk]))
+        k = int(np.argmax(rise))
+        return 0.5 * (tt[k] + (tt[k - 1] if k else 0.0)), float(pk.max())
+
+    tau_p, pk_p = ignition(traces["plain"])
+    tau_s, pk_s = ignition(traces["surrogate"])
+    st = traces["surrogate"][3]
+    out["ignition_window"] = {
+        "case": f"{nx}x{ny} tube 0.02 x 0.004 m, Mach 2.6 incident shock into 0.1 atm / 300 K, {W} steps "
+                f"({traces['plain'][0][-1] * 1e6:.1f} us)",
+        "tau_ign_plain_s": tau_p, "tau_ign_surrogate_s": tau_s, "tau_ign_rel_err": abs(tau_s - tau_p) / tau_p,
+        "T_peak_plain_K": pk_p, "T_peak_surrogate_K": pk_s, "T_peak_rel_err": abs(pk_s - pk_p) / pk_p,
+        "on_network": sum(x["surrogate"] for x in st) / max(sum(x["cells"] for x in st), 1),
+        "plain_window_ms": traces["plain"][2], "surrogate_window_ms": traces["surrogate"][2],
+        "note": "the plain window includes recording the training rows"}
+
+    # 2. the 2048 x 512 tube
+    big = cases.reflected_shock_tube(mech, args.sflow_nx, args.sflow_ny)
+    K = args.sflow_steps
+    r = _plain_vs_surrogate(mech, big, local, weights, norm, K)
+    r["case"] = (f"{big.mx}x{big.my} tube 0.1 x 0.025 m, wall-normal stretching 1.02, Mach 2.2 incident shock "
+                 f"into 0.1 atm / 300 K, {K} steps ({r['plain']['simulated_s'] * 1e9:.1f} ns simulated)")
+    out["tube_2048x512"] = r
+    return out
+
+
+def _plain_vs_surrogate(mech, case, local, weights, norm, K, modes=("plain", "surrogate")):
+    """K Wu-splitting steps of `case` from its initial state with the plain
+    point-implicit reaction sub-step and with the gated surrogate (and, with
+    "rk3" in modes, K RK3 steps with the explicit chemical source replayed as
+    a CUDA graph), each after two untimed steps from a fresh context; device
+    time by CUDA events, phase times by the library's profiling; the mean T
+    and Y_OH differences of the surrogate run against the plain one."""
+    import torch
+
+    res, finals = {}, {}
+    oh = mech.index("OH")
+    for mode in modes:
+        for timed in (False, True):
+            ctx, zone = _flow_ctx(mech, case, local, 7)
+            ctx.surrogate_set_params(weights, norm)
+            gate = ctx.surrogate_default_gate()
+            n = K if timed else 2
+            if timed:
+                ctx.set_profiling(mode != "rk3")
+                ctx.profile_read()
+            stats, now = [], 0.0
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            launches0 = ctx.kernel_launches
+            e0.record()
+            for s_ in range(n):
+                if mode == "plain":
+                    now += ctx.wu_splitting_step()
+                elif mode == "rk3":
+                    now += ctx.rk3_step(graph=True)
+                else:
+                    dt, st_ = ctx.wu_splitting_step_surrogate(gate, s_, want_stats=timed and s_ % 5 == 4)
+                    now += dt
+                    if st_:
+                        stats.append(st_)
+            e1.record()
+            torch.cuda.synchronize()
+            if not timed:
+                ctx.close()
+                continue
+            ms = e0.elapsed_time(e1)
+            r = {"cell_updates_per_s": case.N * K / (ms * 1e-3), "ms_per_step": ms / K, "simulated_s": now,
+                 "gpu_launches": ctx.kernel_launches - launches0}
+            if mode != "rk3":
+                ph = ctx.profile_read()
+                r["reaction_ms_per_step"] = ph["reaction"][0] / K
+                r["phases_ms_per_step"] = {k: v[0] / K for k, v in ph.items()}
+            if stats:
+                r["on_network"] = sum(x["surrogate"] for x in stats) / sum(x["cells"] for x in stats)
+                r["fallback_fraction"] = 1.0 - r["on_network"]
+            res[mode] = r
+            finals[mode] = (_interior_plane(ctx, zone, case, "bv", 5), _interior_plane(ctx, zone, case, "sv", oh))
+            ctx.close()
+    Tp, OHp = finals["plain"]
+    Ts, OHs = finals["surrogate"]
+    out = dict(res)
+    out.update({
+        "speedup_step": res["surrogate"]["cell_updates_per_s"] / res["plain"]["cell_updates_per_s"],
+        "speedup_reaction": res["plain"]["reaction_ms_per_step"] / max(res["surrogate"]["reaction_ms_per_step"], 1e-9),
+        "mean_T_rel_err": float(abs(Ts.mean() - Tp.mean()) / Tp.mean()),
+        "max_T_abs_err_K": float(np.abs(Ts - Tp).max()),
+        "mean_Y_OH_abs_err": float(np.abs(OHs - OHp).mean()), "max_Y_OH_plain": float(OHp.max())})
+    return out
+
+
+def mixing_layer_bench(args, local):
+    """The reacting H2/air mixing layer (cases.mixing_layer: air over H2/N2,
+    600 K, 1 atm, velocity ratio 1.5, convective Mach 0.2, tanh profile with
+    delta_omega 0.5 mm, 1 % white noise at the inflow, WENO7 characteristic +
+    mixture-averaged viscous fluxes, Li-2004 9 species / 19 reactions, span
+    periodic).  The network is trained on rows recorded from plain
+    Wu-splitting steps of a small block of the same layer; then the
+    nx x ny x nz block runs K steps each of plain Wu splitting, Wu splitting
+    with the gated surrogate, and RK3 with the explicit chemical source as a
+    CUDA graph: reacting cell-updates/s, fallback fraction, and the mean T
+    and Y_OH differences of the surrogate run against the plain run."""
+    import torch
+    import mechanism
+    import surrogate as sg
+
+    mech = mechanism.load("li2004")
+    dev = f"cuda:{local}"
+    small = cases.mixing_layer(mech, 64, 32, 16)
+    W, n = args.ml_train_steps, small.N
+    ctx, _ = _flow_ctx(mech, small, local, 9)
+    X = torch.empty((W * n, sg.cf.SG_NIN), dtype=torch.float32, device=dev)
+    G = torch.empty((W * n, sg.cf.SG_NOUT), dtype=torch.float32, device=dev)
+    for s_ in range(W):
+        ctx.wu_splitting_step_record(X[s_ * n].data_ptr(), G[s_ * n].data_ptr())
+    t0 = time.time()
+    losses = sg.fit(ctx, X, G, epochs=args.sflow_epochs, batch=8192, lr0=2e-3, lr1=1e-5, seed=3)
+    torch.cuda.synchronize()
+    weights, norm = ctx.surrogate_get_params()
+    ctx.close()
+    del X, G
+    big = cases.mixing_layer(mech, args.ml_nx, args.ml_ny, args.ml_nz)
+    K = args.ml_steps
+    r = _plain_vs_surrogate(mech, big, local, weights, norm, K, modes=("plain", "surrogate", "rk3"))
+    r["case"] = (f"{big.mx}x{big.my}x{big.mz} mixing layer 0.05 x 0.025 x 0.0125 m (y clustered), {K} steps "
+                 f"({r['plain']['simulated_s'] * 1e9:.1f} ns simulated)")
+    r["training"] = {"case": f"{small.mx}x{small.my}x{small.mz}", "rows": W * n, "epochs": args.sflow_epochs,
+                     "train_s": time.time() - t0, "loss_first": losses[0], "loss_last": losses[-1]}
+    return r
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N_NODES, help="nodes per direction (default 257)")
+    ap.add_argument("--n", "--block-n", dest="n", type=int, default=N_NODES, help="nodes per direction (default 257)")
     ap.add_argument("--scheme", type=int, default=72,
                     help="inviscid_scheme: 72/52 WENO7/5 characteristic (default 72), 1 LF, 2 Roe, 3 AUSM+, 4 HLLC")
     ap.add_argument("--reconstruction", type=int, default=2, help="for schemes 1-4: 1 first order, 2 MUSCL, 3 NND2")
@@ -405,6 +656,22 @@ def main():
     ap.add_argument("--surrogate-train-cells", type=int, default=16384)
     ap.add_argument("--surrogate-accuracy-cells", type=int, default=2048)
     ap.add_argument("--surrogate-epochs", type=int, default=200)
+    ap.add_argument("--no-surrogate-flow", action="store_true")
+    ap.add_argument("--surrogate-flow-only", action="store_true", help="only the surrogate-in-the-flow measurement")
+    ap.add_argument("--sflow-nx", type=int, default=2048)
+    ap.add_argument("--sflow-ny", type=int, default=512)
+    ap.add_argument("--sflow-steps", type=int, default=100, help="timed Wu steps of the 2048x512 tube per mode")
+    ap.add_argument("--sflow-ign-nx", type=int, default=128)
+    ap.add_argument("--sflow-ign-ny", type=int, default=16)
+    ap.add_argument("--sflow-ign-steps", type=int, default=600)
+    ap.add_argument("--sflow-epochs", type=int, default=30)
+    ap.add_argument("--no-mixing-layer", action="store_true")
+    ap.add_argument("--mixing-layer-only", action="store_true", help="only the reacting mixing-layer measurement")
+    ap.add_argument("--ml-nx", type=int, default=512)
+    ap.add_argument("--ml-ny", type=int, default=256)
+    ap.add_argument("--ml-nz", type=int, default=128)
+    ap.add_argument("--ml-steps", type=int, default=10, help="timed steps of the mixing layer per mode")
+    ap.add_argument("--ml-train-steps", type=int, default=100)
     args = ap.parse_args()
     rank, world, local = _env_rank()
     args.warmup = max(args.warmup, 3)
@@ -425,6 +692,14 @@ def main():
     if args.surrogate_only:
         torch.cuda.set_device(local)
         print(json.dumps({"surrogate": surrogate_bench(args, local)}), flush=True)
+        return
+    if args.surrogate_flow_only:
+        torch.cuda.set_device(local)
+        print(json.dumps({"surrogate_flow": surrogate_flow_bench(args, local)}), flush=True)
+        return
+    if args.mixing_layer_only:
+        torch.cuda.set_device(local)
+        print(json.dumps({"mixing_layer": mixing_layer_bench(args, local)}), flush=True)
         return
 
     dist = None
@@ -578,11 +853,15 @@ def main():
     reacting = None if args.no_reacting else reacting_bench(args, local, world, dist)
     # the surrogate measurement runs on rank 0 only (its window is one GPU's work)
     surrogate = None if (args.no_surrogate or args.no_reacting or rank != 0) else surrogate_bench(args, local)
+    surrogate_flow = (None if (args.no_surrogate_flow or args.no_reacting or rank != 0)
+                      else surrogate_flow_bench(args, local))
+    mixing_layer = (None if (args.no_mixing_layer or args.no_reacting or rank != 0)
+                    else mixing_layer_bench(args, local))
 
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample(args.scheme, args.reconstruction)
+            cpu = cpu_baseline_sample(args.scheme, args.reconstruction, case=case)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -604,6 +883,8 @@ def main():
             "clocks": clk.summary(),
             "reacting": reacting,
             "surrogate": surrogate,
+            "surrogate_flow": surrogate_flow,
+            "mixing_layer": mixing_layer,
         }
         print(json.dumps(line), flush=True)
     if dist:

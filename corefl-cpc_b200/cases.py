@@ -42,6 +42,7 @@ class Case:
     x: np.ndarray | None = None  # (P,) node x, for checks against exact solutions
     mech: object = None  # mechanism.Mechanism for the mixture model
     xyz: tuple | None = None  # interior node coordinates (x, y, z), each [k, j, i]
+    y: np.ndarray | None = None  # (P,) padded node y (DZone::y), for the mixing-layer inflow
 
     @property
     def P(self) -> int:
@@ -733,3 +734,94 @@ def reflected_shock_tube(mech, nx: int = 2048, ny: int = 512, length: float = 0.
     faces = [(0, -1, 6), (0, 1, 2), (1, -1, 2), (1, 1, 3)]
     return Case("reflected_shock_tube", nx, ny, 1, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=mech,
                 xyz=(x, y, z))
+
+
+def mixing_layer_streams(mech, upper: dict, lower: dict, ma_c: float, velocity_ratio: float,
+                         upper_faster: bool = True):
+    """The two streams of a mixing layer from the convective Mach number and
+    the velocity ratio, as get_mixing_layer_info computes them (reference
+    src/MixingLayer.cu:9-119, mixture branch): each stream's density and
+    frozen sound speed from (T, p, Y); u_slow = Ma_c (c_upper + c_lower) /
+    (r - 1), u_fast = r u_slow for r > 1 (u_fast = Ma_c (c_upper + c_lower) /
+    (1 - r), u_slow = r u_fast otherwise), the faster stream above y = 0 when
+    upper_faster.  Streams are dicts with T [K], p [Pa] and Y (mass fractions
+    by species name); returns dicts with rho, u, p, T and the Y vector."""
+    out = []
+    for st in (upper, lower):
+        Y = np.zeros(mech.n_spec)
+        for k, v in st["Y"].items():
+            Y[mech.index(k)] = v
+        imw = float(np.sum(Y / mech.mw))
+        cp = mixture_cp(mech, st["T"], Y)
+        R = R_U * imw
+        gamma = cp / (cp - R)
+        out.append(dict(rho=st["p"] / (R * st["T"]), c=math.sqrt(gamma * R * st["T"]), p=st["p"], T=st["T"], Y=Y))
+    up, lo = out
+    if velocity_ratio > 1:
+        u_slow = ma_c * (up["c"] + lo["c"]) / (velocity_ratio - 1)
+        u_fast = velocity_ratio * u_slow
+    else:
+        u_fast = ma_c * (up["c"] + lo["c"]) / (1 - velocity_ratio)
+        u_slow = u_fast * velocity_ratio
+    ma_up, ma_lo = (u_fast / up["c"], u_slow / lo["c"]) if upper_faster else (u_slow / up["c"], u_fast / lo["c"])
+    up["u"], lo["u"] = ma_up * up["c"], ma_lo * lo["c"]
+    return up, lo
+
+
+def mixing_layer(mech, nx: int = 512, ny: int = 256, nz: int = 128, length: float = 0.05, height: float = 0.025,
+                 span: float = 0.0125, delta_omega: float = 5e-4, ma_c: float = 0.2, velocity_ratio: float = 1.5,
+                 T0: float = 600.0, p0: float = 101325.0, fluctuation: float = 0.01, seed: int = 2026,
+                 cluster: float = 3.0, scheme: int = 72, viscous_order: int = 2, reacting: bool = True) -> Case:
+    """Spatially developing H2/air mixing layer: air above y = 0 (the faster
+    stream) and H2/N2 (1 : 1 by mole) below, both at T0 and p0, with the
+    velocity ratio and convective Mach number of mixing_layer_streams; the
+    initial field is the reference's tanh profile u(y) = (u1 + u2)/2 +
+    (u1 - u2)/2 tanh(2 y / delta_omega) with every other variable from the
+    stream on its side (reference src/Initialize.cu, initialize_mixing_layer).
+    Curvilinear block of nx x ny x nz nodes on [0, length] x [-height/2,
+    height/2] x [0, span], clustered towards y = 0 by y = (height/2) sinh(c
+    eta) / sinh(c) (eta in [-1, 1]).  Faces: x = 0 the mixing-layer inflow
+    with white noise of relative intensity `fluctuation` on u, v, w (seeded),
+    x = length and both y faces outflow, z periodic.  WENO7 characteristic
+    with mixture-averaged viscous fluxes; `reacting` keeps the reactions."""
+    m = mech if reacting else without_reactions(mech)
+    X_fuel = np.zeros(m.n_spec)
+    X_fuel[m.index("H2")], X_fuel[m.index("N2")] = 0.5, 0.5
+    X_air = np.zeros(m.n_spec)
+    X_air[m.index("O2")], X_air[m.index("N2")] = 0.21, 0.79
+    Yf, Ya = mole_to_mass(m, X_fuel), mole_to_mass(m, X_air)
+    names = m.species
+    up, lo = mixing_layer_streams(m, dict(T=T0, p=p0, Y={names[l]: Ya[l] for l in range(m.n_spec) if Ya[l] > 0}),
+                                  dict(T=T0, p=p0, Y={names[l]: Yf[l] for l in range(m.n_spec) if Yf[l] > 0}),
+                                  ma_c, velocity_ratio)
+    ngg = ghost_layers(scheme, viscous_order)
+    xs = np.linspace(0.0, length, nx)
+    eta = np.linspace(-1.0, 1.0, ny)
+    ys = 0.5 * height * np.sinh(cluster * eta) / np.sinh(cluster)
+    zs = np.linspace(0.0, span, nz)
+    Z3, Y3, X3 = np.meshgrid(zs, ys, xs, indexing="ij")
+    x, y, z = X3.copy(), Y3.copy(), Z3.copy()
+    jac, metric, xg = metrics(x, y, z, ngg)
+    _, Yg, _ = ghost_grid(x, y, z, ngg)
+    yg = Yg[1:-1, 1:-1, 1:-1].reshape(-1).copy()
+    P = jac.size
+    above = yg >= 0
+    bv = np.zeros((6, P))
+    bv[1] = 0.5 * (up["u"] + lo["u"]) + 0.5 * (up["u"] - lo["u"]) * np.tanh(2 * yg / delta_omega)
+    for l, key in ((0, "rho"), (4, "p"), (5, "T")):
+        bv[l] = np.where(above, up[key], lo[key])
+    sv = np.where(above[None, :], up["Y"][:, None], lo["Y"][:, None])
+    rho_ref, v_ref = _mix_reference(up["rho"], up["u"], up["p"])
+    param = _mix_param(m, dim=3, inviscid_scheme=scheme, reconstruction=2, cfl=0.5, viscous_order=viscous_order,
+                       weno_eps_scale=(rho_ref * v_ref) ** 2, v_ref=v_ref, rho_ref=rho_ref, n_reac=m.n_reac,
+                       inflow_type=2, inflow_density=up["rho"], inflow_u=up["u"], inflow_v=0.0, inflow_w=0.0,
+                       inflow_pressure=up["p"], inflow_temperature=up["T"],
+                       inflow_mw=1.0 / float(np.sum(up["Y"] / m.mw)), inflow_sv=list(up["Y"]),
+                       inflow_density_lower=lo["rho"], inflow_u_lower=lo["u"], inflow_v_lower=0.0,
+                       inflow_w_lower=0.0, inflow_p_lower=lo["p"], inflow_t_lower=lo["T"],
+                       inflow_sv_lower=list(lo["Y"]), inflow_delta_omega=delta_omega,
+                       inflow_fluctuation_type=1 if fluctuation > 0 else 0, inflow_fluctuation_intensity=fluctuation,
+                       inflow_seed=seed)
+    faces = [(0, -1, 5), (0, 1, 6), (1, -1, 6), (1, 1, 6), (2, -1, 8), (2, 1, 8)]
+    return Case("mixing_layer", nx, ny, nz, ngg, metric, jac, bv, sv, param, faces, x=xg, mech=m, xyz=(x, y, z),
+                y=yg)

@@ -44,7 +44,11 @@ class cfk_plt_target(ctypes.Structure):
 
 class cfk_inflow(ctypes.Structure):
     _fields_ = [("subsonic", ctypes.c_int)] + [(n, ctypes.c_double) for n in (
-        "density", "u", "v", "w", "pressure", "temperature", "mw")] + [("sv", ctypes.c_double * 9)]
+        "density", "u", "v", "w", "pressure", "temperature", "mw")] + [("sv", ctypes.c_double * 9)] + [
+        ("inflow_type", ctypes.c_int)] + [(n, ctypes.c_double) for n in (
+            "density_lower", "u_lower", "v_lower", "w_lower", "p_lower", "t_lower")] + [
+        ("sv_lower", ctypes.c_double * 9), ("delta_omega", ctypes.c_double), ("fluctuation_type", ctypes.c_int),
+        ("fluctuation_intensity", ctypes.c_double), ("seed", ctypes.c_ulonglong)]
 
 
 class cfk_outflow(ctypes.Structure):
@@ -134,7 +138,7 @@ class cfk_zone(ctypes.Structure):
     _fields_ = [("mx", ctypes.c_int), ("my", ctypes.c_int), ("mz", ctypes.c_int), ("ngg", ctypes.c_int)] + [
         (n, ctypes.c_void_p) for n in ("jac", "metric", "cv", "bv", "sv", "qn", "mul", "mach", "acoustic_speed",
                                        "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
-                                       "dt_local", "Cn", "shock_sensor")
+                                       "dt_local", "Cn", "shock_sensor", "y")
     ]
 
 
@@ -311,9 +315,10 @@ def make_param(p: dict, faces) -> cfk_param:
         if k == "wall_yk":
             for l, y in enumerate(v):
                 cp.wall.yk[l] = y
-        elif k == "inflow_sv":
+        elif k in ("inflow_sv", "inflow_sv_lower"):
+            arr = getattr(cp.inflow, k[7:])
             for l, y in enumerate(v):
-                cp.inflow.sv[l] = y
+                arr[l] = y
         elif k.startswith("wall_"):
             setattr(cp.wall, k[5:], v)
         elif k.startswith("inflow_"):
@@ -557,7 +562,7 @@ class Context:
         return {name: (ms[k], kn[k]) for k, name in enumerate(PHASES)}
 
 
-PHASES = ("inviscid", "viscous", "update", "bc", "properties", "dt")
+PHASES = ("inviscid", "viscous", "update", "bc", "properties", "dt", "reaction")
 NPHASE = len(PHASES)
 
 

@@ -60,7 +60,8 @@ using namespace cfk_detail;
 
 namespace {
 const char *const kPhaseName[CFK_NPHASE] = {"cfk inviscid flux", "cfk viscous flux", "cfk update",
-                                            "cfk boundary conditions", "cfk properties", "cfk time step"};
+                                            "cfk boundary conditions", "cfk properties", "cfk time step",
+                                            "cfk reaction"};
 
 // One phase of a step: an NVTX range named after it (visible to Nsight
 // Systems; inert when no tool is attached) and, with profiling on, CUDA
@@ -192,6 +193,19 @@ int validate(const cfk_param *p, std::string &why) {
       if (!(q.density > 0) || !(q.pressure > 0) || !(q.temperature > 0) || (p->n_spec > 0 && !(q.mw > 0)) ||
           (q.subsonic != 0 && q.subsonic != 1)) {
         why = "inflow needs density, pressure, temperature (and mw for mixtures) > 0 and subsonic 0 or 1";
+        return -1;
+      }
+      if (q.inflow_type != 0 && q.inflow_type != 2) {
+        why = "inflow_type must be 0 (constant) or 2 (mixing layer); profile inflows are not supported";
+        return -1;
+      }
+      if (q.inflow_type == 2 && (!(q.density_lower > 0) || !(q.p_lower > 0) || !(q.t_lower > 0) ||
+                                 !(q.delta_omega > 0))) {
+        why = "mixing-layer inflow needs density_lower, p_lower, t_lower and delta_omega > 0";
+        return -1;
+      }
+      if (q.fluctuation_type != 0 && q.fluctuation_type != 1) {
+        why = "inflow fluctuation_type must be 0 or 1 (white noise)";
         return -1;
       }
     }
@@ -340,6 +354,11 @@ int cfk_bind_zone(cfk_ctx *c, const cfk_zone *zn) {
   z.reaction_timeScale = zn->reaction_timeScale; z.dq = zn->dq; z.dt_local = zn->dt_local; z.Cn = zn->Cn;
   z.shock_sensor = zn->shock_sensor;
   z.fvis8 = nullptr;
+  z.y = zn->y;
+  z.inflow_draws = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(c->d_dt_bits) + 32);
+  for (int n = 0; n < c->hp.n_face; ++n)
+    if (c->hp.faces[n].label == 5 && c->hp.inflow.inflow_type == 2 && !zn->y)
+      return fail(c, CFK_ERR_ARG, "the mixing-layer inflow needs the zone's y plane");
   if (c->hp.viscous_order == 8 || c->hp.viscous_order == 4) {
     // node fluxes of the collocated viscous schemes, owned by the context
     const size_t n8 = (size_t)z.d.plane(z.d.ngg) * 3 * (c->hp.n_var - 1);
@@ -394,7 +413,7 @@ int cfk_alloc_zone(cfk_ctx *c, int mx, int my, int mz, cfk_zone *out) {
   };
   bool ok = al(&zn.jac, P) && al(&zn.metric, 9 * P) && al(&zn.cv, nv * P) && al(&zn.bv, 6 * P) &&
             al(&zn.sv, nsc * P) && al(&zn.qn, nv * P) && al(&zn.mul, P) && al(&zn.mach, P) &&
-            al(&zn.dq, nv * N) && al(&zn.dt_local, N);
+            al(&zn.dq, nv * N) && al(&zn.dt_local, N) && al(&zn.y, P);
   if (ok && c->hp.sensor_threshold > 1e-10) ok = al(&zn.shock_sensor, P);
   if (ok && ns > 0)
     ok = al(&zn.acoustic_speed, P) && al(&zn.gamma, P) && al(&zn.thermal_conductivity, P) && al(&zn.rho_D, ns * P) &&
@@ -878,6 +897,7 @@ static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *
   int n = 0;
   double dt = c->hp.dt;
   if (!p.fixed_dt) {
+    PhaseScope ps(c, CFK_PH_DT, st, &n);
     CFK_CHECK(c, launch_local_dt(z, p, th, c->d_dt_bits, st, false), "local_time_step_without_reaction");
     n += 2;
     CFK_CHECK(c, cudaMemcpyAsync(&dt, c->d_dt_bits, sizeof(double), cudaMemcpyDeviceToHost, st), "dt copy");
@@ -885,53 +905,82 @@ static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *
   }
   // compute_cn (:15-41): shock sensor, then Cn = transport right-hand side
   if (p.sensor_threshold > 1e-10) {
+    PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
     CFK_CHECK(c, launch_shock_sensor(z, p, st), "compute_shock_sensor");
     ++n;
   }
   CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
-  if (p.viscous_order > 0)
+  if (p.viscous_order > 0) {
+    PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
     CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
-  CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
-  CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "Cn copy");
+  }
+  {
+    PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
+    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
+    CFK_CHECK(c, cudaMemcpyAsync(z.Cn, z.dq, N * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st),
+              "Cn copy");
+  }
   // wu_reaction_subStep (:475-502)
-  if (rx.mode == 2) {
-    c->launches += n;
-    n = 0;
-    if (int r = cfk_surrogate_reaction_step(c, dt, rx.gate, rx.step_index, rx.stats, stream)) return r;
-  } else {
-    if (rx.mode == 1) {
-      if (int r = cfk_surrogate_record(c, 0, dt, nullptr, nullptr, stream)) return r;
-    }
-    unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
-    CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm, st),
-              "wu_reaction_step");
-    ++n;
-    if (rx.mode == 1) {
-      if (int r = cfk_surrogate_record(c, 1, dt, rx.X, rx.G, stream)) return r;
+  {
+    PhaseScope ps(c, CFK_PH_REACTION, st, &n);
+    if (rx.mode == 2) {
+      const long long before = c->launches;
+      if (int r = cfk_surrogate_reaction_step(c, dt, rx.gate, rx.step_index, rx.stats, stream)) return r;
+      n += (int)(c->launches - before);
+      c->launches = before;
+    } else {
+      if (rx.mode == 1) {
+        if (int r = cfk_surrogate_record(c, 0, dt, nullptr, nullptr, stream)) return r;
+      }
+      unsigned int *counter = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dt_bits) + 16);
+      CFK_CHECK(c, launch_wu_reaction(z, p, c->d_mech, c->h_mech, dt, schedule, nullptr, c->d_err, counter, c->n_sm,
+                                      st),
+                "wu_reaction_step");
+      ++n;
+      if (rx.mode == 1) {
+        if (int r = cfk_surrogate_record(c, 1, dt, rx.X, rx.G, stream)) return r;
+      }
     }
   }
-  CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
-                                          c->hp.outflow, st, &n),
-            "boundary conditions");
-  CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
-  ++n;
+  {
+    PhaseScope ps(c, CFK_PH_BC, st, &n);
+    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
+                                            c->hp.outflow, st, &n),
+              "boundary conditions");
+  }
+  {
+    PhaseScope ps(c, CFK_PH_PROPS, st, &n);
+    CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
+    ++n;
+  }
   // wu_RK_subStep (:564-634): SSP-RK3 over dt/2 on dq - Cn, no property update
   CFK_CHECK(c, cudaMemcpyAsync(z.qn, z.cv, P * p.n_var * sizeof(double), cudaMemcpyDeviceToDevice, st), "qn copy");
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
-    if (p.viscous_order > 0)
+    if (p.viscous_order > 0) {
+      PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
       CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
-    CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
-    CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
-    ++n;
-    if (p.limit_flow) {
-      // limit_flow<M> after the update (reference src/StrangSplitting.cu:602-604)
-      CFK_CHECK(c, launch_limit_flow(z, p, th, c->own_limit, limit_counter(c), st), "limit_flow");
-      n += 2;
     }
-    CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
-                                          c->hp.outflow, st, &n),
-            "boundary conditions");
+    {
+      PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
+      CFK_CHECK(c, launch_inviscid(z, p, thermo_host(c), nullptr, dt, c->tile_var, st, &n), "inviscid flux");
+    }
+    {
+      PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
+      CFK_CHECK(c, launch_update_rk(z, p, th, 0.5 * dt, nullptr, rk, c->d_err, st, true), "update (dq - Cn)");
+      ++n;
+      if (p.limit_flow) {
+        // limit_flow<M> after the update (reference src/StrangSplitting.cu:602-604)
+        CFK_CHECK(c, launch_limit_flow(z, p, th, c->own_limit, limit_counter(c), st), "limit_flow");
+        n += 2;
+      }
+    }
+    {
+      PhaseScope ps(c, CFK_PH_BC, st, &n);
+      CFK_CHECK(c, launch_boundary_conditions(z, p, th, c->hp.faces, c->hp.n_face, c->hp.wall, c->hp.inflow,
+                                              c->hp.outflow, st, &n),
+                "boundary conditions");
+    }
   }
   c->launches += n;
   if (dt_used) *dt_used = dt;

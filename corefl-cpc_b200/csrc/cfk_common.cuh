@@ -44,6 +44,8 @@ struct Zone {
   double *dq, *dt_local, *Cn;
   double *shock_sensor;  // ngg ghosts, zero outside the interior; hybrid WENO only
   double *fvis8;         // node viscous fluxes of the 8th-order scheme, 3 x (n_var - 1) planes, ngg ghosts
+  const double *y;       // node y coordinate, ngg ghosts (mixing-layer inflow only)
+  unsigned long long *inflow_draws;  // applications of a fluctuating inflow so far (context-owned counter)
 };
 
 // Kernel-side scalar settings.

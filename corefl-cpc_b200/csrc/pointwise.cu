@@ -4,6 +4,7 @@
 #include "cfk_common.cuh"
 #include "thermo.cuh"
 #include "cv_point.cuh"
+#include "noise.cuh"
 
 namespace cfk {
 
@@ -497,6 +498,15 @@ __global__ void bc_periodic_kernel(Zone z, Param p, const Thermo *th, FaceGeom f
 // inner node g about them with p and rho held above 0.1 of the face values
 // (subsonic).  One thread per face node and its ghost line: the face values
 // depend on the face node's values before they are overwritten.
+// Index of a face node in its face plane, padded, as the reference numbers
+// its per-node random states (src/BoundCond.cu:2485-2496).
+__device__ __forceinline__ uint64_t inflow_noise_node(const Dims &d, int face, int i, int j, int k) {
+  const int g = d.ngg;
+  if (face == 1) return (uint64_t)(k + g) * (d.mx + 2 * g) + (i + g);
+  if (face == 2) return (uint64_t)(j + g) * (d.mx + 2 * g) + (i + g);
+  return (uint64_t)(k + g) * (d.my + 2 * g) + (j + g);
+}
+
 template <bool MIX>
 __global__ void bc_inflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg, cfk_inflow in) {
   const Dims d = z.d;
@@ -508,7 +518,30 @@ __global__ void bc_inflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg,
   const int64_t sz = d.plane(g), id = d.idx(g, i, j, k);
   const int64_t s = d.stride(g, fg.face) * fg.direction;
   double density = in.density, u = in.u, v = in.v, w = in.w, pr = in.pressure, T = in.temperature;
-  if (in.subsonic) {
+  const double *svb = in.sv;
+  if (in.inflow_type == 2) {
+    // mixing layer (src/BoundCond.cu:2455-2506)
+    const double y = z.y[id];
+    u = 0.5 * (in.u + in.u_lower) + 0.5 * (in.u - in.u_lower) * tanh(2 * y / in.delta_omega);
+    if (!(y >= 0)) {
+      density = in.density_lower;
+      v = in.v_lower;
+      w = in.w_lower;
+      pr = in.p_lower;
+      T = in.t_lower;
+      svb = in.sv_lower;
+    }
+    if (in.fluctuation_type == 1) {
+      const uint64_t node = inflow_noise_node(d, fg.face, i, j, k), call = *z.inflow_draws;
+      const double rms = in.fluctuation_intensity * u * exp(-y * y);
+      double n0, n1, n2, n3;
+      noise_normal_pair(in.seed, call, node, 0, n0, n1);
+      noise_normal_pair(in.seed, call, node, 1, n2, n3);
+      u += n0 * rms;
+      v += n1 * rms;
+      w += n2 * rms;
+    }
+  } else if (in.subsonic) {
     const int mf = 3 * fg.face;
     double nx = z.metric[id + mf * sz], ny = z.metric[id + (mf + 1) * sz], nz = z.metric[id + (mf + 2) * sz];
     const double grad_n_inv = fg.direction / sqrt(nx * nx + ny * ny + nz * nz);
@@ -529,6 +562,12 @@ __global__ void bc_inflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg,
       w = in.w - (pr - in.pressure) / (rho1 * c1) * nz;
       T = MIX ? pr * in.mw / (density * kRu) : pr / (density * kRAir);
     }
+  } else if (in.fluctuation_type == 1) {
+    // white noise on u of a constant inflow (src/BoundCond.cu:2573-2596)
+    const uint64_t node = inflow_noise_node(d, fg.face, i, j, k), call = *z.inflow_draws;
+    double n0, n1;
+    noise_normal_pair(in.seed, call, node, 0, n0, n1);
+    u += n0 * in.fluctuation_intensity * sqrt(in.u * in.u + in.v * in.v + in.w * in.w);
   }
   z.bv[id] = density;
   z.bv[id + sz] = u;
@@ -536,11 +575,11 @@ __global__ void bc_inflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg,
   z.bv[id + 3 * sz] = w;
   z.bv[id + 4 * sz] = pr;
   z.bv[id + 5 * sz] = T;
-  for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = in.sv[l];
+  for (int l = 0; l < p.n_scalar; ++l) z.sv[id + l * sz] = svb[l];
   cv_from_bv_point<MIX>(z, p, th, id);
   for (int gg = 1; gg <= g; ++gg) {
     const int64_t gi = id + gg * s;
-    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = in.sv[l];
+    for (int l = 0; l < p.n_scalar; ++l) z.sv[gi + l * sz] = svb[l];
     if (in.subsonic) {
       const int64_t ii = id - gg * s;
       double rho2 = 2 * density - z.bv[ii], p2 = 2 * pr - z.bv[ii + 4 * sz];
@@ -563,6 +602,9 @@ __global__ void bc_inflow_kernel(Zone z, Param p, const Thermo *th, FaceGeom fg,
     cv_from_bv_point<MIX>(z, p, th, gi);
   }
 }
+
+// One more application of the fluctuating inflow: the next one draws new deviates.
+__global__ void inflow_draw_advance_kernel(unsigned long long *draws) { *draws += 1; }
 
 // apply_wall (reference src/BoundCond.cu:2761-3031) without its jet,
 // shock-blowing and wall-fluctuation branches (so v_blow = 0).  The face node
@@ -799,6 +841,10 @@ cudaError_t launch_boundary_conditions(const Zone &z, const Param &p, const Ther
       } else if (order[o] == 5) {
         if (mix) bc_inflow_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg, inflow);
         else bc_inflow_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg, inflow);
+        if (inflow.fluctuation_type == 1) {
+          inflow_draw_advance_kernel<<<1, 1, 0, st>>>(z.inflow_draws);
+          ++*n_launch;
+        }
       } else if (order[o] == 2) {
         if (mix) bc_wall_kernel<true><<<blocks, 128, 0, st>>>(z, p, th, fg, wall);
         else bc_wall_kernel<false><<<blocks, 128, 0, st>>>(z, p, th, fg, wall);

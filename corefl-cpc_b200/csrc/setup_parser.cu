@@ -158,12 +158,85 @@ bool read_wall(const Setup &s, cfk_wall &w, std::string &err) {
 }
 
 
+// The two streams of an air mixing layer (problem_type 1), as
+// get_mixing_layer_info computes them for air (reference
+// src/MixingLayer.cu:9-119): each stream's density and sound speed from its
+// temperature and pressure; with velocity_ratio r > 0, u_slow = Ma_c (c_upper
+// + c_lower) / (r - 1) and u_fast = r u_slow (r > 1; else u_fast = Ma_c (c_upper
+// + c_lower) / (1 - r), u_slow = r u_fast), the faster stream above when
+// upper_faster; with r <= 0 the streams' own Mach numbers (one of them may be
+// derived from Ma_c).
+bool mixing_layer_streams(const Setup &s, cfk_inflow &q, std::string &err) {
+  const double R_u = 8314.462618, mw = 28.9647, gamma = 1.4;
+  auto up_it = s.structs.find("upper_stream"), lo_it = s.structs.find("lower_stream");
+  if (up_it == s.structs.end() || lo_it == s.structs.end()) {
+    err = "problem_type 1 needs the upper_stream and lower_stream structs";
+    return false;
+  }
+  const Struct &up = up_it->second, &lo = lo_it->second;
+  const double ma_c = get(s.reals, "ma_c", 0.0), vel_ratio = get(s.reals, "velocity_ratio", 0.0);
+  const bool upper_faster = get(s.bools, "upper_faster", false);
+  double ma_upper = struct_real(up, "mach", -1), ma_lower = struct_real(lo, "mach", -1);
+  const double T_upper = struct_real(up, "temperature", -1), T_lower = struct_real(lo, "temperature", -1);
+  const double p_upper = struct_real(up, "pressure", -1), p_lower = struct_real(lo, "pressure", -1);
+  if (!(T_upper > 0) || !(T_lower > 0) || !(p_upper > 0) || !(p_lower > 0)) {
+    err = "mixing-layer streams need temperature and pressure > 0";
+    return false;
+  }
+  const double c_upper = std::sqrt(gamma * R_u / mw * T_upper), c_lower = std::sqrt(gamma * R_u / mw * T_lower);
+  if (vel_ratio > 0) {
+    double u_slow, u_fast;
+    if (vel_ratio > 1) {
+      u_slow = ma_c * (c_upper + c_lower) / (vel_ratio - 1);
+      u_fast = vel_ratio * u_slow;
+    } else {
+      u_fast = ma_c * (c_upper + c_lower) / (1 - vel_ratio);
+      u_slow = u_fast * vel_ratio;
+    }
+    ma_upper = (upper_faster ? u_fast : u_slow) / c_upper;
+    ma_lower = (upper_faster ? u_slow : u_fast) / c_lower;
+  } else if (ma_upper < 0 && ma_lower < 0) {
+    err = "at least one of the streams' Mach numbers and the convective Mach number must be given";
+    return false;
+  } else if (ma_upper > 0 && ma_lower > 0) {
+    // both given: the streams win over ma_c, as in the reference
+  } else if (ma_upper > 0) {
+    ma_lower = upper_faster ? (ma_upper - ma_c) * c_upper / c_lower - ma_c
+                            : (ma_c + ma_upper) * c_upper / c_lower + ma_c;
+  } else {
+    ma_upper = upper_faster ? (ma_c + ma_lower) * c_lower / c_upper + ma_c
+                            : (ma_lower - ma_c) * c_lower / c_upper - ma_c;
+  }
+  q.inflow_type = 2;
+  q.density = p_upper * mw / (R_u * T_upper);
+  q.u = ma_upper * c_upper;
+  q.v = q.w = 0;
+  q.pressure = p_upper;
+  q.temperature = T_upper;
+  q.mw = mw;
+  q.density_lower = p_lower * mw / (R_u * T_lower);
+  q.u_lower = ma_lower * c_lower;
+  q.v_lower = q.w_lower = 0;
+  q.p_lower = p_lower;
+  q.t_lower = T_lower;
+  q.delta_omega = get(s.reals, "delta_omega", 0.0);
+  if (!(q.delta_omega > 0)) {
+    err = "problem_type 1 needs delta_omega > 0";
+    return false;
+  }
+  return true;
+}
+
 // The inflow condition of the boundary_conditions list, air (reference
-// src/BoundCond.cpp:9-260, Inflow::Inflow for a constant inflow): the state
+// src/BoundCond.cpp:9-260, Inflow::Inflow): a constant inflow, the state
 // from one of (mach, pressure, temperature), (density, velocity, pressure)
 // or (mach, temperature, reynolds), the velocity along aoa (degrees) or along
-// (u, v, w).  Profile and mixing-layer inflows and inflow fluctuations are
-// not part of this path and are reported; so is a second inflow struct.
+// (u, v, w); with problem_type 1 the mixing-layer inflow of
+// mixing_layer_streams.  fluctuation_type 1 (white noise) takes
+// fluctuation_intensity; the deviates are seeded by the int random_seed
+// (default 0) where the reference seeds curand from the clock.  Profile
+// inflows and the other fluctuation forms are reported; so is a second
+// inflow struct.
 bool read_inflow(const Setup &s, cfk_inflow &q, std::string &err) {
   std::memset(&q, 0, sizeof(q));
   auto list = s.arrays.find("boundary_conditions");
@@ -174,9 +247,26 @@ bool read_inflow(const Setup &s, cfk_inflow &q, std::string &err) {
     if (it == s.structs.end() || struct_string(it->second, "type") != "inflow") continue;
     const Struct &st = it->second;
     if (++n_inflow > 1) { err = "more than one inflow condition; cfk_param carries one"; return false; }
-    if (struct_int(st, "inflow_type", 0) != 0 || struct_int(st, "fluctuation_type", 0) != 0) {
-      err = "inflow " + name + ": profile, mixing-layer and fluctuating inflows are not supported";
+    const int problem_type = get(s.ints, "problem_type", 0);
+    int inflow_type = struct_int(st, "inflow_type", 0);
+    if (problem_type == 1) inflow_type = 2;                      // src/BoundCond.cpp:12-16
+    if (problem_type == 0 && inflow_type == 2) inflow_type = 0;
+    const int fluctuation_type = struct_int(st, "fluctuation_type", 0);
+    if (inflow_type != 0 && inflow_type != 2) {
+      err = "inflow " + name + ": profile inflows are not supported";
       return false;
+    }
+    if (fluctuation_type != 0 && fluctuation_type != 1) {
+      err = "inflow " + name + ": only the white-noise fluctuation (fluctuation_type 1) is supported";
+      return false;
+    }
+    q.fluctuation_type = fluctuation_type;
+    q.fluctuation_intensity = fluctuation_type == 1 ? struct_real(st, "fluctuation_intensity", 0.0) : 0.0;
+    q.seed = (unsigned long long)get(s.ints, "random_seed", 0);
+    q.subsonic = struct_int(st, "inflow_sub", 0);
+    if (inflow_type == 2) {
+      if (!mixing_layer_streams(s, q, err)) return false;
+      continue;
     }
     const double R_u = 8314.462618, mw = 28.9647, gamma = 1.4, pi = 3.141592653589793;
     double mach = struct_real(st, "mach", -1), pressure = struct_real(st, "pressure", -1);

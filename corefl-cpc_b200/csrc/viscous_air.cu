@@ -145,23 +145,35 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
   int cur = 1;  // slot of plane k
   for (int k = k0; k < k_end; ++k) {
     const int nxt = cur ^ 1;  // holds plane k-1, receives plane k+1
-    // k-differences of plane k: u, v, w, T of plane k+1 minus those of plane k-1 (slot nxt)
+    // dq of this node for plane k: loaded now, used after the faces
+    double acc[4];
+    const int64_t iq = d.idx(0, i, j, k);
+    if (mine) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = z.dq[iq + (q + 1) * szq];
+    }
+    // plane k+1 replaces plane k-1 point by point: every point is read and
+    // written by the thread that loads it, so the k-differences
+    // f(k+1) - f(k-1) of u, v, w, T come from the old slot value before the
+    // new one overwrites it, with no barrier between the two
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       int px, py;
       if (!point_ok(threadIdx.x + r * kFT, px, py)) continue;
       const int64_t id = d.idx(g, i0 - 1 + px, j0 - 1 + py, k + 1);
-      S.dzp[0][py][px] = z.bv[id + sz] - S.pl[nxt][0][py][px];
-      S.dzp[1][py][px] = z.bv[id + 2 * sz] - S.pl[nxt][1][py][px];
-      S.dzp[2][py][px] = z.bv[id + 3 * sz] - S.pl[nxt][2][py][px];
-      S.dzp[3][py][px] = z.bv[id + 5 * sz] - S.pl[nxt][3][py][px];
-    }
-    __syncthreads();
-    // plane k+1 replaces plane k-1 (its first four values come back from L1)
+      double v[kNV];
+      v[0] = z.bv[id + sz];
+      v[1] = z.bv[id + 2 * sz];
+      v[2] = z.bv[id + 3 * sz];
+      v[3] = z.bv[id + 5 * sz];
+      v[4] = z.mul[id];
+      v[5] = z.jac[id];
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      int px, py;
-      if (point_ok(threadIdx.x + r * kFT, px, py)) load_point(k + 1, px, py, nxt);
+      for (int l = 0; l < 9; ++l) v[6 + l] = z.metric[id + l * sz];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) S.dzp[q][py][px] = v[q] - S.pl[nxt][q][py][px];
+#pragma unroll
+      for (int q = 0; q < kNV; ++q) S.pl[nxt][q][py][px] = v[q];
     }
     __syncthreads();
     // x faces (33 per row) and y faces (9 per column) of plane k as one work
@@ -194,14 +206,13 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
     }
     __syncthreads();
     if (mine) {
-      const int64_t iq = d.idx(0, i, j, k);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        double acc = z.dq[iq + (q + 1) * szq];
-        acc += S.fx[q][ty][tx + 1] - S.fx[q][ty][tx];
-        acc += S.fy[q][ty + 1][tx] - S.fy[q][ty][tx];
-        if (three_d) acc += fzn[q] - fzp[q];
-        z.dq[iq + (q + 1) * szq] = acc;
+        double a = acc[q];
+        a += S.fx[q][ty][tx + 1] - S.fx[q][ty][tx];
+        a += S.fy[q][ty + 1][tx] - S.fy[q][ty][tx];
+        if (three_d) a += fzn[q] - fzp[q];
+        z.dq[iq + (q + 1) * szq] = a;
       }
     }
 #pragma unroll

@@ -76,17 +76,37 @@ typedef struct cfk_inner_face {
   int n_point[3];
 } cfk_inner_face;
 
-/* The constant inflow of the faces labelled 5 (reference src/BoundCond.h:22-87,
- * Inflow with inflow_type 0 and no fluctuation): the state the reference
- * derives in Inflow::Inflow (src/BoundCond.cpp:160-250) — density, velocity,
- * pressure, temperature, the mean molecular weight (mixtures) and the
- * scalars (mass fractions).  subsonic = the reference's inflow_sub: where the
- * normal Mach number at the face is not below -1 the face takes the
- * characteristic combination of the inflow state and the inner node. */
+/* The inflow of the faces labelled 5 (reference src/BoundCond.h:22-87,
+ * Inflow): the state the reference derives in Inflow::Inflow
+ * (src/BoundCond.cpp:9-260) — density, velocity, pressure, temperature, the
+ * mean molecular weight (mixtures) and the scalars (mass fractions).
+ * subsonic = the reference's inflow_sub: where the normal Mach number at the
+ * face is not below -1 the face takes the characteristic combination of the
+ * inflow state and the inner node.
+ * inflow_type 0: the constant state.  inflow_type 2 (mixing layer, the
+ * reference's problem_type 1): u = (u + u_lower)/2 + (u - u_lower)/2 *
+ * tanh(2 y / delta_omega), and the other variables and scalars from the
+ * upper set (the fields above) where y >= 0, from the *_lower set below
+ * (src/BoundCond.cu:2455-2478); needs the zone's y plane.
+ * fluctuation_type 1 (white noise, src/BoundCond.cu:2290-2313, 2479-2505,
+ * 2573-2596): normal deviates added to the face velocity every time the
+ * boundary conditions are applied — inflow_type 2: u, v, w each plus
+ * N(0,1) * fluctuation_intensity * u * exp(-y^2); inflow_type 0: u plus
+ * N(0,1) * fluctuation_intensity * |V|.  The deviates are this library's own
+ * seeded counter-based stream (SplitMix64 hashing of seed, face node and the
+ * context's count of applications, Box-Muller), not curand's: runs repeat
+ * bit for bit for a given seed.  Not subsonic with inflow_type 2. */
 typedef struct cfk_inflow {
   int subsonic;
   double density, u, v, w, pressure, temperature, mw;
   double sv[CFK_MAX_SPEC];
+  int inflow_type;                 /* 0 constant, 2 mixing layer */
+  double density_lower, u_lower, v_lower, w_lower, p_lower, t_lower;
+  double sv_lower[CFK_MAX_SPEC];
+  double delta_omega;              /* initial vorticity thickness, m */
+  int fluctuation_type;            /* 0 none, 1 white noise */
+  double fluctuation_intensity;
+  unsigned long long seed;
 } cfk_inflow;
 
 /* The outflow of the faces labelled 6 (reference src/BoundCond.h:125-134,
@@ -147,6 +167,8 @@ typedef struct cfk_zone {
   double *dq, *dt_local, *Cn;    /* n_var, 1, n_var planes, 0 ghosts */
   double *shock_sensor;          /* 1 plane, ngg ghosts, zero-initialised; hybrid schemes only.  NULL: the
                                     context allocates its own */
+  double *y;                     /* 1 plane, ngg ghosts: node y coordinate (DZone::y); required by the
+                                    mixing-layer inflow and its white noise, else may be NULL */
 } cfk_zone;
 
 /* Species, thermo, transport and kinetics tables of a mechanism — the
@@ -510,10 +532,12 @@ int cfk_wu_splitting_step_surrogate(cfk_ctx *ctx, const cfk_surrogate_gate *gate
                                     cfk_surrogate_stats *stats, double *dt_used, void *stream);
 
 /* ---- measurement ------------------------------------------------------ */
-/* Phases of a step timed with CUDA events when profiling is on (plain steps
- * only; graph replays are not instrumented). */
+/* Phases of a step timed with CUDA events when profiling is on (RK3 and Wu
+ * steps; graph replays are not instrumented).  CFK_PH_REACTION is the
+ * reaction sub-step of Wu's splitting (plain, recorded or surrogate). */
 enum cfk_phase {
-  CFK_PH_INVISCID = 0, CFK_PH_VISCOUS, CFK_PH_UPDATE, CFK_PH_BC, CFK_PH_PROPS, CFK_PH_DT, CFK_NPHASE
+  CFK_PH_INVISCID = 0, CFK_PH_VISCOUS, CFK_PH_UPDATE, CFK_PH_BC, CFK_PH_PROPS, CFK_PH_DT, CFK_PH_REACTION,
+  CFK_NPHASE
 };
 int cfk_set_profiling(cfk_ctx *ctx, int on);
 /* Synchronises the recorded events, writes the summed milliseconds and kernel

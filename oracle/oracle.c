@@ -10,6 +10,7 @@
  * few ulp.
  */
 #include "oracle.h"
+#include <stdint.h>
 
 #include <math.h>
 #include <stdlib.h>
@@ -1047,8 +1048,46 @@ static void apply_wall_face(orc_zone *z, const orc_param *p, const orc_face *f) 
       }
 }
 
-/* apply_inflow (src/BoundCond.cu:2190-2705), constant inflow without
- * fluctuations (inflow_type 0, fluctuation_type 0). */
+/* Seeded white noise of the fluctuating inflow (test infrastructure: the
+ * same integer steps as the library's counter-based stream): the SplitMix64
+ * output function (Steele, Lea and Flood, OOPSLA 2014) on a key of seed,
+ * application count and face node gives uniforms in (0, 1]; Box-Muller gives
+ * the normal deviates. */
+static uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+double orc_noise_uniform(unsigned long long seed, unsigned long long call, unsigned long long node,
+                         unsigned long long n) {
+  const uint64_t key = splitmix64(seed ^ splitmix64((call << 24) ^ node));
+  const uint64_t r = splitmix64(key + n * 0x9E3779B97F4A7C15ull);
+  return (double)((r >> 11) + 1) * 0x1.0p-53;
+}
+
+static void noise_normal_pair(uint64_t seed, uint64_t call, uint64_t node, uint64_t m, double *n0, double *n1) {
+  const double u1 = orc_noise_uniform(seed, call, node, 2 * m), u2 = orc_noise_uniform(seed, call, node, 2 * m + 1);
+  const double r = sqrt(-2.0 * log(u1));
+  const double a = 2.0 * 3.141592653589793 * u2;
+  *n0 = r * cos(a);
+  *n1 = r * sin(a);
+}
+
+/* index of a face node in its padded face plane (src/BoundCond.cu:2485-2496) */
+static uint64_t inflow_noise_node(const orc_zone *z, int face, int i, int j, int k) {
+  const int g = z->ngg;
+  if (face == 1) return (uint64_t)(k + g) * (uint64_t)(z->mx + 2 * g) + (uint64_t)(i + g);
+  if (face == 2) return (uint64_t)(j + g) * (uint64_t)(z->mx + 2 * g) + (uint64_t)(i + g);
+  return (uint64_t)(k + g) * (uint64_t)(z->my + 2 * g) + (uint64_t)(j + g);
+}
+
+/* apply_inflow (src/BoundCond.cu:2190-2705): the constant inflow
+ * (inflow_type 0, with inflow_sub and with the white noise on u of
+ * :2573-2596) and the mixing-layer inflow (inflow_type 2, :2455-2506, with
+ * the white noise on u, v, w).  Profile inflows and the other fluctuation
+ * forms are not restated. */
 static void apply_inflow_face(orc_zone *z, const orc_param *p, const orc_face *f) {
   const int g = z->ngg;
   const long sz = psz(z, g);
@@ -1057,13 +1096,37 @@ static void apply_inflow_face(orc_zone *z, const orc_param *p, const orc_face *f
   const long s = pstride(z, g, f->face) * f->direction;
   const int mix = p->mech != NULL;
   double *bv = z->bv, *sv = z->sv;
+  const uint64_t call = z->inflow_draws;
   for (int k = lo[2]; k <= hi[2]; ++k)
     for (int j = lo[1]; j <= hi[1]; ++j)
       for (int i = lo[0]; i <= hi[0]; ++i) {
         const long id = pidx(z, g, i, j, k);
         double density = p->inflow_density, u = p->inflow_u, v = p->inflow_v, w = p->inflow_w;
         double pr = p->inflow_pressure, T = p->inflow_temperature;
-        if (p->inflow_subsonic) {
+        const double *svb = p->inflow_sv;
+        if (p->inflow_type == 2) {
+          const double y = z->y[id];
+          u = 0.5 * (p->inflow_u + p->inflow_u_lower) +
+              0.5 * (p->inflow_u - p->inflow_u_lower) * tanh(2 * y / p->inflow_delta_omega);
+          if (!(y >= 0)) {
+            density = p->inflow_density_lower;
+            v = p->inflow_v_lower;
+            w = p->inflow_w_lower;
+            pr = p->inflow_p_lower;
+            T = p->inflow_t_lower;
+            svb = p->inflow_sv_lower;
+          }
+          if (p->inflow_fluctuation_type == 1) {
+            const uint64_t node = inflow_noise_node(z, f->face, i, j, k);
+            const double rms = p->inflow_fluctuation_intensity * u * exp(-y * y);
+            double n0, n1, n2, n3;
+            noise_normal_pair(p->inflow_seed, call, node, 0, &n0, &n1);
+            noise_normal_pair(p->inflow_seed, call, node, 1, &n2, &n3);
+            u += n0 * rms;
+            v += n1 * rms;
+            w += n2 * rms;
+          }
+        } else if (p->inflow_subsonic) {
           const double *mt = z->metric;
           const int mf = 3 * f->face;
           double nx = mt[id + mf * sz], ny = mt[id + (mf + 1) * sz], nz = mt[id + (mf + 2) * sz];
@@ -1086,14 +1149,20 @@ static void apply_inflow_face(orc_zone *z, const orc_param *p, const orc_face *f
             w = p->inflow_w - (pr - p->inflow_pressure) / (rho1 * c1) * nz;
             T = mix ? pr * p->inflow_mw / (density * R_U) : pr / (density * R_AIR);
           }
+        } else if (p->inflow_fluctuation_type == 1) {
+          const uint64_t node = inflow_noise_node(z, f->face, i, j, k);
+          double n0, n1;
+          noise_normal_pair(p->inflow_seed, call, node, 0, &n0, &n1);
+          u += n0 * p->inflow_fluctuation_intensity *
+               sqrt(p->inflow_u * p->inflow_u + p->inflow_v * p->inflow_v + p->inflow_w * p->inflow_w);
         }
         bv[id] = density; bv[id + sz] = u; bv[id + 2 * sz] = v; bv[id + 3 * sz] = w;
         bv[id + 4 * sz] = pr; bv[id + 5 * sz] = T;
-        for (int l = 0; l < p->n_scalar; ++l) sv[id + l * sz] = p->inflow_sv[l];
+        for (int l = 0; l < p->n_scalar; ++l) sv[id + l * sz] = svb[l];
         cv_from_bv_point(z, p, id);
         for (int gg = 1; gg <= g; ++gg) {
           const long gi = id + gg * s;
-          for (int l = 0; l < p->n_scalar; ++l) sv[gi + l * sz] = p->inflow_sv[l];
+          for (int l = 0; l < p->n_scalar; ++l) sv[gi + l * sz] = svb[l];
           if (p->inflow_subsonic) {
             const long ii = id - gg * s;
             double rho2 = 2 * density - bv[ii], p2 = 2 * pr - bv[ii + 4 * sz];
@@ -1112,6 +1181,7 @@ static void apply_inflow_face(orc_zone *z, const orc_param *p, const orc_face *f
           cv_from_bv_point(z, p, gi);
         }
       }
+  if (p->inflow_fluctuation_type == 1) z->inflow_draws += 1;
 }
 
 void orc_apply_boundary_conditions(orc_zone *z, const orc_param *p) {

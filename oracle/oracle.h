@@ -45,6 +45,10 @@ typedef struct {
   /* the step's dt as DParameter::dt holds it after update_dt_global
    * (src/DParameter.cu:396-398); read by the positive-preserving limiter */
   double dt_step;
+  /* node y coordinate with ngg ghosts (the mixing-layer inflow; may be NULL) */
+  double *y;
+  /* applications of a fluctuating inflow so far */
+  unsigned long long inflow_draws;
 } orc_zone;
 
 /* Species / mechanism tables (reference src/DParameter.cuh:84-130). */
@@ -101,6 +105,16 @@ typedef struct {
   int inflow_subsonic;
   double inflow_density, inflow_u, inflow_v, inflow_w, inflow_pressure, inflow_temperature, inflow_mw;
   double inflow_sv[ORC_MAX_SPEC];
+  /* inflow_type 2: the mixing-layer inflow (src/BoundCond.cu:2455-2506) with
+   * the lower stream below y = 0; inflow_fluctuation_type 1: white noise on
+   * the face velocity, seeded SplitMix64 + Box-Muller deviates */
+  int inflow_type;
+  double inflow_density_lower, inflow_u_lower, inflow_v_lower, inflow_w_lower, inflow_p_lower, inflow_t_lower;
+  double inflow_sv_lower[ORC_MAX_SPEC];
+  double inflow_delta_omega;
+  int inflow_fluctuation_type;
+  double inflow_fluctuation_intensity;
+  unsigned long long inflow_seed;
   /* outflow faces (src/BoundCond.h:125-134): if_backPressure, backPressure */
   int outflow_back_pressure_on;
   double outflow_back_pressure;
@@ -144,6 +158,9 @@ int orc_limit_flow(orc_zone *z, const orc_param *p, const double ll[5], const do
 long orc_halo_size(const orc_zone *z, const orc_param *p, int face);
 void orc_halo_pack(const orc_zone *z, const orc_param *p, int face, int direction, double *buf);
 void orc_halo_assign(orc_zone *z, const orc_param *p, int face, int direction, const double *buf);
+/* uniform deviate n of face node `node` at inflow application `call` */
+double orc_noise_uniform(unsigned long long seed, unsigned long long call, unsigned long long node,
+                         unsigned long long n);
 
 /* zone memory management (host, zero-filled) */
 int orc_zone_alloc(orc_zone *z, int mx, int my, int mz, int ngg, int n_var, int n_spec, int n_scalar);

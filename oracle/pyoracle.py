@@ -27,7 +27,7 @@ class orc_zone(ctypes.Structure):
         (n, _DP) for n in ("cv", "bv", "sv", "qn", "metric", "jac", "mul", "mach", "fFlux", "gFlux", "hFlux",
                            "acoustic_speed", "gamma", "thermal_conductivity", "rho_D", "reaction_timeScale", "dq",
                            "dt_local", "Cn", "vis_flux", "shock_sensor")
-    ] + [("dt_step", ctypes.c_double)]
+    ] + [("dt_step", ctypes.c_double), ("y", _DP), ("inflow_draws", ctypes.c_ulonglong)]
 
 
 class orc_param(ctypes.Structure):
@@ -45,6 +45,11 @@ class orc_param(ctypes.Structure):
         ("inflow_subsonic", ctypes.c_int), ("inflow_density", ctypes.c_double), ("inflow_u", ctypes.c_double),
         ("inflow_v", ctypes.c_double), ("inflow_w", ctypes.c_double), ("inflow_pressure", ctypes.c_double),
         ("inflow_temperature", ctypes.c_double), ("inflow_mw", ctypes.c_double), ("inflow_sv", ctypes.c_double * 20),
+        ("inflow_type", ctypes.c_int), ("inflow_density_lower", ctypes.c_double), ("inflow_u_lower", ctypes.c_double),
+        ("inflow_v_lower", ctypes.c_double), ("inflow_w_lower", ctypes.c_double), ("inflow_p_lower", ctypes.c_double),
+        ("inflow_t_lower", ctypes.c_double), ("inflow_sv_lower", ctypes.c_double * 20),
+        ("inflow_delta_omega", ctypes.c_double), ("inflow_fluctuation_type", ctypes.c_int),
+        ("inflow_fluctuation_intensity", ctypes.c_double), ("inflow_seed", ctypes.c_ulonglong),
         ("outflow_back_pressure_on", ctypes.c_int), ("outflow_back_pressure", ctypes.c_double),
         ("limit_flow", ctypes.c_int), ("limit_ll", ctypes.c_double * 5), ("limit_ul", ctypes.c_double * 5),
     ]
@@ -140,6 +145,20 @@ def register_inner_face(dim, ngg, src, tar, target_block) -> orc_inner_face:
     return f
 
 
+def use_native_build() -> bool:
+    """Switch this process to the oracle built with -march=native for the
+    host it runs on (the timed CPU baseline); must precede the first lib().
+    Returns False, keeping the portable build, when the compiler fails."""
+    global LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("the oracle library is already loaded")
+    r = subprocess.run(["make", "-C", _HERE, "native"], capture_output=True)
+    if r.returncode != 0:
+        return False
+    LIB_PATH = os.path.join(_HERE, "_native", "liboracle.so")
+    return True
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
@@ -188,6 +207,8 @@ def lib() -> ctypes.CDLL:
         L.orc_halo_pack.restype = None
         L.orc_halo_assign.argtypes = [zp, pp, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.orc_halo_assign.restype = None
+        L.orc_noise_uniform.argtypes = [ctypes.c_ulonglong] * 4
+        L.orc_noise_uniform.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -220,12 +241,14 @@ class OracleZone:
         }
         if c.sv.shape[0]:
             self.arrays["sv"][: c.sv.shape[0]] = c.sv
+        if getattr(c, "y", None) is not None:
+            self.arrays["y"] = np.ascontiguousarray(c.y, dtype=np.float64)
         self.z = orc_zone(c.mx, c.my, c.mz, g)
         for k, a in self.arrays.items():
             setattr(self.z, k, _ptr(a))
         self.p = orc_param()
         for k, v in c.param.items():
-            if k in ("wall_yk", "inflow_sv", "limit_ll", "limit_ul"):
+            if k in ("wall_yk", "inflow_sv", "inflow_sv_lower", "limit_ll", "limit_ul"):
                 arr = getattr(self.p, k)
                 for l, y in enumerate(v):
                     arr[l] = y

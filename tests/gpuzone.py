@@ -36,6 +36,8 @@ class GpuZone:
                 self.t[k] = z(P)
             self.t["rho_D"] = z(ns, P)
             self.t["Cn"] = z(nv, N)
+        if getattr(c, "y", None) is not None:
+            self.t["y"] = torch.from_numpy(np.ascontiguousarray(c.y)).to(dev)
         if sensor_array and p.get("sensor_threshold", 0.0) > 1e-10:
             self.t["shock_sensor"] = z(P)  # else the context allocates its own
         self.ctx.bind(c.mx, c.my, c.mz, c.ngg, {k: v.data_ptr() for k, v in self.t.items()})

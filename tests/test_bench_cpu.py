@@ -15,8 +15,9 @@ def test_cpu_baseline_sample_runs_for_each_scheme_family():
     import bench
 
     for scheme, recon in ((72, 2), (4, 2)):
-        r = bench.cpu_baseline_sample(scheme, recon, target_s=0.2, n=13)
-        assert r["value"] > 0 and r["steps"] >= 1 and r["kind"] == "port" and r["cores"] >= 1
+        r = bench.cpu_baseline_sample(scheme, recon, steps=3, warm=0, n=13)
+        assert r["value"] > 0 and r["steps"] == 3 and r["kind"] == "port" and r["cores"] >= 1
+        assert r["spread"][0] <= r["value"] <= r["spread"][1] and "median of 3" in r["sample"]
 
 
 def test_reference_arm_prints_one_json_line():
@@ -65,7 +66,7 @@ def test_reference_arm_under_torchrun_prints_once():
         port = sk.getsockname()[1]
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus",
-           "2", "--steps", "1", "--warmup", "0"]
+           "2", "--steps", "1", "--warmup", "0", "--block-n", "17"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]

@@ -167,3 +167,45 @@ def test_setup_inflow_struct_and_checks(tmp_path):
     bad = corefl_b200.make_param(dict(dim=3, n_var=5, inviscid_scheme=52, weno_eps_scale=1.0, inflow_density=-1.0,
                                       inflow_pressure=1.0, inflow_temperature=1.0), [(0, -1, 5)])
     assert corefl_b200.lib().cfk_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+
+
+def test_setup_mixing_layer_and_white_noise(tmp_path):
+    """problem_type 1 makes the inflow the mixing-layer inflow with the air
+    streams of get_mixing_layer_info (src/MixingLayer.cu:9-119); the white
+    noise takes its intensity and the seed; other fluctuation forms and
+    profile inflows are reported."""
+    import corefl_b200
+
+    def param_of(text):
+        f = tmp_path / "setup.txt"
+        f.write_text(text)
+        p = corefl_b200.cfk_param()
+        err = ctypes.create_string_buffer(256)
+        rc = corefl_b200.lib().cfk_param_from_setup(str(f).encode(), ctypes.byref(p), err, 256)
+        return rc, p, err.value.decode()
+
+    head = "int inviscid_scheme = 52\narray string boundary_conditions {\n  farfield outflow\n}\n"
+    inflow = ("struct farfield {\n string type = inflow\n int label = 5\n int fluctuation_type = 1\n"
+              " real fluctuation_intensity = 0.01\n}\n")
+    streams = ("int problem_type = 1\nreal ma_c = 0.3\nreal velocity_ratio = 1.5\nbool upper_faster = 1\n"
+               "real delta_omega = 1e-3\nint random_seed = 42\n"
+               "struct upper_stream {\n real temperature = 600\n real pressure = 101325\n}\n"
+               "struct lower_stream {\n real temperature = 400\n real pressure = 101325\n}\n")
+    rc, p, err = param_of(head + streams + inflow)
+    assert rc == 0, err
+    q = p.inflow
+    c_up, c_lo = np.sqrt(1.4 * R_U / MW_AIR * 600.0), np.sqrt(1.4 * R_U / MW_AIR * 400.0)
+    u_slow = 0.3 * (c_up + c_lo) / 0.5
+    assert q.inflow_type == 2 and q.u == pytest.approx(1.5 * u_slow, rel=1e-14)
+    assert q.u_lower == pytest.approx(u_slow, rel=1e-14)
+    assert q.density_lower == pytest.approx(101325 * MW_AIR / (R_U * 400.0), rel=1e-14)
+    assert q.delta_omega == 1e-3 and q.fluctuation_type == 1 and q.fluctuation_intensity == 0.01 and q.seed == 42
+    rc, _, err = param_of(head + "int problem_type = 1\n" + inflow)
+    assert rc == -5 and "upper_stream" in err
+    rc, _, err = param_of(head + "struct farfield {\n string type = inflow\n int fluctuation_type = 2\n"
+                          " real mach = 2\n real pressure = 1e5\n real temperature = 300\n}\n")
+    assert rc == -5 and "white-noise" in err
+    rc, p, err = param_of(head + "struct farfield {\n string type = inflow\n int fluctuation_type = 1\n"
+                          " real fluctuation_intensity = 0.02\n real mach = 2\n real pressure = 1e5\n"
+                          " real temperature = 300\n}\n")
+    assert rc == 0 and p.inflow.inflow_type == 0 and p.inflow.fluctuation_intensity == 0.02
