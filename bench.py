@@ -354,6 +354,11 @@ def surrogate_bench(args, local):
         "T_max_abs_err_K": float(np.abs(Ts_ - Tp).max()),
         "on_network": sum(x["surrogate"] for x in st) / max(sum(x["cells"] for x in st), 1),
         "plain_ms": traj["plain"][1], "surrogate_ms": traj["surrogate"][1]}
+    # the whole window from the unburnt start: total device time of each path
+    out["whole_window"] = {"cells": n_acc, "steps": window, "plain_s": traj["plain"][1] * 1e-3,
+                           "surrogate_s": traj["surrogate"][1] * 1e-3,
+                           "speedup": traj["plain"][1] / traj["surrogate"][1],
+                           "note": "includes the per-step copy of the temperature plane for the accuracy check"}
 
     # 3. throughput on 2^20 reactors at the run's state mix
     n = args.reacting_cells
@@ -654,7 +659,7 @@ def main():
     ap.add_argument("--surrogate-only", action="store_true", help="only the MLP surrogate measurement")
     ap.add_argument("--surrogate-window", type=int, default=600, help="steps of the training/accuracy window")
     ap.add_argument("--surrogate-train-cells", type=int, default=16384)
-    ap.add_argument("--surrogate-accuracy-cells", type=int, default=2048)
+    ap.add_argument("--surrogate-accuracy-cells", type=int, default=16384)
     ap.add_argument("--surrogate-epochs", type=int, default=200)
     ap.add_argument("--no-surrogate-flow", action="store_true")
     ap.add_argument("--surrogate-flow-only", action="store_true", help="only the surrogate-in-the-flow measurement")
@@ -726,6 +731,7 @@ def main():
     ctx.sync()
     # tile shapes of the WENO sweeps, timed on this block (outside the timed region)
     tiles, tile_ms = ([0, 0, 0], None) if args.no_autotune else ctx.autotune_tiles(reps=3)
+    visc_var, visc_ms = ctx.viscous_variant()
 
     for _ in range(args.warmup):
         ctx.rk3_step(want_dt=False)
@@ -873,7 +879,8 @@ def main():
                                    " + 2nd-order viscous, SSP-RK3 CFL 0.5 (device dt)",
                        "nodes": f"{n}^3", "global_nodes": nodes * world,
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cv alone "
-                       f"{5 * P * 8 / 1e6:.0f} MB)", "weno_tile_variants": tiles, "autotune_ms": tile_ms},
+                       f"{5 * P * 8 / 1e6:.0f} MB)", "weno_tile_variants": tiles, "autotune_ms": tile_ms,
+                       "viscous_form": ["staged", "ring"][visc_var], "viscous_form_ms": visc_ms},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "gpu_launches": launches,
             "roofline": roofline,

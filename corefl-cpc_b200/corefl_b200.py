@@ -184,6 +184,7 @@ def lib() -> ctypes.CDLL:
             "cfk_compute_shock_sensor": (i, [vp, vp]),
             "cfk_autotune_tiles": (i, [vp, i, ctypes.POINTER(d), ctypes.POINTER(i), vp]),
             "cfk_set_tile_variants": (i, [vp, ctypes.POINTER(i)]),
+            "cfk_viscous_variant": (i, [vp, i, ctypes.POINTER(i), _DP]),
             "cfk_update_cv_and_bv_rk": (i, [vp, d, i, vp]),
             "cfk_update_physical_properties": (i, [vp, vp]),
             "cfk_limit_flow": (i, [vp, ctypes.POINTER(ctypes.c_longlong), vp]),
@@ -461,6 +462,15 @@ class Context:
         ch = (ctypes.c_int * 3)()
         self._ck(self.L.cfk_autotune_tiles(self.h, reps, ms, ch, stream), "autotune_tiles")
         return list(ch), [list(ms[d * TILE_VARIANTS:(d + 1) * TILE_VARIANTS]) for d in range(3)]
+
+    def viscous_variant(self, set_to=None):
+        """The fused air viscous kernel's form (0 staged, 1 ring) and the last
+        autotune's per-launch times; set_to selects a form."""
+        v = ctypes.c_int(set_to if set_to is not None else 0)
+        ms = (ctypes.c_double * 2)()
+        self._ck(self.L.cfk_viscous_variant(self.h, 1 if set_to is not None else 0, ctypes.byref(v), ms),
+                 "viscous_variant")
+        return v.value, list(ms)
 
     def set_tile_variants(self, var):
         v = (ctypes.c_int * 3)(*var)

@@ -26,12 +26,13 @@ cudaError_t launch_weno_mix_dir(const Zone &z, const Param &p, const Thermo &th,
 cudaError_t weno_mix_init_attributes();
 cudaError_t launch_viscous_mix(const Zone &z, const Param &p, const Thermo &th, cudaStream_t st, int *n_launch);
 cudaError_t viscous_mix_init_attributes();
-cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch);
+cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch, int var);
 cudaError_t viscous_air_init_attributes();
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
-                             int rk, int *err, cudaStream_t st, bool minus_cn = false);
+                             int rk, int *err, cudaStream_t st, bool minus_cn = false, bool with_props = false);
 cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
-cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
+cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st,
+                                     bool shell = false);
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
                             cudaStream_t st, bool with_reaction = true);
 cudaError_t launch_limit_flow(const Zone &z, const Param &p, const Thermo *th, unsigned char *bad,
@@ -113,9 +114,9 @@ cudaError_t launch_inviscid(const Zone &z, const Param &p, const Thermo *th, con
 // compute_viscous_flux dispatch (reference src/ViscousScheme.cu:7-73): the
 // 2nd-order face scheme or the 8th-order collocated one.
 cudaError_t launch_viscous(const Zone &z, const Param &p, const Thermo *th, const cfk_face *faces, int n_face,
-                           cudaStream_t st, int *n) {
+                           cudaStream_t st, int *n, int visc_var = 0) {
   if (p.viscous_order == 8 || p.viscous_order == 4) return launch_viscous8(z, p, th, faces, n_face, z.fvis8, st, n);
-  return th ? launch_viscous_mix(z, p, *th, st, n) : launch_viscous_air(z, p, st, n);
+  return th ? launch_viscous_mix(z, p, *th, st, n) : launch_viscous_air(z, p, st, n, visc_var);
 }
 
 int validate(const cfk_param *p, std::string &why) {
@@ -524,7 +525,7 @@ int cfk_compute_viscous_flux(cfk_ctx *c, void *stream) {
   if (c->hp.viscous_order == 0) return CFK_OK;
   if (int r = need_mech_for_mixture(c)) return r;
   int n = 0;
-  CFK_CHECK(c, launch_viscous(c->z, c->p, thermo_host(c), c->hp.faces, c->hp.n_face, S(stream), &n),
+  CFK_CHECK(c, launch_viscous(c->z, c->p, thermo_host(c), c->hp.faces, c->hp.n_face, S(stream), &n, c->visc_var),
             "viscous flux");
   c->launches += n;
   return CFK_OK;
@@ -602,13 +603,45 @@ int cfk_autotune_tiles(cfk_ctx *c, int reps, double *ms_out, int *choice_out, vo
       c->launches += reps + 1;
     }
   }
+  // the two forms of the fused air viscous kernel (staged, ring)
+  int visc_choice = c->visc_var;
+  if (e == cudaSuccess && !th && c->p.viscous_order == 2) {
+    double best = 1e300;
+    for (int var = 0; var < 2 && e == cudaSuccess; ++var) {
+      int nl = 0;
+      e = launch_viscous_air(zt, pt, st, &nl, var);  // warm-up
+      if (e == cudaSuccess) e = cudaEventRecord(a, st);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) e = launch_viscous_air(zt, pt, st, &nl, var);
+      if (e == cudaSuccess) e = cudaEventRecord(b, st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(b);
+      float ms = 0;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+      if (e == cudaSuccess && ms / reps < best) { best = ms / reps; visc_choice = var; }
+      c->visc_ms[var] = ms / reps;
+      c->launches += nl;
+    }
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   cudaFree(scratch);
   if (e != cudaSuccess) return cuda_fail(c, e, "autotune");
+  c->visc_var = visc_choice;
   for (int d = 0; d < 3; ++d) c->tile_var[d] = choice[d];
   if (choice_out) for (int d = 0; d < 3; ++d) choice_out[d] = choice[d];
   if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  return CFK_OK;
+}
+
+int cfk_viscous_variant(cfk_ctx *c, int set, int *var, double *ms) {
+  if (!c || !var) return CFK_ERR_ARG;
+  if (set) {
+    if (*var != 0 && *var != 1) return fail(c, CFK_ERR_ARG, "viscous variant must be 0 or 1");
+    c->visc_var = *var;
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+  } else {
+    *var = c->visc_var;
+  }
+  if (ms) { ms[0] = c->visc_ms[0]; ms[1] = c->visc_ms[1]; }
   return CFK_OK;
 }
 
@@ -803,11 +836,17 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     n += 2;
     dt_dev = reinterpret_cast<const double *>(c->d_dt_bits);
   }
+  // the properties of the nodes the boundary conditions cannot change are
+  // computed by the update kernel; the pass after the boundary conditions
+  // covers the rest (the ghost layers and the outermost interior layer).
+  // limit_flow rewrites interior nodes after the update, so with it the
+  // properties stay one pass over the padded block.
+  const bool fuse_props = !p.limit_flow;
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order > 0) {
       PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
-      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
+      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n, c->visc_var), "viscous flux");
     }
     if (c->have_mech && p.n_reac > 0) {
       // explicit chemical source of a reacting mixture (reference src/RK.cuh:147-149)
@@ -820,7 +859,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_UPDATE, st, &n);
-      CFK_CHECK(c, launch_update_rk(z, p, th, c->hp.dt, dt_dev, rk, c->d_err, st), "update");
+      CFK_CHECK(c, launch_update_rk(z, p, th, c->hp.dt, dt_dev, rk, c->d_err, st, false, fuse_props), "update");
       ++n;
       if (p.limit_flow) {
         // limit_flow<M> after the update (reference src/RK.cuh:163-164)
@@ -836,7 +875,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_PROPS, st, &n);
-      CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
+      CFK_CHECK(c, launch_update_properties(z, p, th, st, fuse_props), "properties");
       ++n;
     }
   }
@@ -912,7 +951,7 @@ static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *
   CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
   if (p.viscous_order > 0) {
     PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
-    CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
+    CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n, c->visc_var), "viscous flux");
   }
   {
     PhaseScope ps(c, CFK_PH_INVISCID, st, &n);
@@ -959,7 +998,7 @@ static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order > 0) {
       PhaseScope ps(c, CFK_PH_VISCOUS, st, &n);
-      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n), "viscous flux");
+      CFK_CHECK(c, launch_viscous(z, p, thermo_host(c), c->hp.faces, c->hp.n_face, st, &n, c->visc_var), "viscous flux");
     }
     {
       PhaseScope ps(c, CFK_PH_INVISCID, st, &n);

@@ -26,12 +26,36 @@ __constant__ double kRkB[3] = {0.0, 0.25, 2.0 / 3.0};
 __constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
 
 // ---------------------------------------------------------------------------
+// update_physical_properties (reference src/FieldOperation.cuh:86-120) of one
+// node: Sutherland viscosity and Mach number for air; the mixture branch also
+// computes the mixture-averaged transport properties (reference
+// src/Transport.cu:43-165).
+// ---------------------------------------------------------------------------
+template <bool MIX>
+__device__ __forceinline__ void properties_point(const Zone &z, const Param &p, const Thermo *th, int64_t id) {
+  const int64_t sz = z.d.plane(z.d.ngg);
+  const double t = z.bv[id + 5 * sz];
+  const double V = norm3d(z.bv[id + sz], z.bv[id + 2 * sz], z.bv[id + 3 * sz]);
+  if (MIX) {
+    mixture_properties_point(z, p, th, id, t, V);
+  } else {
+    constexpr double c_temp = kGammaAir * kRu / kMwAir;
+    z.mul[id] = sutherland(t);
+    if (z.mach) z.mach[id] = V / sqrt(c_temp * t);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // update_cv_and_bv_rk (reference src/RK.cuh:224-281).  dt comes from the
 // device scalar when dt_dev is non-null (CFL step computed on the device).
 // ---------------------------------------------------------------------------
 // With minus_cn the right-hand side is dq - Cn: update_cv_and_bv_rk_wu
 // (reference src/StrangSplitting.cu:504-562).
-template <bool MIX>
+// PROPS: the node's physical properties (update_physical_properties, below)
+// are computed here from the values just written, so that after the boundary
+// conditions only the nodes they can change need the separate pass
+// (update_physical_properties_kernel with shell = true).
+template <bool MIX, bool PROPS>
 __global__ void __launch_bounds__(256) update_cv_and_bv_rk_kernel(Zone z, Param p, const Thermo *th, double dt_host,
                                                                   const double *dt_dev, int rk, int *err,
                                                                   bool minus_cn) {
@@ -89,6 +113,7 @@ __global__ void __launch_bounds__(256) update_cv_and_bv_rk_kernel(Zone z, Param 
     z.bv[id + 5 * sz] = pres * kMwAir * density_inv / kRu;
   }
   for (int l = 0; l < nv; ++l) z.cv[id + l * sz] = cvl[l];
+  if (PROPS) properties_point<MIX>(z, p, th, id);
 }
 
 template <bool MIX>
@@ -182,7 +207,7 @@ __global__ void limit_flow_fix_kernel(Zone z, Param p, const Thermo *th, const u
 // transport properties (reference src/Transport.cu:43-165).
 // ---------------------------------------------------------------------------
 template <bool MIX>
-__global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo *th) {
+__global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo *th, bool shell) {
   const Dims d = z.d;
   const int g = d.ngg;
   int i, j;
@@ -190,17 +215,13 @@ __global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo 
   i -= g;
   j -= g;
   const int k = blockIdx.y - g;
-  const int64_t sz = d.plane(g);
-  const int64_t id = d.idx(g, i, j, k);
-  const double t = z.bv[id + 5 * sz];
-  const double V = norm3d(z.bv[id + sz], z.bv[id + 2 * sz], z.bv[id + 3 * sz]);
-  if (MIX) {
-    mixture_properties_point(z, p, th, id, t, V);
-  } else {
-    constexpr double c_temp = kGammaAir * kRu / kMwAir;
-    z.mul[id] = sutherland(t);
-    if (z.mach) z.mach[id] = V / sqrt(c_temp * t);
-  }
+  // shell: only the nodes the boundary conditions, the inner-face and halo
+  // assignments and the 2-D k-ghost copy can write — the ghost layers and the
+  // outermost interior layer; the update computed the others' properties
+  if (shell && i >= 1 && i <= d.mx - 2 && j >= 1 && j <= d.my - 2 &&
+      (d.mz == 1 ? k == 0 : (k >= 1 && k <= d.mz - 2)))
+    return;
+  properties_point<MIX>(z, p, th, d.idx(g, i, j, k));
 }
 
 // ---------------------------------------------------------------------------
@@ -758,11 +779,15 @@ static dim3 padded_grid(const Dims &d, int tpb) {
 }
 
 cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, double dt, const double *dt_dev,
-                             int rk, int *err, cudaStream_t st, bool minus_cn) {
-  if (p.n_spec > 0)
-    update_cv_and_bv_rk_kernel<true><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
-  else
-    update_cv_and_bv_rk_kernel<false><<<interior_grid(z.d, 128), 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
+                             int rk, int *err, cudaStream_t st, bool minus_cn, bool with_props) {
+  const dim3 grid = interior_grid(z.d, 128);
+  if (p.n_spec > 0) {
+    if (with_props) update_cv_and_bv_rk_kernel<true, true><<<grid, 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
+    else update_cv_and_bv_rk_kernel<true, false><<<grid, 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
+  } else {
+    if (with_props) update_cv_and_bv_rk_kernel<false, true><<<grid, 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
+    else update_cv_and_bv_rk_kernel<false, false><<<grid, 128, 0, st>>>(z, p, th, dt, dt_dev, rk, err, minus_cn);
+  }
   return cudaGetLastError();
 }
 
@@ -780,9 +805,9 @@ cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st) {
-  if (p.n_spec > 0) update_physical_properties_kernel<true><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
-  else update_physical_properties_kernel<false><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th);
+cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, bool shell) {
+  if (p.n_spec > 0) update_physical_properties_kernel<true><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th, shell);
+  else update_physical_properties_kernel<false><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th, shell);
   return cudaGetLastError();
 }
 

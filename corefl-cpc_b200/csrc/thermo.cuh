@@ -29,8 +29,10 @@ struct Thermo {
 };
 
 __host__ __device__ inline double sutherland(double t) {
-  // reference src/Transport.cu:6-9
-  return 1.7894e-5 * pow(t / 288.16, 1.5) * (288.16 + 110) / (t + 110);
+  // reference src/Transport.cu:6-9; (T/288.16)^1.5 as x sqrt(x) (correctly
+  // rounded sqrt and one product) instead of the general power function
+  const double x = t / 288.16;
+  return 1.7894e-5 * (x * sqrt(x)) * (288.16 + 110) / (t + 110);
 }
 
 __device__ __forceinline__ void compute_enthalpy_and_cp(const Thermo *th, double t, double *h, double *cp) {
@@ -151,7 +153,8 @@ __device__ __forceinline__ void mixture_properties_point(const Zone &z, const Pa
   for (int l = 0; l < ns; ++l) {
     X[l] = yk[l] * mw_total / th->mw[l];
     const double t_dl = temperature * th->LJ_potent_inv[l];
-    vis_denom[l] = th->vis_coeff[l] * temp / (1.147 * pow(t_dl, -0.145) + pow(t_dl + 0.5, -2));
+    const double t5 = t_dl + 0.5;  // (t_dl + 0.5)^-2 as a reciprocal square, not the general power
+    vis_denom[l] = th->vis_coeff[l] * temp / (1.147 * pow(t_dl, -0.145) + 1.0 / (t5 * t5));
   }
   const double t_3over2_over_p = temperature * temp;
   double viscosity = 0, conductivity = 0;

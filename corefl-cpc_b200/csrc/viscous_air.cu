@@ -221,16 +221,220 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
   }
 }
 
-// Opt the kernel in to its dynamic shared-memory size (108 KB, two CTAs per SM).
-cudaError_t viscous_air_init_attributes() {
-  return cudaFuncSetAttribute(viscous_air_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FusedSmem));
+// Ring variant: the same tile, march and arithmetic, with only the dynamic
+// values (u, v, w, T, mu) staged in shared memory, in a ring of three plane
+// slots filled by cp.async: plane k+2 is requested before the faces of plane
+// k are computed and lands while they run, so the loads never stall a warp.
+// The metric and J (read-only) come through L1 from global memory.  70 KB of
+// shared memory per CTA, two CTAs per SM, two barriers per plane.  The face
+// flux is term for term that of staged_face, so both variants give the same
+// bits.
+namespace {
+constexpr int kRV = 5;  // u v w T mu
+
+struct RingSmem {
+  double dyn[3][kRV][kPY][kPX];  // planes k-1, k, k+1 (slots rotate; one is refilled with k+2)
+  double dzp[4][kPY][kPX];       // f(k+1) - f(k-1) of u, v, w, T on plane k
+  double fx[4][kFY][kFX + 1];
+  double fy[4][kFY + 1][kFX];
+};
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// staged_face with the metric and J of the two nodes (global indices ida, idb) read from global memory.
+template <int DIR>
+__device__ __forceinline__ void ring_face(const RingSmem &S, const double *__restrict__ met,
+                                          const double *__restrict__ jac, int64_t sz, int sa, int pa, int qa,
+                                          int64_t ida, int sb, int pb, int qb, int64_t idb, double Pr, double F[4]) {
+  const auto &A = S.dyn[sa];
+  const auto &B = S.dyn[sb];
+  auto tdiff = [&](const double (&p)[kRV][kPY][kPX], int D, int q, int px, int py) -> double {
+    if (D == 0) return p[q][py][px + 1] - p[q][py][px - 1];
+    if (D == 1) return p[q][py + 1][px] - p[q][py - 1][px];
+    return S.dzp[q][py][px];
+  };
+  constexpr int TLO = DIR == 0 ? 1 : 0, THI = DIR == 2 ? 1 : 2;
+  double gm[9];
+#pragma unroll
+  for (int l = 0; l < 9; ++l) gm[l] = 0.5 * (__ldg(met + ida + l * sz) + __ldg(met + idb + l * sz));
+  double dd[4][3];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    dd[q][DIR] = B[q][qb][pb] - A[q][qa][pa];
+    dd[q][TLO] = 0.25 * (tdiff(A, TLO, q, pa, qa) + tdiff(B, TLO, q, pb, qb));
+    dd[q][THI] = 0.25 * (tdiff(A, THI, q, pa, qa) + tdiff(B, THI, q, pb, qb));
+  }
+  const double u_x = dd[0][0] * gm[0] + dd[0][1] * gm[3] + dd[0][2] * gm[6];
+  const double u_y = dd[0][0] * gm[1] + dd[0][1] * gm[4] + dd[0][2] * gm[7];
+  const double u_z = dd[0][0] * gm[2] + dd[0][1] * gm[5] + dd[0][2] * gm[8];
+  const double v_x = dd[1][0] * gm[0] + dd[1][1] * gm[3] + dd[1][2] * gm[6];
+  const double v_y = dd[1][0] * gm[1] + dd[1][1] * gm[4] + dd[1][2] * gm[7];
+  const double v_z = dd[1][0] * gm[2] + dd[1][1] * gm[5] + dd[1][2] * gm[8];
+  const double w_x = dd[2][0] * gm[0] + dd[2][1] * gm[3] + dd[2][2] * gm[6];
+  const double w_y = dd[2][0] * gm[1] + dd[2][1] * gm[4] + dd[2][2] * gm[7];
+  const double w_z = dd[2][0] * gm[2] + dd[2][1] * gm[5] + dd[2][2] * gm[8];
+  const double t_x = dd[3][0] * gm[0] + dd[3][1] * gm[3] + dd[3][2] * gm[6];
+  const double t_y = dd[3][0] * gm[1] + dd[3][1] * gm[4] + dd[3][2] * gm[7];
+  const double t_z = dd[3][0] * gm[2] + dd[3][1] * gm[5] + dd[3][2] * gm[8];
+  const double mul = 0.5 * (A[4][qa][pa] + B[4][qb][pb]);
+  const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+  const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+  const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double tau_xy = mul * (u_y + v_x);
+  const double tau_xz = mul * (u_z + w_x);
+  const double tau_yz = mul * (v_z + w_y);
+  const double ja = __ldg(jac + ida), jb = __ldg(jac + idb);
+  const double gk0 = 0.5 * (__ldg(met + ida + (3 * DIR) * sz) * ja + __ldg(met + idb + (3 * DIR) * sz) * jb);
+  const double gk1 = 0.5 * (__ldg(met + ida + (3 * DIR + 1) * sz) * ja + __ldg(met + idb + (3 * DIR + 1) * sz) * jb);
+  const double gk2 = 0.5 * (__ldg(met + ida + (3 * DIR + 2) * sz) * ja + __ldg(met + idb + (3 * DIR + 2) * sz) * jb);
+  F[0] = gk0 * tau_xx + gk1 * tau_xy + gk2 * tau_xz;
+  F[1] = gk0 * tau_xy + gk1 * tau_yy + gk2 * tau_yz;
+  F[2] = gk0 * tau_xz + gk1 * tau_yz + gk2 * tau_zz;
+  const double um = 0.5 * (A[0][qa][pa] + B[0][qb][pb]);
+  const double vm = 0.5 * (A[1][qa][pa] + B[1][qb][pb]);
+  const double wm = 0.5 * (A[2][qa][pa] + B[2][qb][pb]);
+  constexpr double cp = kGammaAir * kRAir / (kGammaAir - 1);
+  const double conductivity = mul / Pr * cp;
+  F[3] = um * F[0] + vm * F[1] + wm * F[2] + conductivity * (gk0 * t_x + gk1 * t_y + gk2 * t_z);
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kFT, 2) viscous_air_ring(Zone z, double Pr) {
+  extern __shared__ __align__(16) double rsm[];
+  RingSmem &S = *reinterpret_cast<RingSmem *>(rsm);
+  const Dims d = z.d;
+  const int g = d.ngg;
+  const int64_t sz = d.plane(g), szq = d.plane(0);
+  const int64_t srow = d.stride(g, 1), spl = d.stride(g, 2);
+  const int i0 = blockIdx.x * kFX, j0 = blockIdx.y * kFY, k0 = blockIdx.z * kFZ;
+  const int tx = threadIdx.x % kFX, ty = threadIdx.x / kFX;
+  const bool three_d = d.mz > 1;
+  const int k_end = min(k0 + kFZ, d.mz);
+  const double *__restrict__ met = z.metric;
+  const double *__restrict__ jac = z.jac;
+
+  auto point_ok = [&](int p, int &px, int &py) {
+    py = p / kPX;
+    px = p - py * kPX;
+    return p < kPX * kPY && i0 - 1 + px <= d.mx && j0 - 1 + py <= d.my;
+  };
+  // this thread's points of plane k into slot sl (the same points every plane)
+  auto request = [&](int k, int sl) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      int px, py;
+      if (!point_ok(threadIdx.x + r * kFT, px, py)) continue;
+      const int64_t id = d.idx(g, i0 - 1 + px, j0 - 1 + py, k);
+      cp_async8(&S.dyn[sl][0][py][px], z.bv + id + sz);
+      cp_async8(&S.dyn[sl][1][py][px], z.bv + id + 2 * sz);
+      cp_async8(&S.dyn[sl][2][py][px], z.bv + id + 3 * sz);
+      cp_async8(&S.dyn[sl][3][py][px], z.bv + id + 5 * sz);
+      cp_async8(&S.dyn[sl][4][py][px], z.mul + id);
+    }
+  };
+  request(k0 - 1, 0);
+  request(k0, 1);
+  request(k0 + 1, 2);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  const bool mine = i < d.mx && j < d.my;
+  double fzp[4] = {0, 0, 0, 0};
+  if (three_d && mine) {
+    const int64_t ida = d.idx(g, i, j, k0 - 1);
+    ring_face<2>(S, met, jac, sz, 0, tx + 1, ty + 1, ida, 1, tx + 1, ty + 1, ida + spl, Pr, fzp);
+  }
+  int sp = 0, sc = 1, sn = 2;  // slots of planes k-1, k, k+1
+  for (int k = k0; k < k_end; ++k) {
+    double acc[4];
+    const int64_t iq = d.idx(0, i, j, k);
+    if (mine) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q] = z.dq[iq + (q + 1) * szq];
+    }
+    // k-differences at this thread's points: its own copies of planes k-1
+    // and k+1 are complete, and no other thread reads these points of
+    // slot sp before the next barrier
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      int px, py;
+      if (!point_ok(threadIdx.x + r * kFT, px, py)) continue;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) S.dzp[q][py][px] = S.dyn[sn][q][py][px] - S.dyn[sp][q][py][px];
+    }
+    if (k + 2 <= k_end) request(k + 2, sp);  // plane k+2 into the slot of plane k-1
+    cp_async_commit();
+    __syncthreads();
+    constexpr int kNXF = kFY * (kFX + 1), kNYF = (kFY + 1) * kFX;
+    constexpr int kYF0 = (kNXF + 31) / 32 * 32;
+    for (int f = threadIdx.x; f < kYF0 + kNYF; f += kFT) {
+      if (f < kYF0) {
+        if (f >= kNXF) continue;
+        const int fy_ = f / (kFX + 1), fx_ = f - fy_ * (kFX + 1);
+        if (i0 - 1 + fx_ > d.mx - 1 || j0 + fy_ >= d.my) continue;
+        const int64_t ida = d.idx(g, i0 - 1 + fx_, j0 + fy_, k);
+        double F[4];
+        ring_face<0>(S, met, jac, sz, sc, fx_, fy_ + 1, ida, sc, fx_ + 1, fy_ + 1, ida + 1, Pr, F);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) S.fx[q][fy_][fx_] = F[q];
+      } else {
+        const int e = f - kYF0;
+        const int fy_ = e / kFX, fx_ = e - fy_ * kFX;
+        if (i0 + fx_ >= d.mx || j0 - 1 + fy_ > d.my - 1) continue;
+        const int64_t ida = d.idx(g, i0 + fx_, j0 - 1 + fy_, k);
+        double F[4];
+        ring_face<1>(S, met, jac, sz, sc, fx_ + 1, fy_, ida, sc, fx_ + 1, fy_ + 1, ida + srow, Pr, F);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) S.fy[q][fy_][fx_] = F[q];
+      }
+    }
+    double fzn[4] = {0, 0, 0, 0};
+    if (three_d && mine) {
+      const int64_t ida = d.idx(g, i, j, k);
+      ring_face<2>(S, met, jac, sz, sc, tx + 1, ty + 1, ida, sn, tx + 1, ty + 1, ida + spl, Pr, fzn);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (mine) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double a = acc[q];
+        a += S.fx[q][ty][tx + 1] - S.fx[q][ty][tx];
+        a += S.fy[q][ty + 1][tx] - S.fy[q][ty][tx];
+        if (three_d) a += fzn[q] - fzp[q];
+        z.dq[iq + (q + 1) * szq] = a;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) fzp[q] = fzn[q];
+    const int t = sp;
+    sp = sc;
+    sc = sn;
+    sn = t;
+  }
 }
 
-// compute_viscous_flux for air (reference src/ViscousScheme.cu:7-40): one launch for all directions.
-cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch) {
+// Opt the kernel in to its dynamic shared-memory size (108 KB, two CTAs per SM).
+cudaError_t viscous_air_init_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(viscous_air_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(FusedSmem));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(viscous_air_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
+}
+
+// compute_viscous_flux for air (reference src/ViscousScheme.cu:7-40): one
+// launch for all directions; var 0 the staged kernel, 1 the ring kernel.
+cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch, int var) {
   const Dims &d = z.d;
   const dim3 grid((d.mx + kFX - 1) / kFX, (d.my + kFY - 1) / kFY, (d.mz + kFZ - 1) / kFZ);
-  viscous_air_fused<<<grid, kFT, sizeof(FusedSmem), st>>>(z, p.Pr);
+  if (var == 1) viscous_air_ring<<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
+  else viscous_air_fused<<<grid, kFT, sizeof(FusedSmem), st>>>(z, p.Pr);
   *n_launch += 1;
   return cudaGetLastError();
 }

@@ -240,6 +240,14 @@ int cfk_compute_shock_sensor(cfk_ctx *ctx, void *stream);
  * capture.  A no-op for the primitive-variable schemes (one tile shape). */
 #define CFK_TILE_VARIANTS 3
 int cfk_autotune_tiles(cfk_ctx *ctx, int reps, double *ms_out, int *choice_out, void *stream);
+/* For air with viscous_order 2, cfk_autotune_tiles also times the two forms of
+ * the fused viscous kernel — 0: all per-node inputs staged in shared memory
+ * (two plane slots); 1: only u, v, w, T, mu staged, in a three-slot ring
+ * filled by cp.async ahead of use, with the metric read through L1 — and
+ * keeps the faster (both give the same bits).  cfk_viscous_variant reads
+ * (set = 0) or sets (set = 1) the form in *var; ms (optional, 2 doubles)
+ * receives the last autotune's times per launch. */
+int cfk_viscous_variant(cfk_ctx *ctx, int set, int *var, double *ms);
 /* Sets the tile variant of each sweep (var[3], each 0..CFK_TILE_VARIANTS-1). */
 int cfk_set_tile_variants(cfk_ctx *ctx, const int *var);
 /* SSP-RK3 stage update of cv and bv/sv.  Replaces update_cv_and_bv_rk<M>

@@ -99,3 +99,32 @@ def test_autotune_mixture_and_pv_noop():
     pv = GpuZone(cases.sod(64, 7, scheme=4))
     choice, ms = pv.ctx.autotune_tiles(reps=2)
     assert choice == [0, 0, 0] and all(t == 0 for row in ms for t in row)
+
+
+@pytest.mark.parametrize("name", ["wave_3d", "walls_3d", "tube_2d"])
+def test_viscous_forms_identical_and_in_parity(name):
+    """The staged and the cp.async-ring forms of the fused air viscous kernel
+    give the same bits (blocks not a multiple of the 32 x 8 x 32 tile, 2-D and
+    3-D, walls widening the boundary ranges) and match the oracle's viscous
+    flux at the single-call bar."""
+    if name == "wave_3d":
+        case = cases.perturbed(cases.sine_wave(n=41, ny=37, nz=35, scheme=52, amp=0.2), seed=5, amp=0.3)
+    elif name == "walls_3d":
+        case = cases.with_walls(cases.perturbed(cases.sine_wave(n=33, ny=19, nz=13, scheme=72), seed=6, amp=0.1))
+    else:
+        case = cases.sod(70, 11, scheme=52, viscous_order=2)
+    oz = pyoracle.OracleZone(case)
+    oz.initialize()
+    oz.call("orc_compute_viscous_flux")
+    gz = GpuZone(case)
+    gz.initialize()
+    out = []
+    for v in (0, 1):
+        gz.t["dq"].zero_()
+        gz.ctx.viscous_variant(v)
+        gz.ctx.viscous()
+        out.append(gz.get("dq"))
+    assert np.array_equal(out[0], out[1])
+    assert rel_err(out[1][1:], oz["dq"][1:], momentum=(0, 1, 2)) <= 1e-11
+    var, ms = gz.ctx.viscous_variant()
+    assert var == 1

@@ -230,7 +230,7 @@ def test_trained_surrogate_throughput_on_burnt_mix(trained):
     still integrates the judged and reverted burnt nodes with the plain
     integrator, whose serial substep chain (~1800 substeps) bounds the step
     time from below whatever the node count, while the plain step grows with
-    the node count: at this size the bar is 1.5x (the benchmark measures
+    the node count: at this size the bar is 1.7x (measured 1.9x; the benchmark measures
     2^20 nodes)."""
     torch = pytest.importorskip("torch")
     n, dt = 131072, 1e-7
@@ -260,4 +260,4 @@ def test_trained_surrogate_throughput_on_burnt_mix(trained):
         ms[mode] = e0.elapsed_time(e1)
     print(f"plain {ms['plain']:.1f} ms, surrogate {ms['surrogate']:.1f} ms, "
           f"speed-up {ms['plain'] / ms['surrogate']:.2f}x")
-    assert ms["plain"] / ms["surrogate"] >= 1.5
+    assert ms["plain"] / ms["surrogate"] >= 1.7
