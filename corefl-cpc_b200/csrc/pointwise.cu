@@ -233,12 +233,15 @@ __global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo 
 // with_reaction = false: local_time_step_without_reaction (reference
 // src/TimeAdvanceFunc.cu:21-100), the step of Wu's splitting.
 template <bool MIX>
+// Each CTA walks the planes k = blockIdx.y, + gridDim.y, ... so that the
+// grid minimum costs one atomic per CTA of several planes, not per plane.
 __global__ void __launch_bounds__(256) local_time_step_kernel(Zone z, Param p, const Thermo *th,
                                                               unsigned long long *dt_min_bits, bool with_reaction) {
   const Dims d = z.d;
   int i, j;
   const bool node = flat_ij(d.mx, d.my, i, j);
-  const int k = blockIdx.y;
+  double dt_cta = 1e6;
+  for (int k = blockIdx.y; k < d.mz; k += gridDim.y) {
   double dt = 1e6;
   if (node) {
     const int g = d.ngg;
@@ -277,6 +280,9 @@ __global__ void __launch_bounds__(256) local_time_step_kernel(Zone z, Param p, c
     }
     if (z.dt_local) z.dt_local[d.idx(0, i, j, k)] = dt;
   }
+  dt_cta = min(dt_cta, dt);
+  }
+  double dt = dt_cta;
   for (int o = 16; o > 0; o >>= 1) dt = min(dt, __shfl_xor_sync(0xffffffffu, dt, o));
   __shared__ double wmin[8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -814,10 +820,12 @@ cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
                             cudaStream_t st, bool with_reaction) {
   reset_dt_kernel<<<1, 1, 0, st>>>(dt_bits);
+  dim3 grid = interior_grid(z.d, 256);
+  grid.y = grid.y < 16 ? grid.y : 16;  // planes per CTA: ceil(mz / 16)
   if (p.n_spec > 0)
-    local_time_step_kernel<true><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits, with_reaction);
+    local_time_step_kernel<true><<<grid, 256, 0, st>>>(z, p, th, dt_bits, with_reaction);
   else
-    local_time_step_kernel<false><<<interior_grid(z.d, 256), 256, 0, st>>>(z, p, th, dt_bits, with_reaction);
+    local_time_step_kernel<false><<<grid, 256, 0, st>>>(z, p, th, dt_bits, with_reaction);
   return cudaGetLastError();
 }
 
