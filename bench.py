@@ -467,14 +467,14 @@ def surrogate_flow_bench(args, local):
     small = cases.reflected_shock_tube(mech, nx, ny, length=0.02, height=0.004, mach=2.6)
     n = small.N
     traces, rows = {}, None
-    for mode in ("plain", "surrogate"):
+    for mode in ("plain", "surrogate", "surrogate_all"):
         ctx, zone = _flow_ctx(mech, small, local, 7)
         if mode == "plain":
             X = torch.empty((W * n, sg.cf.SG_NIN), dtype=torch.float32, device=dev)
             G = torch.empty((W * n, sg.cf.SG_NOUT), dtype=torch.float32, device=dev)
         else:
             ctx.surrogate_set_params(weights, norm)
-            gate = ctx.surrogate_default_gate()
+            gate = ctx.surrogate_default_gate(**GATES[mode])
         Tpad = torch.empty(small.P, dtype=torch.float64, device=dev)
         Tint = Tpad.view(small.shape())[small.ngg:small.ngg + 1, small.ngg:small.ngg + ny, small.ngg:small.ngg + nx]
         peak = torch.empty(W, dtype=torch.float64, device=dev)
@@ -513,16 +513,17 @@ def surrogate_flow_bench(args, local):
         return 0.5 * (tt[k] + (tt[k - 1] if k else 0.0)), float(pk.max())
 
     tau_p, pk_p = ignition(traces["plain"])
-    tau_s, pk_s = ignition(traces["surrogate"])
-    st = traces["surrogate"][3]
     out["ignition_window"] = {
         "case": f"{nx}x{ny} tube 0.02 x 0.004 m, Mach 2.6 incident shock into 0.1 atm / 300 K, {W} steps "
                 f"({traces['plain'][0][-1] * 1e6:.1f} us)",
-        "tau_ign_plain_s": tau_p, "tau_ign_surrogate_s": tau_s, "tau_ign_rel_err": abs(tau_s - tau_p) / tau_p,
-        "T_peak_plain_K": pk_p, "T_peak_surrogate_K": pk_s, "T_peak_rel_err": abs(pk_s - pk_p) / pk_p,
-        "on_network": sum(x["surrogate"] for x in st) / max(sum(x["cells"] for x in st), 1),
-        "plain_window_ms": traces["plain"][2], "surrogate_window_ms": traces["surrogate"][2],
+        "tau_ign_plain_s": tau_p, "T_peak_plain_K": pk_p, "plain_window_ms": traces["plain"][2],
         "note": "the plain window includes recording the training rows"}
+    for mode in ("surrogate", "surrogate_all"):
+        tau_s, pk_s = ignition(traces[mode])
+        out["ignition_window"][mode] = {
+            "gate": GATES[mode] or "default", "tau_ign_s": tau_s, "tau_ign_rel_err": abs(tau_s - tau_p) / tau_p,
+            "T_peak_K": pk_s, "T_peak_rel_err": abs(pk_s - pk_p) / pk_p, "window_ms": traces[mode][2],
+            **_stat_summary(traces[mode][3])}
 
     # 2. the 2048 x 512 tube
     big = cases.reflected_shock_tube(mech, args.sflow_nx, args.sflow_ny)
@@ -534,7 +535,23 @@ def surrogate_flow_bench(args, local):
     return out
 
 
-def _plain_vs_surrogate(mech, case, local, weights, norm, K, modes=("plain", "surrogate")):
+GATES = {"surrogate": {}, "surrogate_all": {"min_substeps": 0.0}}
+
+
+def _stat_summary(stats):
+    """Fraction of node-steps on the network and the fallback reasons, summed
+    over the sampled steps."""
+    if not stats:
+        return {}
+    cells = sum(x["cells"] for x in stats)
+    out = {"on_network": sum(x["surrogate"] for x in stats) / max(cells, 1)}
+    for k in stats[0]:
+        if k.startswith("fallback_") or k in ("judged", "judge_failed"):
+            out[k] = sum(x[k] for x in stats) / max(cells, 1)
+    return out
+
+
+def _plain_vs_surrogate(mech, case, local, weights, norm, K, modes=("plain", "surrogate", "surrogate_all")):
     """K Wu-splitting steps of `case` from its initial state with the plain
     point-implicit reaction sub-step and with the gated surrogate (and, with
     "rk3" in modes, K RK3 steps with the explicit chemical source replayed as
@@ -549,7 +566,7 @@ def _plain_vs_surrogate(mech, case, local, weights, norm, K, modes=("plain", "su
         for timed in (False, True):
             ctx, zone = _flow_ctx(mech, case, local, 7)
             ctx.surrogate_set_params(weights, norm)
-            gate = ctx.surrogate_default_gate()
+            gate = ctx.surrogate_default_gate(**GATES.get(mode, {}))
             n = K if timed else 2
             if timed:
                 ctx.set_profiling(mode != "rk3")
@@ -582,20 +599,25 @@ def _plain_vs_surrogate(mech, case, local, weights, norm, K, modes=("plain", "su
                 r["reaction_ms_per_step"] = ph["reaction"][0] / K
                 r["phases_ms_per_step"] = {k: v[0] / K for k, v in ph.items()}
             if stats:
-                r["on_network"] = sum(x["surrogate"] for x in stats) / sum(x["cells"] for x in stats)
+                r.update(_stat_summary(stats))
                 r["fallback_fraction"] = 1.0 - r["on_network"]
             res[mode] = r
             finals[mode] = (_interior_plane(ctx, zone, case, "bv", 5), _interior_plane(ctx, zone, case, "sv", oh))
             ctx.close()
     Tp, OHp = finals["plain"]
-    Ts, OHs = finals["surrogate"]
     out = dict(res)
-    out.update({
-        "speedup_step": res["surrogate"]["cell_updates_per_s"] / res["plain"]["cell_updates_per_s"],
-        "speedup_reaction": res["plain"]["reaction_ms_per_step"] / max(res["surrogate"]["reaction_ms_per_step"], 1e-9),
-        "mean_T_rel_err": float(abs(Ts.mean() - Tp.mean()) / Tp.mean()),
-        "max_T_abs_err_K": float(np.abs(Ts - Tp).max()),
-        "mean_Y_OH_abs_err": float(np.abs(OHs - OHp).mean()), "max_Y_OH_plain": float(OHp.max())})
+    for mode in modes:
+        if not mode.startswith("surrogate"):
+            continue
+        Ts, OHs = finals[mode]
+        out[mode].update({
+            "gate": GATES[mode] or "default",
+            "speedup_step": res[mode]["cell_updates_per_s"] / res["plain"]["cell_updates_per_s"],
+            "speedup_reaction": res["plain"]["reaction_ms_per_step"] / max(res[mode]["reaction_ms_per_step"], 1e-9),
+            "mean_T_rel_err": float(abs(Ts.mean() - Tp.mean()) / Tp.mean()),
+            "max_T_abs_err_K": float(np.abs(Ts - Tp).max()),
+            "mean_Y_OH_abs_err": float(np.abs(OHs - OHp).mean())})
+    out["max_Y_OH_plain"] = float(OHp.max())
     return out
 
 
@@ -631,7 +653,7 @@ def mixing_layer_bench(args, local):
     del X, G
     big = cases.mixing_layer(mech, args.ml_nx, args.ml_ny, args.ml_nz)
     K = args.ml_steps
-    r = _plain_vs_surrogate(mech, big, local, weights, norm, K, modes=("plain", "surrogate", "rk3"))
+    r = _plain_vs_surrogate(mech, big, local, weights, norm, K, modes=("plain", "surrogate", "surrogate_all", "rk3"))
     r["case"] = (f"{big.mx}x{big.my}x{big.mz} mixing layer 0.05 x 0.025 x 0.0125 m (y clustered), {K} steps "
                  f"({r['plain']['simulated_s'] * 1e9:.1f} ns simulated)")
     r["training"] = {"case": f"{small.mx}x{small.my}x{small.mz}", "rows": W * n, "epochs": args.sflow_epochs,

@@ -316,6 +316,8 @@ def make_param(p: dict, faces) -> cfk_param:
         if k == "wall_yk":
             for l, y in enumerate(v):
                 cp.wall.yk[l] = y
+        elif k == "inflow_type":
+            cp.inflow.inflow_type = v
         elif k in ("inflow_sv", "inflow_sv_lower"):
             arr = getattr(cp.inflow, k[7:])
             for l, y in enumerate(v):

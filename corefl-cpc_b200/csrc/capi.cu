@@ -32,7 +32,7 @@ cudaError_t launch_update_rk(const Zone &z, const Param &p, const Thermo *th, do
                              int rk, int *err, cudaStream_t st, bool minus_cn = false, bool with_props = false);
 cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st);
 cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st,
-                                     bool shell = false);
+                                     bool shell = false, bool planar = false);
 cudaError_t launch_local_dt(const Zone &z, const Param &p, const Thermo *th, unsigned long long *dt_bits,
                             cudaStream_t st, bool with_reaction = true);
 cudaError_t launch_limit_flow(const Zone &z, const Param &p, const Thermo *th, unsigned char *bad,
@@ -839,9 +839,14 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
   // the properties of the nodes the boundary conditions cannot change are
   // computed by the update kernel; the pass after the boundary conditions
   // covers the rest (the ghost layers and the outermost interior layer).
-  // limit_flow rewrites interior nodes after the update, so with it the
-  // properties stay one pass over the padded block.
-  const bool fuse_props = !p.limit_flow;
+  // limit_flow rewrites interior nodes after the update, and the subsonic
+  // inflow of a mixture reads the acoustic speed of the stage before, so with
+  // either the properties stay one pass over the padded block after the
+  // boundary conditions.
+  bool bc_reads_props = false;
+  for (int f = 0; f < c->hp.n_face; ++f)
+    if (c->hp.faces[f].label == 5 && c->hp.inflow.subsonic && p.n_spec > 0) bc_reads_props = true;
+  const bool fuse_props = !p.limit_flow && !bc_reads_props;
   for (int rk = 0; rk < 3; ++rk) {
     CFK_CHECK(c, cudaMemsetAsync(z.dq, 0, N * p.n_var * sizeof(double), st), "dq memset");
     if (p.viscous_order > 0) {
@@ -875,7 +880,7 @@ static int rk3_step_async(cfk_ctx *c, cudaStream_t st) {
     }
     {
       PhaseScope ps(c, CFK_PH_PROPS, st, &n);
-      CFK_CHECK(c, launch_update_properties(z, p, th, st, fuse_props), "properties");
+      CFK_CHECK(c, launch_update_properties(z, p, th, st, fuse_props, true), "properties");
       ++n;
     }
   }
@@ -989,7 +994,7 @@ static int wu_splitting(cfk_ctx *c, int schedule, const WuReaction &rx, double *
   }
   {
     PhaseScope ps(c, CFK_PH_PROPS, st, &n);
-    CFK_CHECK(c, launch_update_properties(z, p, th, st), "properties");
+    CFK_CHECK(c, launch_update_properties(z, p, th, st, false, true), "properties");
     ++n;
   }
   // wu_RK_subStep (:564-634): SSP-RK3 over dt/2 on dq - Cn, no property update

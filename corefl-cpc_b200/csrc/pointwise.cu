@@ -206,22 +206,39 @@ __global__ void limit_flow_fix_kernel(Zone z, Param p, const Thermo *th, const u
 // the padded block.  The mixture branch also computes the mixture-averaged
 // transport properties (reference src/Transport.cu:43-165).
 // ---------------------------------------------------------------------------
+// planar (2-D blocks, inside the step drivers, after the k-ghost copy): the
+// k-ghost planes hold copies of plane k = 0, so their properties are those of
+// plane 0 — computed once on plane 0 and copied, instead of 2 ngg + 1 times.
 template <bool MIX>
-__global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo *th, bool shell) {
+__global__ void update_physical_properties_kernel(Zone z, Param p, const Thermo *th, bool shell, bool planar) {
   const Dims d = z.d;
   const int g = d.ngg;
   int i, j;
   if (!flat_ij(d.mx + 2 * g, d.my + 2 * g, i, j)) return;
   i -= g;
   j -= g;
-  const int k = blockIdx.y - g;
+  const int k = planar ? 0 : (int)blockIdx.y - g;
   // shell: only the nodes the boundary conditions, the inner-face and halo
   // assignments and the 2-D k-ghost copy can write — the ghost layers and the
   // outermost interior layer; the update computed the others' properties
-  if (shell && i >= 1 && i <= d.mx - 2 && j >= 1 && j <= d.my - 2 &&
-      (d.mz == 1 ? k == 0 : (k >= 1 && k <= d.mz - 2)))
-    return;
-  properties_point<MIX>(z, p, th, d.idx(g, i, j, k));
+  const bool inner = i >= 1 && i <= d.mx - 2 && j >= 1 && j <= d.my - 2 &&
+                     (d.mz == 1 ? k == 0 : (k >= 1 && k <= d.mz - 2));
+  const int64_t id = d.idx(g, i, j, k);
+  if (!(shell && inner)) properties_point<MIX>(z, p, th, id);
+  if (!planar) return;
+  const int64_t sz = d.plane(g), sk = d.stride(g, 2);
+  for (int q = -g; q <= g; ++q) {
+    if (q == 0) continue;
+    const int64_t o = id + q * sk;
+    z.mul[o] = z.mul[id];
+    if (z.mach) z.mach[o] = z.mach[id];
+    if (MIX) {
+      z.gamma[o] = z.gamma[id];
+      z.acoustic_speed[o] = z.acoustic_speed[id];
+      z.thermal_conductivity[o] = z.thermal_conductivity[id];
+      for (int l = 0; l < p.n_spec; ++l) z.rho_D[o + l * sz] = z.rho_D[id + l * sz];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -811,9 +828,13 @@ cudaError_t launch_cv_from_bv(const Zone &z, const Param &p, const Thermo *th, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, bool shell) {
-  if (p.n_spec > 0) update_physical_properties_kernel<true><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th, shell);
-  else update_physical_properties_kernel<false><<<padded_grid(z.d, 128), 128, 0, st>>>(z, p, th, shell);
+cudaError_t launch_update_properties(const Zone &z, const Param &p, const Thermo *th, cudaStream_t st, bool shell,
+                                     bool planar) {
+  dim3 grid = padded_grid(z.d, 128);
+  planar = planar && z.d.mz == 1;
+  if (planar) grid.y = 1;
+  if (p.n_spec > 0) update_physical_properties_kernel<true><<<grid, 128, 0, st>>>(z, p, th, shell, planar);
+  else update_physical_properties_kernel<false><<<grid, 128, 0, st>>>(z, p, th, shell, planar);
   return cudaGetLastError();
 }
 

@@ -227,8 +227,8 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
 // k are computed and lands while they run, so the loads never stall a warp.
 // The metric and J (read-only) come through L1 from global memory.  70 KB of
 // shared memory per CTA, two CTAs per SM, two barriers per plane.  The face
-// flux is term for term that of staged_face, so both variants give the same
-// bits.
+// flux is term for term that of staged_face (the compiler may contract its
+// products into FMAs differently, so the two agree to the last bits).
 namespace {
 constexpr int kRV = 5;  // u v w T mu
 

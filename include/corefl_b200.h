@@ -244,7 +244,7 @@ int cfk_autotune_tiles(cfk_ctx *ctx, int reps, double *ms_out, int *choice_out, 
  * the fused viscous kernel — 0: all per-node inputs staged in shared memory
  * (two plane slots); 1: only u, v, w, T, mu staged, in a three-slot ring
  * filled by cp.async ahead of use, with the metric read through L1 — and
- * keeps the faster (both give the same bits).  cfk_viscous_variant reads
+ * keeps the faster (the same arithmetic; they agree to the last bits).  cfk_viscous_variant reads
  * (set = 0) or sets (set = 1) the form in *var; ms (optional, 2 doubles)
  * receives the last autotune's times per launch. */
 int cfk_viscous_variant(cfk_ctx *ctx, int set, int *var, double *ms);

@@ -8,9 +8,14 @@ same state: with the plain point-implicit reaction sub-step, recording one
 training row per node per step from the reaction sub-step with its frozen
 transport term (cfk_wu_splitting_step_record), and, after the network is
 trained on those rows, with the gated surrogate sub-step
-(cfk_wu_splitting_step_surrogate).  Bar: ignition delay (time of the largest
-rise of the domain's peak temperature) and peak temperature within 1 % of the
-plain run's; most node-steps on the network."""
+(cfk_wu_splitting_step_surrogate).  The default gate keeps a node on the
+plain integrator when its plain step would take fewer than 50 substeps; at
+this flow's CFL step (~7e-8 s) that is every node, so the run is made with
+that rule off (min_substeps = 0): the network takes every node the
+range, ignition, consistency and judge rules leave it.  Bar: ignition delay
+(time of the largest rise of the domain's peak temperature) and peak
+temperature within 1 % of the plain run's; most node-steps on the
+network."""
 import numpy as np
 import pytest
 
@@ -72,7 +77,7 @@ def test_surrogate_flow_ignition_matches_plain():
 
     t_p, pk_p, _ = _peak_trace(plain, STEPS, rec)
     tau_p, peak_p, rise_p = _ignition(t_p, pk_p)
-    assert rise_p > 100.0 and tau_p < 0.9 * t_p[-1], "the plain run must ignite inside the window"
+    assert peak_p > pk_p[0] + 1000.0 and tau_p < 0.9 * t_p[-1], "the plain run must ignite inside the window"
 
     losses = sg.fit(plain.ctx, X, G, epochs=30, batch=8192)
     weights, norm = plain.ctx.surrogate_get_params()
@@ -80,7 +85,7 @@ def test_surrogate_flow_ignition_matches_plain():
     model.initialize()
     model.ctx.surrogate_init(7, mech.element_mass_fractions())
     model.ctx.surrogate_set_params(weights, norm)
-    gate = model.ctx.surrogate_default_gate()
+    gate = model.ctx.surrogate_default_gate(min_substeps=0.0)
 
     def surr(s):
         return model.ctx.wu_splitting_step_surrogate(gate, s, want_stats=(s % 20 == 19))
@@ -88,6 +93,8 @@ def test_surrogate_flow_ignition_matches_plain():
     t_s, pk_s, stats = _peak_trace(model, STEPS, surr)
     tau_s, peak_s, _ = _ignition(t_s, pk_s)
     on_net = sum(st["surrogate"] for st in stats) / sum(st["cells"] for st in stats)
+    reasons = {k: sum(st[k] for st in stats) for k in stats[0] if k.startswith("fallback_") or k.startswith("judge")}
+    print("fallback reasons over the window:", reasons)
     e_tau, e_pk = abs(tau_s - tau_p) / tau_p, abs(peak_s - peak_p) / peak_p
     print(f"loss {losses[0]:.3e} -> {losses[-1]:.3e}; tau_ign plain {tau_p:.4e} s, surrogate {tau_s:.4e} s "
           f"(err {e_tau:.2e}); T_peak plain {peak_p:.1f} K, surrogate {peak_s:.1f} K (err {e_pk:.2e}); "
