@@ -37,13 +37,17 @@ METRIC = "RK cell-updates/s (FP64)"
 UNIT = "cell-updates/s"
 N_NODES = 257
 
-# Algorithmic FP64 operations of one WENO7 characteristic face flux (air) plus
-# its share of the staging and flux difference, counted from the arithmetic of
-# the restated routine (each +, -, *, /, sqrt = 1; fma = 2): face set-up (Roe
-# average, basis, Lax-Friedrichs bound) 93; per characteristic field the left
-# eigenvector row 14, projection of 8 points 186, two WENO7-Z sides 361,
-# times 5 fields; back-projection 44; staging share 30, difference share 10.
-FLOPS_PER_FACE_WENO7_CH = 2980.0
+# FP64 operations of one WENO7 characteristic face flux (air) with its share
+# of the staging and flux difference, counted by the hardware: 2 x DFMA + DADD
+# + DMUL per face from ncu's instruction counters on a 161^3 block
+# (profiles/weno_air_flux_diff_161_fp64_counts.md; the same in all three
+# sweeps).  It includes the FMA/multiply steps into which divisions and square
+# roots expand.  The hand count of the restated arithmetic (each +, -, *, /,
+# sqrt = 1; fma = 2) is 2980: face set-up 93; per characteristic field the left
+# eigenvector row 14, projection of 8 points 186, two WENO7-Z sides 361, times
+# 5 fields; back-projection 44; staging share 30, difference share 10.
+FLOPS_PER_FACE_WENO7_CH = 3281.7
+FLOPS_PER_FACE_WENO7_CH_HAND = 2980.0
 
 
 WENO_PROFILE = os.path.join(ROOT, "profiles", "weno_air_flux_diff_161.md")
@@ -525,10 +529,14 @@ def surrogate_flow_bench(args, local):
             "T_peak_K": pk_s, "T_peak_rel_err": abs(pk_s - pk_p) / pk_p, "window_ms": traces[mode][2],
             **_stat_summary(traces[mode][3])}
 
-    # 2. the 2048 x 512 tube
+    # 2. the 2048 x 512 tube, with a network trained on its own wall strip
+    # (the same grid spacing, CFL step and Mach 2.2 states)
+    strip = cases.reflected_shock_tube(mech, args.sflow_nx, args.sflow_ny, ny_keep=32)
+    weights, norm, train2 = _train_on_flow(mech, strip, local, args.sflow_train_steps, args.sflow_epochs)
     big = cases.reflected_shock_tube(mech, args.sflow_nx, args.sflow_ny)
     K = args.sflow_steps
     r = _plain_vs_surrogate(mech, big, local, weights, norm, K)
+    r["training"] = train2
     r["case"] = (f"{big.mx}x{big.my} tube 0.1 x 0.025 m, wall-normal stretching 1.02, Mach 2.2 incident shock "
                  f"into 0.1 atm / 300 K, {K} steps ({r['plain']['simulated_s'] * 1e9:.1f} ns simulated)")
     out["tube_2048x512"] = r
@@ -637,28 +645,40 @@ def mixing_layer_bench(args, local):
     import surrogate as sg
 
     mech = mechanism.load("li2004")
-    dev = f"cuda:{local}"
-    small = cases.mixing_layer(mech, 64, 32, 16)
-    W, n = args.ml_train_steps, small.N
-    ctx, _ = _flow_ctx(mech, small, local, 9)
-    X = torch.empty((W * n, sg.cf.SG_NIN), dtype=torch.float32, device=dev)
-    G = torch.empty((W * n, sg.cf.SG_NOUT), dtype=torch.float32, device=dev)
-    for s_ in range(W):
-        ctx.wu_splitting_step_record(X[s_ * n].data_ptr(), G[s_ * n].data_ptr())
-    t0 = time.time()
-    losses = sg.fit(ctx, X, G, epochs=args.sflow_epochs, batch=8192, lr0=2e-3, lr1=1e-5, seed=3)
-    torch.cuda.synchronize()
-    weights, norm = ctx.surrogate_get_params()
-    ctx.close()
-    del X, G
+    # a 64 x 32 x 16 piece of the same grid (the same spacing and CFL step)
+    small = cases.mixing_layer(mech, args.ml_nx, args.ml_ny, args.ml_nz, window=(64, 32, 16))
+    weights, norm, train = _train_on_flow(mech, small, local, args.ml_train_steps, args.sflow_epochs)
     big = cases.mixing_layer(mech, args.ml_nx, args.ml_ny, args.ml_nz)
     K = args.ml_steps
     r = _plain_vs_surrogate(mech, big, local, weights, norm, K, modes=("plain", "surrogate", "surrogate_all", "rk3"))
     r["case"] = (f"{big.mx}x{big.my}x{big.mz} mixing layer 0.05 x 0.025 x 0.0125 m (y clustered), {K} steps "
                  f"({r['plain']['simulated_s'] * 1e9:.1f} ns simulated)")
-    r["training"] = {"case": f"{small.mx}x{small.my}x{small.mz}", "rows": W * n, "epochs": args.sflow_epochs,
-                     "train_s": time.time() - t0, "loss_first": losses[0], "loss_last": losses[-1]}
+    r["training"] = train
     return r
+
+
+def _train_on_flow(mech, case, local, steps, epochs):
+    """Training rows from `steps` plain Wu steps of `case` (one per node and
+    step, cfk_wu_splitting_step_record), then Adam on the device; returns the
+    weights, the standardisation and a summary."""
+    import torch
+    import surrogate as sg
+
+    dev = f"cuda:{local}"
+    n = case.N
+    ctx, _ = _flow_ctx(mech, case, local, 9)
+    X = torch.empty((steps * n, sg.cf.SG_NIN), dtype=torch.float32, device=dev)
+    G = torch.empty((steps * n, sg.cf.SG_NOUT), dtype=torch.float32, device=dev)
+    for s_ in range(steps):
+        ctx.wu_splitting_step_record(X[s_ * n].data_ptr(), G[s_ * n].data_ptr())
+    t0 = time.time()
+    losses = sg.fit(ctx, X, G, epochs=epochs, batch=8192, lr0=2e-3, lr1=1e-5, seed=3)
+    torch.cuda.synchronize()
+    weights, norm = ctx.surrogate_get_params()
+    ctx.close()
+    return weights, norm, {"case": f"{case.mx}x{case.my}x{case.mz} piece of the same grid", "rows": steps * n,
+                           "epochs": epochs, "train_s": time.time() - t0, "loss_first": losses[0],
+                           "loss_last": losses[-1]}
 
 
 def main():
@@ -691,7 +711,8 @@ def main():
     ap.add_argument("--sflow-ign-nx", type=int, default=128)
     ap.add_argument("--sflow-ign-ny", type=int, default=16)
     ap.add_argument("--sflow-ign-steps", type=int, default=600)
-    ap.add_argument("--sflow-epochs", type=int, default=30)
+    ap.add_argument("--sflow-epochs", type=int, default=300)
+    ap.add_argument("--sflow-train-steps", type=int, default=100, help="recorded Wu steps of the tube's wall strip")
     ap.add_argument("--no-mixing-layer", action="store_true")
     ap.add_argument("--mixing-layer-only", action="store_true", help="only the reacting mixing-layer measurement")
     ap.add_argument("--ml-nx", type=int, default=512)
@@ -801,7 +822,11 @@ def main():
                     "traffic": traffic, "traffic_source": traffic_source,
                     "kernel": "weno_air_flux_diff<dir,7> (x/y/z sweeps)",
                     "peak_source": "measured live: cfk_measure_fp64_peak FMA-chain kernel",
-                    "avg_launch_ms": avg_launch_ms, "flops_per_launch": FLOPS_PER_FACE_WENO7_CH * faces_per_launch}
+                    "avg_launch_ms": avg_launch_ms, "flops_per_launch": FLOPS_PER_FACE_WENO7_CH * faces_per_launch,
+                    "flops_source": "ncu DFMA/DADD/DMUL counters per face, 161^3 "
+                                    "(profiles/weno_air_flux_diff_161_fp64_counts.md)",
+                    "frac_hand_count": FLOPS_PER_FACE_WENO7_CH_HAND * faces_per_launch / (avg_launch_ms * 1e-3)
+                    / 1e12 / peak}
     else:
         # primitive-variable schemes are HBM-bound: algorithmic bytes per node
         # and direction = bv[5] + metric[3] + jac + dq[5] read-modify-write
@@ -902,7 +927,7 @@ def main():
                        "nodes": f"{n}^3", "global_nodes": nodes * world,
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cv alone "
                        f"{5 * P * 8 / 1e6:.0f} MB)", "weno_tile_variants": tiles, "autotune_ms": tile_ms,
-                       "viscous_form": ["staged", "ring"][visc_var], "viscous_form_ms": visc_ms},
+                       "viscous_form": ["staged", "ring (2 CTAs/SM)", "ring (3 CTAs/SM)"][visc_var], "viscous_form_ms": visc_ms},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "gpu_launches": launches,
             "roofline": roofline,

@@ -697,7 +697,8 @@ def reflected_shock_states(mech, Y: np.ndarray, T1: float, p1: float, mach: floa
 
 def reflected_shock_tube(mech, nx: int = 2048, ny: int = 512, length: float = 0.1, height: float = 0.025,
                          stretch: float = 1.02, mach: float = 2.2, T1: float = 300.0, p1: float = 0.1 * 101325.0,
-                         x_shock: float | None = None, scheme: int = 52, viscous_order: int = 2) -> Case:
+                         x_shock: float | None = None, scheme: int = 52, viscous_order: int = 2,
+                         ny_keep: int | None = None) -> Case:
     """Reflected-shock ignition: stoichiometric H2-O2 diluted by 70 % Ar (2 : 1 : 7
     by mole) at (T1, p1), hit by an incident shock of Mach `mach`, as the gas
     just after the shock has reflected from the closed end x = length: state 5
@@ -707,7 +708,8 @@ def reflected_shock_tube(mech, nx: int = 2048, ny: int = 512, length: float = 0.
     the ratio `stretch` per cell; faces: x = 0 outflow, x = length adiabatic
     no-slip wall (the end wall), y = 0 adiabatic no-slip wall, y = height
     symmetry.  WENO5 characteristic (52) with mixture-averaged viscous fluxes;
-    the mechanism's reactions are kept."""
+    the mechanism's reactions are kept.  ny_keep: only the first ny_keep rows of
+    that grid (a wall strip with the same spacing, hence the same CFL step)."""
     X = np.zeros(mech.n_spec)
     X[mech.index("H2")], X[mech.index("O2")], X[mech.index("AR")] = 2.0, 1.0, 7.0
     Y = mole_to_mass(mech, X / X.sum())
@@ -716,6 +718,9 @@ def reflected_shock_tube(mech, nx: int = 2048, ny: int = 512, length: float = 0.
     xs = np.linspace(0.0, length, nx)
     widths = stretch ** np.arange(ny - 1)
     ys = np.concatenate([[0.0], np.cumsum(widths)]) * (height / widths.sum())
+    if ny_keep is not None:  # the wall strip of the same grid: its first ny_keep rows
+        ys = ys[:ny_keep]
+        ny = ny_keep
     x = np.broadcast_to(xs[None, None, :], (1, ny, nx)).copy()
     y = np.broadcast_to(ys[None, :, None], (1, ny, nx)).copy()
     z = np.zeros_like(x)
@@ -771,7 +776,8 @@ def mixing_layer_streams(mech, upper: dict, lower: dict, ma_c: float, velocity_r
 def mixing_layer(mech, nx: int = 512, ny: int = 256, nz: int = 128, length: float = 0.05, height: float = 0.025,
                  span: float = 0.0125, delta_omega: float = 5e-4, ma_c: float = 0.2, velocity_ratio: float = 1.5,
                  T0: float = 600.0, p0: float = 101325.0, fluctuation: float = 0.01, seed: int = 2026,
-                 cluster: float = 3.0, scheme: int = 72, viscous_order: int = 2, reacting: bool = True) -> Case:
+                 cluster: float = 3.0, scheme: int = 72, viscous_order: int = 2, reacting: bool = True,
+                 window: tuple | None = None) -> Case:
     """Spatially developing H2/air mixing layer: air above y = 0 (the faster
     stream) and H2/N2 (1 : 1 by mole) below, both at T0 and p0, with the
     velocity ratio and convective Mach number of mixing_layer_streams; the
@@ -783,7 +789,9 @@ def mixing_layer(mech, nx: int = 512, ny: int = 256, nz: int = 128, length: floa
     eta) / sinh(c) (eta in [-1, 1]).  Faces: x = 0 the mixing-layer inflow
     with white noise of relative intensity `fluctuation` on u, v, w (seeded),
     x = length and both y faces outflow, z periodic.  WENO7 characteristic
-    with mixture-averaged viscous fluxes; `reacting` keeps the reactions."""
+    with mixture-averaged viscous fluxes; `reacting` keeps the reactions.
+    window (wx, wy, wz): a piece of that grid (same spacing, so the same CFL
+    step): the first wx nodes in x, the middle wy rows, the first wz in z."""
     m = mech if reacting else without_reactions(mech)
     X_fuel = np.zeros(m.n_spec)
     X_fuel[m.index("H2")], X_fuel[m.index("N2")] = 0.5, 0.5
@@ -799,6 +807,12 @@ def mixing_layer(mech, nx: int = 512, ny: int = 256, nz: int = 128, length: floa
     eta = np.linspace(-1.0, 1.0, ny)
     ys = 0.5 * height * np.sinh(cluster * eta) / np.sinh(cluster)
     zs = np.linspace(0.0, span, nz)
+    if window is not None:  # a piece of the same grid: the first wx x nodes, the middle wy rows, the first wz
+        wx, wy, wz = window
+        xs, zs = xs[:wx], zs[:wz]
+        j0 = (ny - wy) // 2
+        ys = ys[j0:j0 + wy]
+        nx, ny, nz = wx, wy, wz
     Z3, Y3, X3 = np.meshgrid(zs, ys, xs, indexing="ij")
     x, y, z = X3.copy(), Y3.copy(), Z3.copy()
     jac, metric, xg = metrics(x, y, z, ngg)

@@ -607,7 +607,7 @@ int cfk_autotune_tiles(cfk_ctx *c, int reps, double *ms_out, int *choice_out, vo
   int visc_choice = c->visc_var;
   if (e == cudaSuccess && !th && c->p.viscous_order == 2) {
     double best = 1e300;
-    for (int var = 0; var < 2 && e == cudaSuccess; ++var) {
+    for (int var = 0; var < 3 && e == cudaSuccess; ++var) {
       int nl = 0;
       e = launch_viscous_air(zt, pt, st, &nl, var);  // warm-up
       if (e == cudaSuccess) e = cudaEventRecord(a, st);
@@ -635,13 +635,13 @@ int cfk_autotune_tiles(cfk_ctx *c, int reps, double *ms_out, int *choice_out, vo
 int cfk_viscous_variant(cfk_ctx *c, int set, int *var, double *ms) {
   if (!c || !var) return CFK_ERR_ARG;
   if (set) {
-    if (*var != 0 && *var != 1) return fail(c, CFK_ERR_ARG, "viscous variant must be 0 or 1");
+    if (*var < 0 || *var > 2) return fail(c, CFK_ERR_ARG, "viscous variant must be 0, 1 or 2");
     c->visc_var = *var;
     if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
   } else {
     *var = c->visc_var;
   }
-  if (ms) { ms[0] = c->visc_ms[0]; ms[1] = c->visc_ms[1]; }
+  if (ms) { ms[0] = c->visc_ms[0]; ms[1] = c->visc_ms[1]; ms[2] = c->visc_ms[2]; }
   return CFK_OK;
 }
 

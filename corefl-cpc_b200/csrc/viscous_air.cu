@@ -24,6 +24,11 @@ constexpr int kFX = 32, kFY = 8, kFZ = 32;     // tile and planes per chunk
 constexpr int kPX = kFX + 2, kPY = kFY + 2;    // staged points per plane
 constexpr int kNV = 15;                        // u v w T mu J metric[9]
 constexpr int kFT = kFX * kFY;                 // threads
+// the flux's constant factors as products: 1/3 of the normal stresses and
+// cp / Pr of the conductivity, formed once (the reference divides by 3 and
+// by Pr at every face; the results differ in the last bits)
+constexpr double kThird = 1.0 / 3.0;
+constexpr double kCpAir = kGammaAir * kRAir / (kGammaAir - 1);
 
 struct FusedSmem {
   double pl[2][kNV][kPY][kPX];   // planes k and k+1 (slots swap)
@@ -40,7 +45,7 @@ struct FusedSmem {
 // as 0.25 ((f(A+) - f(A-)) + (f(B+) - f(B-))).
 template <int DIR>
 __device__ __forceinline__ void staged_face(const FusedSmem &S, int sa, int pa, int qa, int sb, int pb, int qb,
-                                            double Pr, double F[4]) {
+                                            double cp_pr, double F[4]) {
   const auto &A = S.pl[sa];
   const auto &B = S.pl[sb];
   // transverse difference of variable q at a point along direction D (0 x, 1 y, 2 z)
@@ -73,9 +78,9 @@ __device__ __forceinline__ void staged_face(const FusedSmem &S, int sa, int pa, 
   const double t_y = dd[3][0] * gm[1] + dd[3][1] * gm[4] + dd[3][2] * gm[7];
   const double t_z = dd[3][0] * gm[2] + dd[3][1] * gm[5] + dd[3][2] * gm[8];
   const double mul = 0.5 * (A[4][qa][pa] + B[4][qb][pb]);
-  const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
-  const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
-  const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) * kThird;
+  const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) * kThird;
+  const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) * kThird;
   const double tau_xy = mul * (u_y + v_x);
   const double tau_xz = mul * (u_z + w_x);
   const double tau_yz = mul * (v_z + w_y);
@@ -89,14 +94,14 @@ __device__ __forceinline__ void staged_face(const FusedSmem &S, int sa, int pa, 
   const double um = 0.5 * (A[0][qa][pa] + B[0][qb][pb]);
   const double vm = 0.5 * (A[1][qa][pa] + B[1][qb][pb]);
   const double wm = 0.5 * (A[2][qa][pa] + B[2][qb][pb]);
-  constexpr double cp = kGammaAir * kRAir / (kGammaAir - 1);
-  const double conductivity = mul / Pr * cp;
+  const double conductivity = mul * cp_pr;
   F[3] = um * F[0] + vm * F[1] + wm * F[2] + conductivity * (gk0 * t_x + gk1 * t_y + gk2 * t_z);
 }
 }  // namespace
 
 __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
   extern __shared__ __align__(16) double fsm[];
+  const double cp_pr = kCpAir / Pr;
   FusedSmem &S = *reinterpret_cast<FusedSmem *>(fsm);
   const Dims d = z.d;
   const int g = d.ngg;
@@ -140,8 +145,11 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
   const bool mine = i < d.mx && j < d.my;
   double fzp[4] = {0, 0, 0, 0};
   if (three_d && mine) {
-    staged_face<2>(S, 0, tx + 1, ty + 1, 1, tx + 1, ty + 1, Pr, fzp);
+    staged_face<2>(S, 0, tx + 1, ty + 1, 1, tx + 1, ty + 1, cp_pr, fzp);
   }
+  // the first iteration refills slot 0, which the z faces above read at
+  // neighbouring points
+  __syncthreads();
   int cur = 1;  // slot of plane k
   for (int k = k0; k < k_end; ++k) {
     const int nxt = cur ^ 1;  // holds plane k-1, receives plane k+1
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
         const int fy_ = f / (kFX + 1), fx_ = f - fy_ * (kFX + 1);
         if (i0 - 1 + fx_ > d.mx - 1 || j0 + fy_ >= d.my) continue;
         double F[4];
-        staged_face<0>(S, cur, fx_, fy_ + 1, cur, fx_ + 1, fy_ + 1, Pr, F);
+        staged_face<0>(S, cur, fx_, fy_ + 1, cur, fx_ + 1, fy_ + 1, cp_pr, F);
 #pragma unroll
         for (int q = 0; q < 4; ++q) S.fx[q][fy_][fx_] = F[q];
       } else {
@@ -195,14 +203,14 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_fused(Zone z, double Pr) {
         const int fy_ = e / kFX, fx_ = e - fy_ * kFX;
         if (i0 + fx_ >= d.mx || j0 - 1 + fy_ > d.my - 1) continue;
         double F[4];
-        staged_face<1>(S, cur, fx_ + 1, fy_, cur, fx_ + 1, fy_ + 1, Pr, F);
+        staged_face<1>(S, cur, fx_ + 1, fy_, cur, fx_ + 1, fy_ + 1, cp_pr, F);
 #pragma unroll
         for (int q = 0; q < 4; ++q) S.fy[q][fy_][fx_] = F[q];
       }
     }
     double fzn[4] = {0, 0, 0, 0};
     if (three_d && mine) {
-      staged_face<2>(S, cur, tx + 1, ty + 1, nxt, tx + 1, ty + 1, Pr, fzn);
+      staged_face<2>(S, cur, tx + 1, ty + 1, nxt, tx + 1, ty + 1, cp_pr, fzn);
     }
     __syncthreads();
     if (mine) {
@@ -250,7 +258,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int DIR>
 __device__ __forceinline__ void ring_face(const RingSmem &S, const double *__restrict__ met,
                                           const double *__restrict__ jac, int64_t sz, int sa, int pa, int qa,
-                                          int64_t ida, int sb, int pb, int qb, int64_t idb, double Pr, double F[4]) {
+                                          int64_t ida, int sb, int pb, int qb, int64_t idb, double cp_pr,
+                                          double F[4]) {
   const auto &A = S.dyn[sa];
   const auto &B = S.dyn[sb];
   auto tdiff = [&](const double (&p)[kRV][kPY][kPX], int D, int q, int px, int py) -> double {
@@ -282,9 +291,9 @@ __device__ __forceinline__ void ring_face(const RingSmem &S, const double *__res
   const double t_y = dd[3][0] * gm[1] + dd[3][1] * gm[4] + dd[3][2] * gm[7];
   const double t_z = dd[3][0] * gm[2] + dd[3][1] * gm[5] + dd[3][2] * gm[8];
   const double mul = 0.5 * (A[4][qa][pa] + B[4][qb][pb]);
-  const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
-  const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
-  const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double tau_xx = mul * (4 * u_x - 2 * v_y - 2 * w_z) * kThird;
+  const double tau_yy = mul * (4 * v_y - 2 * u_x - 2 * w_z) * kThird;
+  const double tau_zz = mul * (4 * w_z - 2 * u_x - 2 * v_y) * kThird;
   const double tau_xy = mul * (u_y + v_x);
   const double tau_xz = mul * (u_z + w_x);
   const double tau_yz = mul * (v_z + w_y);
@@ -298,14 +307,17 @@ __device__ __forceinline__ void ring_face(const RingSmem &S, const double *__res
   const double um = 0.5 * (A[0][qa][pa] + B[0][qb][pb]);
   const double vm = 0.5 * (A[1][qa][pa] + B[1][qb][pb]);
   const double wm = 0.5 * (A[2][qa][pa] + B[2][qb][pb]);
-  constexpr double cp = kGammaAir * kRAir / (kGammaAir - 1);
-  const double conductivity = mul / Pr * cp;
+  const double conductivity = mul * cp_pr;
   F[3] = um * F[0] + vm * F[1] + wm * F[2] + conductivity * (gk0 * t_x + gk1 * t_y + gk2 * t_z);
 }
 }  // namespace
 
-__global__ void __launch_bounds__(kFT, 2) viscous_air_ring(Zone z, double Pr) {
+// MINB: CTAs per SM the register budget is sized for (2: no spills; 3: about
+// 80 registers with a few spills, 24 warps per SM).
+template <int MINB>
+__global__ void __launch_bounds__(kFT, MINB) viscous_air_ring(Zone z, double Pr) {
   extern __shared__ __align__(16) double rsm[];
+  const double cp_pr = kCpAir / Pr;
   RingSmem &S = *reinterpret_cast<RingSmem *>(rsm);
   const Dims d = z.d;
   const int g = d.ngg;
@@ -348,8 +360,11 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_ring(Zone z, double Pr) {
   double fzp[4] = {0, 0, 0, 0};
   if (three_d && mine) {
     const int64_t ida = d.idx(g, i, j, k0 - 1);
-    ring_face<2>(S, met, jac, sz, 0, tx + 1, ty + 1, ida, 1, tx + 1, ty + 1, ida + spl, Pr, fzp);
+    ring_face<2>(S, met, jac, sz, 0, tx + 1, ty + 1, ida, 1, tx + 1, ty + 1, ida + spl, cp_pr, fzp);
   }
+  // the first iteration refills slot 0, which the z faces above read at
+  // neighbouring points
+  __syncthreads();
   int sp = 0, sc = 1, sn = 2;  // slots of planes k-1, k, k+1
   for (int k = k0; k < k_end; ++k) {
     double acc[4];
@@ -380,7 +395,7 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_ring(Zone z, double Pr) {
         if (i0 - 1 + fx_ > d.mx - 1 || j0 + fy_ >= d.my) continue;
         const int64_t ida = d.idx(g, i0 - 1 + fx_, j0 + fy_, k);
         double F[4];
-        ring_face<0>(S, met, jac, sz, sc, fx_, fy_ + 1, ida, sc, fx_ + 1, fy_ + 1, ida + 1, Pr, F);
+        ring_face<0>(S, met, jac, sz, sc, fx_, fy_ + 1, ida, sc, fx_ + 1, fy_ + 1, ida + 1, cp_pr, F);
 #pragma unroll
         for (int q = 0; q < 4; ++q) S.fx[q][fy_][fx_] = F[q];
       } else {
@@ -389,7 +404,7 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_ring(Zone z, double Pr) {
         if (i0 + fx_ >= d.mx || j0 - 1 + fy_ > d.my - 1) continue;
         const int64_t ida = d.idx(g, i0 + fx_, j0 - 1 + fy_, k);
         double F[4];
-        ring_face<1>(S, met, jac, sz, sc, fx_ + 1, fy_, ida, sc, fx_ + 1, fy_ + 1, ida + srow, Pr, F);
+        ring_face<1>(S, met, jac, sz, sc, fx_ + 1, fy_, ida, sc, fx_ + 1, fy_ + 1, ida + srow, cp_pr, F);
 #pragma unroll
         for (int q = 0; q < 4; ++q) S.fy[q][fy_][fx_] = F[q];
       }
@@ -397,7 +412,7 @@ __global__ void __launch_bounds__(kFT, 2) viscous_air_ring(Zone z, double Pr) {
     double fzn[4] = {0, 0, 0, 0};
     if (three_d && mine) {
       const int64_t ida = d.idx(g, i, j, k);
-      ring_face<2>(S, met, jac, sz, sc, tx + 1, ty + 1, ida, sn, tx + 1, ty + 1, ida + spl, Pr, fzn);
+      ring_face<2>(S, met, jac, sz, sc, tx + 1, ty + 1, ida, sn, tx + 1, ty + 1, ida + spl, cp_pr, fzn);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -425,15 +440,19 @@ cudaError_t viscous_air_init_attributes() {
   cudaError_t e = cudaFuncSetAttribute(viscous_air_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(FusedSmem));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(viscous_air_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
+  e = cudaFuncSetAttribute(viscous_air_ring<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(viscous_air_ring<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
 }
 
 // compute_viscous_flux for air (reference src/ViscousScheme.cu:7-40): one
-// launch for all directions; var 0 the staged kernel, 1 the ring kernel.
+// launch for all directions; var 0 the staged kernel, 1 the ring kernel at
+// two CTAs per SM, 2 the ring kernel at three.
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch, int var) {
   const Dims &d = z.d;
   const dim3 grid((d.mx + kFX - 1) / kFX, (d.my + kFY - 1) / kFY, (d.mz + kFZ - 1) / kFZ);
-  if (var == 1) viscous_air_ring<<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
+  if (var == 1) viscous_air_ring<2><<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
+  else if (var == 2) viscous_air_ring<3><<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
   else viscous_air_fused<<<grid, kFT, sizeof(FusedSmem), st>>>(z, p.Pr);
   *n_launch += 1;
   return cudaGetLastError();

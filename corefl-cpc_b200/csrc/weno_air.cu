@@ -28,7 +28,7 @@ namespace cfk {
 
 namespace {
 
-constexpr int kNQ = 16;  // staged values per point: Q0..4, G0..4, p, J/2, lambda, the sweep's metric row
+constexpr int kNQ = 13;  // staged values per point: Q0..4, G0..4, p, J/2, lambda
 
 // Tile shapes of a sweep: VAR selects one of the CFK_TILE_VARIANTS shapes
 // (nodes per column TN x columns C), chosen per direction by the tile
@@ -83,9 +83,6 @@ __device__ __forceinline__ void air_stage_point(double *s, int c, int t, double 
   s[T::spt(10, c, t)] = pk;
   s[T::spt(11, c, t)] = 0.5 * jac;
   s[T::spt(12, c, t)] = abs(Uk) + cGradK;
-  s[T::spt(13, c, t)] = m0;
-  s[T::spt(14, c, t)] = m1;
-  s[T::spt(15, c, t)] = m2;
 }
 
 // Flux of the face between local points t + R and t + R + 1 of column c:
@@ -244,25 +241,11 @@ __global__ void __launch_bounds__(256, 2) weno_air_flux_diff(Zone z, double eps_
     const int f = n0 - 1 + t;  // face between node f and f+1 along DIR
     if (cbase + c >= ncol_max || f > m - 1) continue;
     // face normal, averaged with the (i+1) node in every direction as the
-    // reference does (reference src/WENO.cu:886-888, 1627-1629, 2303-2305):
-    // for x the next point of the column, for y and z the same point of the
-    // next column — both staged, except past the tile's last column
+    // reference does (reference src/WENO.cu:886-888, 1627-1629, 2303-2305)
     const int64_t idf = node_idx(g, c, f);
-    const int pc = t + R;
-    double kx, ky, kz;
-    if (DIR == 0) {
-      kx = 0.5 * (spts[T::spt(13, c, pc)] + spts[T::spt(13, c, pc + 1)]);
-      ky = 0.5 * (spts[T::spt(14, c, pc)] + spts[T::spt(14, c, pc + 1)]);
-      kz = 0.5 * (spts[T::spt(15, c, pc)] + spts[T::spt(15, c, pc + 1)]);
-    } else if (c + 1 < C && cbase + c + 1 < ncol_max) {
-      kx = 0.5 * (spts[T::spt(13, c, pc)] + spts[T::spt(13, c + 1, pc)]);
-      ky = 0.5 * (spts[T::spt(14, c, pc)] + spts[T::spt(14, c + 1, pc)]);
-      kz = 0.5 * (spts[T::spt(15, c, pc)] + spts[T::spt(15, c + 1, pc)]);
-    } else {
-      kx = 0.5 * (spts[T::spt(13, c, pc)] + z.metric[idf + 1 + mmo * sz]);
-      ky = 0.5 * (spts[T::spt(14, c, pc)] + z.metric[idf + 1 + (mmo + 1) * sz]);
-      kz = 0.5 * (spts[T::spt(15, c, pc)] + z.metric[idf + 1 + (mmo + 2) * sz]);
-    }
+    double kx = 0.5 * (z.metric[idf + mmo * sz] + z.metric[idf + 1 + mmo * sz]);
+    double ky = 0.5 * (z.metric[idf + (mmo + 1) * sz] + z.metric[idf + 1 + (mmo + 1) * sz]);
+    double kz = 0.5 * (z.metric[idf + (mmo + 2) * sz] + z.metric[idf + 1 + (mmo + 2) * sz]);
 
     const bool shock = !HYB || face_shocked(sensor, idf, d.stride(g, DIR), g, threshold);
     air_face<ORD, T>(spts, sflx, c, t, kx, ky, kz, eps_ref, shock);

@@ -240,13 +240,14 @@ int cfk_compute_shock_sensor(cfk_ctx *ctx, void *stream);
  * capture.  A no-op for the primitive-variable schemes (one tile shape). */
 #define CFK_TILE_VARIANTS 3
 int cfk_autotune_tiles(cfk_ctx *ctx, int reps, double *ms_out, int *choice_out, void *stream);
-/* For air with viscous_order 2, cfk_autotune_tiles also times the two forms of
+/* For air with viscous_order 2, cfk_autotune_tiles also times the forms of
  * the fused viscous kernel — 0: all per-node inputs staged in shared memory
  * (two plane slots); 1: only u, v, w, T, mu staged, in a three-slot ring
- * filled by cp.async ahead of use, with the metric read through L1 — and
- * keeps the faster (the same arithmetic; they agree to the last bits).  cfk_viscous_variant reads
- * (set = 0) or sets (set = 1) the form in *var; ms (optional, 2 doubles)
- * receives the last autotune's times per launch. */
+ * filled by cp.async ahead of use, with the metric read through L1, two CTAs
+ * per SM; 2: the same at three CTAs per SM (fewer registers) — and keeps the
+ * fastest (the same arithmetic; they agree to the last bits).
+ * cfk_viscous_variant reads (set = 0) or sets (set = 1) the form in *var;
+ * ms (optional, 3 doubles) receives the last autotune's times per launch. */
 int cfk_viscous_variant(cfk_ctx *ctx, int set, int *var, double *ms);
 /* Sets the tile variant of each sweep (var[3], each 0..CFK_TILE_VARIANTS-1). */
 int cfk_set_tile_variants(cfk_ctx *ctx, const int *var);

@@ -79,7 +79,7 @@ def test_surrogate_flow_ignition_matches_plain():
     tau_p, peak_p, rise_p = _ignition(t_p, pk_p)
     assert peak_p > pk_p[0] + 1000.0 and tau_p < 0.9 * t_p[-1], "the plain run must ignite inside the window"
 
-    losses = sg.fit(plain.ctx, X, G, epochs=30, batch=8192)
+    losses = sg.fit(plain.ctx, X, G, epochs=300, batch=8192)
     weights, norm = plain.ctx.surrogate_get_params()
     model = GpuZone(case)
     model.initialize()
