@@ -184,7 +184,9 @@ def write_grid(spec: Spec, d: str):
         f.write("1\n0\n\n")
 
 
-def run_case(spec: Spec, workdir: str) -> dict:
+def prepare_case(spec: Spec, workdir: str) -> str:
+    """Writes the case directory of `spec` (setup.txt, grid, boundary files,
+    chemistry files, initial-state override) under `workdir`; returns it."""
     c = spec.case
     d = os.path.join(workdir, spec.name)
     for sub in ("input/grid", "input/boundary_condition", "input/chemistry", "out", "output/message",
@@ -201,6 +203,11 @@ def run_case(spec: Spec, workdir: str) -> dict:
         c.bv.astype(np.float64).tofile(os.path.join(d, "input", "init_bv.bin"))
         if c.mech is not None:
             c.sv.astype(np.float64).tofile(os.path.join(d, "input", "init_sv.bin"))
+    return d
+
+
+def run_case(spec: Spec, workdir: str) -> dict:
+    d = prepare_case(spec, workdir)
     cmd = [HARNESS, d, spec.mode, str(spec.steps)] + ([repr(spec.react_dt)] if spec.mode == "react" else [])
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     with open(os.path.join(workdir, spec.name + ".log"), "w") as f:
@@ -372,10 +379,10 @@ def _mix_wave(reacting):
     return Spec(name, c, "rk3", 2, mech_name="li2004", reference_state=ref)
 
 
-def _reactors(n_side=32, steps=10, dt=1e-7):
+def _reactors(n_side=32, steps=10, dt=1e-7, seed=2024):
     mech = mechanism.load("li2004")
     n = n_side * n_side
-    base = cases.reactor_batch(mech, n, seed=2024)
+    base = cases.reactor_batch(mech, n, seed=seed)
     # the same reactors as an n_side x n_side 2-D block with the ghost layers
     # of the reference's WENO5 scheme
     ngg = cases.ghost_layers(52)

@@ -19,6 +19,10 @@
 //   refharness <case dir> react <steps> <dt>
 //        reaction steps only: wu_reaction_step with Cn = 0 on every node
 //        (src/StrangSplitting.cu:373-421, constant-volume reactors)
+//   refharness <case dir> rk3time <steps> <warm-up>
+//   refharness <case dir> reacttime <steps> <dt> <warm-up>
+//        the same steps timed with CUDA events, without any file output:
+//        one JSON line on stdout with the per-step times
 //
 // Output, under <case dir>/out/: state_<s>_<name>.bin for s = 0 (after
 // initialisation and compute_cv_from_bv) .. steps, name in cv, bv, sv
@@ -57,8 +61,12 @@ __global__ void wu_reaction_step(DZone *zone, const DParameter *param, real dt);
 
 namespace {
 
+// Timed runs (rk3time, reacttime) check launches without synchronising, so
+// the timed region holds only the reference's own synchronisation points.
+bool g_sync_checks = true;
+
 void check(const char *what) {
-  cudaError_t e = cudaDeviceSynchronize();
+  cudaError_t e = g_sync_checks ? cudaDeviceSynchronize() : cudaSuccess;
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
     std::fprintf(stderr, "refharness: %s: %s\n", what, cudaGetErrorString(e));
@@ -275,21 +283,62 @@ template<MixtureModel M> struct Run {
     write_device("out/visc_h.bin", z.hFlux.data(), nf);
   }
 
-  // Reaction only, Cn = 0: a batch of constant-volume reactors.
-  real react_step(real dt) {
+  // Reaction only, Cn = 0: a batch of constant-volume reactors.  Timed runs
+  // zero Cn once before their first step (zero_cn = false afterwards).
+  real react_step(real dt, bool zero_cn = true) {
     cfd::DZone &z = zone();
-    cudaMemset(z.Cn.data(), 0, static_cast<size_t>(z.Cn.size()) * n_var * sizeof(real));
+    if (zero_cn) cudaMemset(z.Cn.data(), 0, static_cast<size_t>(z.Cn.size()) * n_var * sizeof(real));
     cfd::wu_reaction_step<<<bpg(), tpb()>>>(driver.field[0].d_ptr, driver.param, dt);
     check("wu_reaction_step");
     return dt;
   }
 };
 
+// Timed steps of the reference's own kernels: `warmup` untimed steps, then
+// `steps` steps, each between two CUDA events on the legacy default stream,
+// which is where every reference kernel driven here is launched.  Prints one
+// JSON line: the total and the per-step times (ms) and the node count.
+template<MixtureModel M> int timed(Run<M> &r, const std::string &mode, int steps, int warmup, double react_dt) {
+  const bool rk3 = mode == "rk3time";
+  if (!rk3) r.react_step(react_dt, true);  // zero Cn; this step counts as a warm-up step
+  g_sync_checks = false;
+  for (int s = 1; s <= warmup; ++s) rk3 ? r.rk3_step(s) : r.react_step(react_dt, false);
+  g_sync_checks = true;
+  check("warm-up steps");
+  g_sync_checks = false;
+  std::vector<cudaEvent_t> ev(static_cast<size_t>(steps) + 1);
+  for (auto &e : ev) cudaEventCreate(&e);
+  real dt = 0;
+  cudaEventRecord(ev[0]);
+  for (int s = 1; s <= steps; ++s) {
+    dt = rk3 ? r.rk3_step(warmup + s) : r.react_step(react_dt, false);
+    cudaEventRecord(ev[static_cast<size_t>(s)]);
+  }
+  cudaEventSynchronize(ev.back());
+  g_sync_checks = true;
+  check("timed steps");
+  float total = 0;
+  cudaEventElapsedTime(&total, ev[0], ev.back());
+  std::printf("{\"mode\": \"%s\", \"steps\": %d, \"warmup\": %d, \"ms_total\": %.6f, \"ms_per_step\": [",
+              mode.c_str(), steps, warmup, total);
+  for (int s = 1; s <= steps; ++s) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[static_cast<size_t>(s) - 1], ev[static_cast<size_t>(s)]);
+    std::printf("%s%.6f", s > 1 ? ", " : "", ms);
+  }
+  const auto &b = r.mesh[0];
+  std::printf("], \"nodes\": %lld, \"mx\": %d, \"my\": %d, \"mz\": %d, \"dt\": %.17g}\n",
+              static_cast<long long>(b.mx) * b.my * b.mz, b.mx, b.my, b.mz, dt);
+  for (auto &e : ev) cudaEventDestroy(e);
+  return 0;
+}
+
 template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, const std::string &mode, int steps,
-                                 double react_dt) {
+                                 double react_dt, int warmup) {
   Run<M> r(parameter, mesh);
   r.initialise();
   r.start();
+  if (mode == "rk3time" || mode == "reacttime") return timed(r, mode, steps, warmup, react_dt);
   r.dump_grid();
   r.dump_param();
   r.dump_state(0);
@@ -316,17 +365,27 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
 
 int main(int argc, char *argv[]) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react|visc <steps> [dt]\n");
+    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react|visc <steps> [dt]\n"
+                         "       refharness <case dir> rk3time <steps> <warm-up steps>\n"
+                         "       refharness <case dir> reacttime <steps> <dt> <warm-up steps>\n");
     return 2;
   }
   const std::string mode = argv[2];
   const int steps = std::atoi(argv[3]);
-  const double react_dt = argc > 4 ? std::atof(argv[4]) : 0.0;
-  if (mode != "rk3" && mode != "wu" && mode != "react" && mode != "visc") {
+  const bool react = mode == "react" || mode == "reacttime";
+  const double react_dt = react && argc > 4 ? std::atof(argv[4]) : 0.0;
+  const int warmup = mode == "rk3time" ? (argc > 4 ? std::atoi(argv[4]) : 0)
+                                       : (mode == "reacttime" && argc > 5 ? std::atoi(argv[5]) : 0);
+  if (mode != "rk3" && mode != "wu" && mode != "react" && mode != "visc" && mode != "rk3time" &&
+      mode != "reacttime") {
     std::fprintf(stderr, "refharness: unknown mode %s\n", mode.c_str());
     return 2;
   }
-  if (mode == "react" && !(react_dt > 0)) {
+  if ((mode == "rk3time" || mode == "reacttime") && (steps < 1 || warmup < 0)) {
+    std::fprintf(stderr, "refharness: a timed run needs steps >= 1 and warm-up steps >= 0\n");
+    return 2;
+  }
+  if (react && !(react_dt > 0)) {
     std::fprintf(stderr, "refharness: react needs a positive dt\n");
     return 2;
   }
@@ -344,6 +403,6 @@ int main(int argc, char *argv[]) {
   }
   const int species = parameter.get_int("species");
   if (!parameter.get_bool("turbulence")) parameter.update_parameter("turbulence_method", 0);
-  if (species == 1) return run<MixtureModel::Mixture>(parameter, mesh, mode, steps, react_dt);
-  return run<MixtureModel::Air>(parameter, mesh, mode, steps, react_dt);
+  if (species == 1) return run<MixtureModel::Mixture>(parameter, mesh, mode, steps, react_dt, warmup);
+  return run<MixtureModel::Air>(parameter, mesh, mode, steps, react_dt, warmup);
 }
