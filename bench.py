@@ -50,6 +50,15 @@ FLOPS_PER_FACE_WENO7_CH = 3281.7
 FLOPS_PER_FACE_WENO7_CH_HAND = 2980.0
 
 
+# The reference's own CUDA kernels (its sources built unmodified for sm_100a,
+# oracle/ref/) timed on a B200 on the same 257^3 workload by
+# oracle/ref/time_ref_gpu.py: a recorded figure, stated beside the live one
+# (profiles/reference_build_rk3_257_and_reactors.md).
+REFERENCE_GPU_257 = {"ms_per_step": 69.84, "cell_updates_per_s": 2.43e8, "kind": "recorded",
+                     "what": "reference sources built unmodified for sm_100a, RK3 loop body with its own CFL "
+                             "step, median of 10 timed steps after 3 on one B200",
+                     "source": "profiles/reference_build_rk3_257_and_reactors.md"}
+
 WENO_PROFILE = os.path.join(ROOT, "profiles", "weno_air_flux_diff_161.md")
 WENO_PROFILE_NODES = 161 ** 3
 
@@ -933,6 +942,7 @@ def main():
             "roofline": roofline,
             "hbm_peak_gbs": hbm_peak,
             "cpu_baseline": cpu,
+            "reference_gpu": dict(REFERENCE_GPU_257) if (n == N_NODES and args.scheme == 72) else None,
             "e2e": e2e,
             "clocks": clk.summary(),
             "reacting": reacting,

@@ -94,14 +94,23 @@ def assemble(whole, slabs, arrays, axis):
     return out, seam
 
 
-def rel_diff(a, b):
-    """Largest difference relative to each variable plane's largest magnitude
-    in b (the three momentum planes sharing one scale)."""
-    scale = np.abs(b).reshape(b.shape[0], -1).max(axis=1)
-    if b.shape[0] >= 4:
+def plane_scale(*arrays):
+    """Largest magnitude of each variable plane over all the given (n, ...)
+    arrays, the three momentum planes sharing one scale."""
+    scale = np.max([np.abs(b).reshape(b.shape[0], -1).max(axis=1) for b in arrays], axis=0)
+    if scale.shape[0] >= 4:
         scale[1:4] = scale[1:4].max()
-    scale = np.where(scale == 0, 1.0, scale)
-    return float((np.abs(a - b).reshape(b.shape[0], -1) / scale[:, None]).max())
+    return np.where(scale == 0, 1.0, scale)
+
+
+def rel_diff(a, b, scale=None):
+    """Largest difference relative to each variable plane's largest magnitude
+    in b (the three momentum planes sharing one scale), or to `scale` (per
+    plane, e.g. plane_scale over every slab of a decomposition: a slab of gas
+    at rest has momenta at round-off level, which are no scale of their own)."""
+    if scale is None:
+        scale = plane_scale(b)
+    return float((np.abs(a - b).reshape(b.shape[0], -1) / np.asarray(scale)[:, None]).max())
 
 
 def run_rank(rank, world, port, spec, out):

@@ -12,7 +12,7 @@ import cases
 import mechanism
 import slabs as sl
 from gpuzone import GpuZone
-from slabzone import OracleSlabZone, assemble, rel_diff
+from slabzone import OracleSlabZone, assemble, plane_scale, rel_diff
 
 pytestmark = pytest.mark.gpu
 
@@ -91,8 +91,11 @@ def test_slab_run_on_the_gpu_matches_the_oracle_and_the_whole_block(case_fn, n, 
     for _ in range(3):
         assert run.step() == pytest.approx(ref.step(), rel=1e-13)
     torch.cuda.synchronize()
+    # every slab against the decomposition's scale: the Sod tube's outer slabs
+    # are gas at rest, whose momenta are round-off on both sides
+    scale = plane_scale(*[o["cv"] for o in oz])
     for g, o in zip(gz, oz):
-        assert rel_diff(g.get("cv"), o["cv"]) <= tol
+        assert rel_diff(g.get("cv"), o["cv"], scale) <= tol
     cv, seam = assemble(whole, parts, [g.get("cv") for g in gz], axis)
     assert seam <= 1e-13 * np.abs(cv).max()
     whole_gz = GpuZone(whole)
