@@ -299,9 +299,8 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
         }
         // a node the transport term leaves unchanged keeps its own state
         if (moved) {
-          bool ok = sg_transported(th, ns, q0, rY0, cq, crY, 0.5, T0, qm, Yf, Tf, pf);
           double pe = 0;
-          ok = ok && sg_transported(th, ns, q0, rY0, cq, crY, 1.0, Tf, qe, Y0, Te, pe);
+          const bool ok = sg_transported_pair(th, ns, q0, rY0, cq, crY, T0, qm, Yf, Tf, pf, qe, Y0, Te, pe);
           if (!ok) {
             reason = SG_NEWTON_FAILED;
             Tf = T0;
@@ -491,8 +490,8 @@ __global__ void sg_snapshot_kernel(Zone z, const Thermo *th, int n_nodes, double
       crY[l] = z.Cn[iq + (5 + l) * szq] * sc;
       moved |= crY[l] != 0.0;
     }
-    if (moved && !(sg_transported(th, ns, q0, rY0, cq, crY, 0.5, T0, qt, Yf, Tf, pf) &&
-          sg_transported(th, ns, q0, rY0, cq, crY, 1.0, Tf, qt, Ye, Te, pe))) {
+    double qm[5];
+    if (moved && !sg_transported_pair(th, ns, q0, rY0, cq, crY, T0, qm, Yf, Tf, pf, qt, Ye, Te, pe)) {
       // no transported state: the row falls back to the node's own (a
       // training sample of the reaction alone)
       Tf = Te = T0;

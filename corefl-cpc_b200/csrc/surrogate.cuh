@@ -138,6 +138,21 @@ __device__ inline bool sg_transported(const Thermo *th, int ns, const double *q0
   return temperature_newton(th, ns, Y, q[4], q[0], u * u + v * v + w * w, T, p);
 }
 
+// Both transported states of a node in one out-of-line call: the mid-step
+// state (f = 1/2, Newton from T0) the features are read at, and the end state
+// (f = 1, Newton from the mid-step T) the predicted change applies to.  With
+// two inlined sg_transported calls in one kernel, nvcc 12.9 for sm_100a
+// returned a wrong end state (a composition unrelated to q0 + cq and a
+// spurious negative temperature root) while the mid-step state was right;
+// the out-of-line form computes both correctly.
+static __device__ __noinline__ bool sg_transported_pair(const Thermo *th, int ns, const double *q0, const double *rY0,
+                                                        const double *cq, const double *crY, double T0, double *qm,
+                                                        double *Ym, double &Tm, double &pm, double *qe, double *Ye,
+                                                        double &Te, double &pe) {
+  if (!sg_transported(th, ns, q0, rY0, cq, crY, 0.5, T0, qm, Ym, Tm, pm)) return false;
+  return sg_transported(th, ns, q0, rY0, cq, crY, 1.0, Tm, qe, Ye, Te, pe);
+}
+
 // Weighted least-squares projection of Y onto {mu Y = Z0, Y >= 0}: the
 // correction of species k is proportional to (Y_k + 1e-12), so trace species
 // move least; species driven negative are clipped to 0 and frozen, and the
