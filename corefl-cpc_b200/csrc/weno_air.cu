@@ -160,10 +160,14 @@ __device__ __forceinline__ void air_face(const double *s, double *sflx, int c, i
 #pragma unroll
       for (int q = 0; q < NPF; ++q) {
         const int tq = t + q;
-        const double LF = L0 * s[T::spt(5, c, tq)] + L1 * s[T::spt(6, c, tq)] + L2 * s[T::spt(7, c, tq)] +
-                          L3 * s[T::spt(8, c, tq)] + L4 * s[T::spt(9, c, tq)];
-        const double LQ = L0 * s[T::spt(0, c, tq)] + L1 * s[T::spt(1, c, tq)] + L2 * s[T::spt(2, c, tq)] +
-                          L3 * s[T::spt(3, c, tq)] + L4 * s[T::spt(4, c, tq)];
+        double LF = L0 * s[T::spt(5, c, tq)] + L1 * s[T::spt(6, c, tq)] + L2 * s[T::spt(7, c, tq)] +
+                    L3 * s[T::spt(8, c, tq)];
+        double LQ = L0 * s[T::spt(0, c, tq)] + L1 * s[T::spt(1, c, tq)] + L2 * s[T::spt(2, c, tq)] +
+                    L3 * s[T::spt(3, c, tq)];
+        if (l != 1 && l != 2) {  // the rows of fields 1 and 2 have no energy term
+          LF += L4 * s[T::spt(9, c, tq)];
+          LQ += L4 * s[T::spt(4, c, tq)];
+        }
         const double hj = s[T::spt(11, c, tq)];
         if (q < NPF - 1) vp[q] = hj * (LF + lam * LQ);
         if (q > 0) vmn[q - 1] = hj * (LF - lam * LQ);

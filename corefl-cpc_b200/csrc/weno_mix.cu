@@ -307,10 +307,14 @@ __global__ void __launch_bounds__(256) weno_mix_flux_diff(Zone z, double eps_ref
 #pragma unroll
       for (int q = 0; q < NPF; ++q) {
         const int tq = t + q;
-        const double LF = L0 * s[T::spt(5, c, tq)] + L1 * s[T::spt(6, c, tq)] + L2 * s[T::spt(7, c, tq)] +
-                          L3 * s[T::spt(8, c, tq)] + L4 * s[T::spt(9, c, tq)] + tb * sbf[q];
-        const double LQ = L0 * s[T::spt(0, c, tq)] + L1 * s[T::spt(1, c, tq)] + L2 * s[T::spt(2, c, tq)] +
-                          L3 * s[T::spt(3, c, tq)] + L4 * s[T::spt(4, c, tq)] + tb * sbq[q];
+        double LF = L0 * s[T::spt(5, c, tq)] + L1 * s[T::spt(6, c, tq)] + L2 * s[T::spt(7, c, tq)] +
+                    L3 * s[T::spt(8, c, tq)];
+        double LQ = L0 * s[T::spt(0, c, tq)] + L1 * s[T::spt(1, c, tq)] + L2 * s[T::spt(2, c, tq)] +
+                    L3 * s[T::spt(3, c, tq)];
+        if (l != 1 && l != 2) {  // the rows of fields 1 and 2 have no energy or species term
+          LF = LF + L4 * s[T::spt(9, c, tq)] + tb * sbf[q];
+          LQ = LQ + L4 * s[T::spt(4, c, tq)] + tb * sbq[q];
+        }
         const double jq = s[T::spt(V::J, c, tq)];
         if (q < NPF - 1) vp[q] = 0.5 * jq * (LF + lam * LQ);
         if (q > 0) vmn[q - 1] = 0.5 * jq * (LF - lam * LQ);
