@@ -949,7 +949,7 @@ def main():
                        "nodes": f"{n}^3", "global_nodes": nodes * world,
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cv alone "
                        f"{5 * P * 8 / 1e6:.0f} MB)", "weno_tile_variants": tiles, "autotune_ms": tile_ms,
-                       "viscous_form": ["staged", "ring (2 CTAs/SM)", "ring (3 CTAs/SM)"][visc_var], "viscous_form_ms": visc_ms},
+                       "viscous_form": ["staged", "ring", "ring + L2 prefetch of the metric"][visc_var], "viscous_form_ms": visc_ms},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "gpu_launches": launches,
             "roofline": roofline,

@@ -466,9 +466,9 @@ class Context:
         return list(ch), [list(ms[d * TILE_VARIANTS:(d + 1) * TILE_VARIANTS]) for d in range(3)]
 
     def viscous_variant(self, set_to=None):
-        """The fused air viscous kernel's form (0 staged, 1 ring at two CTAs
-        per SM, 2 ring at three) and the last autotune's per-launch times;
-        set_to selects a form."""
+        """The fused air viscous kernel's form (0 staged, 1 ring, 2 ring with
+        the L2 prefetch of the metric two planes ahead) and the last
+        autotune's per-launch times; set_to selects a form."""
         v = ctypes.c_int(set_to if set_to is not None else 0)
         ms = (ctypes.c_double * 3)()
         self._ck(self.L.cfk_viscous_variant(self.h, 1 if set_to is not None else 0, ctypes.byref(v), ms),

@@ -42,7 +42,7 @@ struct cfk_ctx {
   long long graph_kernels = 0;
   // tile variant of each sweep of the WENO flux kernels (tile autotuner)
   int tile_var[3] = {0, 0, 0};
-  int visc_var = 0;                 // fused air viscous kernel: 0 staged, 1/2 cp.async ring at 2/3 CTAs per SM
+  int visc_var = 0;                 // fused air viscous kernel: 0 staged, 1 cp.async ring, 2 ring + L2 prefetch
   double visc_ms[3] = {0, 0, 0};    // their times in the last autotune (ms per launch)
   // phase timing with CUDA events (plain steps only)
   bool profiling = false;

@@ -251,6 +251,9 @@ __device__ __forceinline__ void cp_async8(double *dst, const double *src) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
 }
+__device__ __forceinline__ void prefetch_l2(const double *p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -313,8 +316,11 @@ __device__ __forceinline__ void ring_face(const RingSmem &S, const double *__res
 }  // namespace
 
 // MINB: CTAs per SM the register budget is sized for (2: no spills; 3: about
-// 80 registers with a few spills, 24 warps per SM).
-template <int MINB>
+// 80 registers with a few spills, 24 warps per SM).  PF: with the request of
+// plane k+2's dynamic values, also ask L2 for its metric and J (the faces of
+// plane k+2 read them through L1 two planes later), so that those loads no
+// longer wait on DRAM.
+template <int MINB, bool PF>
 __global__ void __launch_bounds__(kFT, MINB) viscous_air_ring(Zone z, double Pr) {
   extern __shared__ __align__(16) double rsm[];
   const double cp_pr = kCpAir / Pr;
@@ -384,6 +390,17 @@ __global__ void __launch_bounds__(kFT, MINB) viscous_air_ring(Zone z, double Pr)
       for (int q = 0; q < 4; ++q) S.dzp[q][py][px] = S.dyn[sn][q][py][px] - S.dyn[sp][q][py][px];
     }
     if (k + 2 <= k_end) request(k + 2, sp);  // plane k+2 into the slot of plane k-1
+    if (PF && k + 2 <= k_end) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        int px, py;
+        if (!point_ok(threadIdx.x + r * kFT, px, py)) continue;
+        const int64_t id = d.idx(g, i0 - 1 + px, j0 - 1 + py, k + 2);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) prefetch_l2(met + id + m * sz);
+        prefetch_l2(jac + id);
+      }
+    }
     cp_async_commit();
     __syncthreads();
     constexpr int kNXF = kFY * (kFX + 1), kNYF = (kFY + 1) * kFX;
@@ -440,19 +457,21 @@ cudaError_t viscous_air_init_attributes() {
   cudaError_t e = cudaFuncSetAttribute(viscous_air_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(FusedSmem));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(viscous_air_ring<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
+  e = cudaFuncSetAttribute(viscous_air_ring<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(RingSmem));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(viscous_air_ring<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RingSmem));
+  return cudaFuncSetAttribute(viscous_air_ring<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(RingSmem));
 }
 
 // compute_viscous_flux for air (reference src/ViscousScheme.cu:7-40): one
-// launch for all directions; var 0 the staged kernel, 1 the ring kernel at
-// two CTAs per SM, 2 the ring kernel at three.
+// launch for all directions; var 0 the staged kernel, 1 the ring kernel,
+// 2 the ring kernel with the L2 prefetch of the metric two planes ahead.
 cudaError_t launch_viscous_air(const Zone &z, const Param &p, cudaStream_t st, int *n_launch, int var) {
   const Dims &d = z.d;
   const dim3 grid((d.mx + kFX - 1) / kFX, (d.my + kFY - 1) / kFY, (d.mz + kFZ - 1) / kFZ);
-  if (var == 1) viscous_air_ring<2><<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
-  else if (var == 2) viscous_air_ring<3><<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
+  if (var == 1) viscous_air_ring<2, false><<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
+  else if (var == 2) viscous_air_ring<2, true><<<grid, kFT, sizeof(RingSmem), st>>>(z, p.Pr);
   else viscous_air_fused<<<grid, kFT, sizeof(FusedSmem), st>>>(z, p.Pr);
   *n_launch += 1;
   return cudaGetLastError();

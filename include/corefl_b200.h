@@ -244,8 +244,9 @@ int cfk_autotune_tiles(cfk_ctx *ctx, int reps, double *ms_out, int *choice_out, 
  * the fused viscous kernel — 0: all per-node inputs staged in shared memory
  * (two plane slots); 1: only u, v, w, T, mu staged, in a three-slot ring
  * filled by cp.async ahead of use, with the metric read through L1, two CTAs
- * per SM; 2: the same at three CTAs per SM (fewer registers) — and keeps the
- * fastest (the same arithmetic; they agree to the last bits).
+ * per SM; 2: the same with the metric and J of the plane two ahead
+ * prefetched into L2 — and keeps the fastest (the same arithmetic; they agree
+ * to the last bits).
  * cfk_viscous_variant reads (set = 0) or sets (set = 1) the form in *var;
  * ms (optional, 3 doubles) receives the last autotune's times per launch. */
 int cfk_viscous_variant(cfk_ctx *ctx, int set, int *var, double *ms);

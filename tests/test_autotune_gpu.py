@@ -103,7 +103,8 @@ def test_autotune_mixture_and_pv_noop():
 
 @pytest.mark.parametrize("name", ["wave_3d", "walls_3d", "tube_2d"])
 def test_viscous_forms_identical_and_in_parity(name):
-    """The staged and the two cp.async-ring forms of the fused air viscous kernel
+    """The staged and the two cp.async-ring forms (the second with the L2
+    prefetch of the metric) of the fused air viscous kernel
     agree to the last bits (blocks not a multiple of the 32 x 8 x 32 tile, 2-D
     and 3-D, walls widening the boundary ranges) and each matches the oracle's
     viscous flux at the single-call bar."""
