@@ -46,7 +46,7 @@ N_NODES = 257
 # sqrt = 1; fma = 2) is 2980: face set-up 93; per characteristic field the left
 # eigenvector row 14, projection of 8 points 186, two WENO7-Z sides 361, times
 # 5 fields; back-projection 44; staging share 30, difference share 10.
-FLOPS_PER_FACE_WENO7_CH = 3281.7
+FLOPS_PER_FACE_WENO7_CH = 3214.9
 FLOPS_PER_FACE_WENO7_CH_HAND = 2980.0
 
 
