@@ -926,11 +926,14 @@ def main():
     ctx.close()
 
     reacting = None if args.no_reacting else reacting_bench(args, local, world, dist)
-    # the surrogate measurement runs on rank 0 only (its window is one GPU's work)
-    surrogate = None if (args.no_surrogate or args.no_reacting or rank != 0) else surrogate_bench(args, local)
-    surrogate_flow = (None if (args.no_surrogate_flow or args.no_reacting or rank != 0)
+    # the surrogate and reacting-flow measurements are one GPU's work: they run
+    # in single-GPU runs only, so that a multi-GPU run does not hold every GPU
+    # while one rank works through them
+    single = world == 1
+    surrogate = None if (args.no_surrogate or args.no_reacting or not single) else surrogate_bench(args, local)
+    surrogate_flow = (None if (args.no_surrogate_flow or args.no_reacting or not single)
                       else surrogate_flow_bench(args, local))
-    mixing_layer = (None if (args.no_mixing_layer or args.no_reacting or rank != 0)
+    mixing_layer = (None if (args.no_mixing_layer or args.no_reacting or not single)
                     else mixing_layer_bench(args, local))
 
     if rank == 0:
