@@ -480,7 +480,7 @@ def surrogate_flow_bench(args, local):
     small = cases.reflected_shock_tube(mech, nx, ny, length=0.02, height=0.004, mach=2.6)
     n = small.N
     traces, rows = {}, None
-    for mode in ("plain", "surrogate", "surrogate_all"):
+    for mode in ("plain", "surrogate", "surrogate_10", "surrogate_all"):
         ctx, zone = _flow_ctx(mech, small, local, 7)
         if mode == "plain":
             X = torch.empty((W * n, sg.cf.SG_NIN), dtype=torch.float32, device=dev)
@@ -543,7 +543,7 @@ def surrogate_flow_bench(args, local):
         "tau_ign_plain_s": tau_p, "tau_largest_rise_plain_s": trise_p, "T_peak_plain_K": pk_p,
         "plain_window_ms": traces["plain"][2], "ignition_delay": "peak T risen by 400 K",
         "note": "the plain window includes recording the training rows"}
-    for mode in ("surrogate", "surrogate_all"):
+    for mode in ("surrogate", "surrogate_10", "surrogate_all"):
         tau_s, pk_s, trise_s = ignition(traces[mode])
         out["ignition_window"][mode] = {
             "gate": GATES[mode] or "default", "tau_ign_s": tau_s, "tau_ign_rel_err": abs(tau_s - tau_p) / tau_p,
@@ -565,7 +565,9 @@ def surrogate_flow_bench(args, local):
     return out
 
 
-GATES = {"surrogate": {}, "surrogate_all": {"min_substeps": 0.0}}
+# gates of the ignition window: the default (few-substeps threshold 50), the
+# threshold at 10 substeps, and the rule off
+GATES = {"surrogate": {}, "surrogate_10": {"min_substeps": 10.0}, "surrogate_all": {"min_substeps": 0.0}}
 
 
 def _stat_summary(stats):

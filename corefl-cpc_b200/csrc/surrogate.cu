@@ -310,13 +310,23 @@ __global__ void __launch_bounds__(256, 1) sg_step_kernel(const __grid_constant__
       }
       double f[kSgIn];
       sg_raw_features(Tf, pf, Yf, ns, a.dt, f);
+      // the range check runs in raw feature units, with an excursion of
+      // 1e-3 max(1, |mean|) allowed beyond the training range (a feature that
+      // sits at an end of its range in most rows, such as a mass fraction at
+      // zero, must not fall out by the rounding of the stored bounds), plus
+      // ood_margin standard deviations
       bool ood = false;
       for (int c = 0; c < kSgIn; ++c) {
-        const double dev = f[c] - (double)a.nrm.in_mean[c];
-        const float xs = (float)(dev * (double)a.nrm.in_rstd[c]);
-        x[c] = xs;
-        if (a.nrm.in_rstd[c] == 0.f) ood |= fabs(dev) > 1e-3 * fmax(1.0, fabs((double)a.nrm.in_mean[c]));
-        else ood |= xs < a.nrm.in_lo[c] - a.gate.ood_margin || xs > a.nrm.in_hi[c] + a.gate.ood_margin;
+        const double mean = (double)a.nrm.in_mean[c], rs = (double)a.nrm.in_rstd[c];
+        const double dev = f[c] - mean;
+        x[c] = (float)(dev * rs);
+        const double tol = 1e-3 * fmax(1.0, fabs(mean));
+        if (rs == 0.0) {
+          ood |= fabs(dev) > tol;
+        } else {
+          const double m = a.gate.ood_margin / rs + tol;
+          ood |= dev < (double)a.nrm.in_lo[c] / rs - m || dev > (double)a.nrm.in_hi[c] / rs + m;
+        }
       }
       // expected substeps of the plain integrator (its substep plan)
       double tau = a.z.reaction_timeScale[id];

@@ -460,7 +460,8 @@ int cfk_local_time_step_static(const cfk_param *param, const cfk_zone *zone, dou
 #define CFK_SG_NOUT 11
 
 typedef struct cfk_surrogate_gate {
-  double ood_margin;     /* allowed excursion beyond the training range (standardised units) */
+  double ood_margin;     /* allowed excursion beyond the training range (standardised units), on top of
+                            1e-3 max(1, |training mean|) in the feature's own units */
   double dT_max;         /* |dT| per step (K) above which a node takes the plain integrator */
   double dT_consistency; /* |network dT - energy-consistent dT| (K) above which it does */
   double judge_tol_T;    /* judged node: |T_surrogate - T_plain| tolerance (K) */
