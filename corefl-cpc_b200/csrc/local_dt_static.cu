@@ -1,7 +1,8 @@
 // Local CFL time step with its grid minimum, in a form that allocates no
-// device memory: for callers that cannot call cudaMalloc — a host that runs
-// inside a CUDA graph it is building, under a memory-pool policy that forbids
-// allocations after start-up, or that owns all device memory itself.  The
+// device memory: for callers that cannot call cudaMalloc — a host whose
+// memory policy forbids allocations after start-up (a pool sized once), one
+// that owns all device memory itself, or a time-critical loop in which a
+// cudaMalloc would synchronise the device.  The
 // context-based entry point needs a context (whose creation allocates); this
 // one takes the settings and the zone directly and keeps its scratch in a
 // file-scope device array instead.

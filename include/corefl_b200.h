@@ -424,9 +424,9 @@ long long cfk_kernel_launches(const cfk_ctx *ctx);
 /* ---- allocation-free variant ------------------------------------------- */
 /* No counterpart in the reference.  The local CFL step (dt_local and its grid
  * minimum, written to *dt_min_device) for callers that cannot call
- * cudaMalloc: a host that is itself building a CUDA graph, a memory-pool
- * policy that forbids allocation after start-up, or a framework that owns all
- * device memory.  It needs no context and allocates nothing: its scratch (one
+ * cudaMalloc: a memory policy that forbids allocation after start-up (a pool
+ * sized once), a framework that owns all device memory, or a time-critical
+ * loop in which a cudaMalloc would synchronise the device.  It needs no context and allocates nothing: its scratch (one
  * partial minimum per 256-node row segment, ceil(mx/256)*my*mz <= 262144, i.e.
  * 2 MiB) is a file-scope device array that every GPU loading the library holds
  * until exit.  The first call on a device looks up that array's device address

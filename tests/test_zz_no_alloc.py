@@ -1,8 +1,8 @@
 """The allocation-free local time step (cfk_local_time_step_static).
 
-Some callers cannot allocate device memory (a host building a CUDA graph, a
-memory-pool policy that forbids allocation after start-up, a framework that
-owns all device memory).  This entry point gives them the CFL step without a
+Some callers cannot allocate device memory (a memory policy that forbids
+allocation after start-up, a framework that owns all device memory, a
+time-critical loop in which a cudaMalloc would synchronise the device).  This entry point gives them the CFL step without a
 context: its scratch is a file-scope device array.  The tests call it through
 the C ABI twice in a row — on two different zones, so that scratch left over
 from the first call cannot leak into the second — and check both results
