@@ -19,6 +19,8 @@
 //   refharness <case dir> react <steps> <dt>
 //        reaction steps only: wu_reaction_step with Cn = 0 on every node
 //        (src/StrangSplitting.cu:373-421, constant-volume reactors)
+//   refharness <case dir> reactlast <steps> <dt>
+//        the same reaction steps, writing only the state after the last one
 //   refharness <case dir> rk3time <steps> <warm-up>
 //   refharness <case dir> reacttime <steps> <dt> <warm-up>
 //        the same steps timed with CUDA events, without any file output:
@@ -339,9 +341,13 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
   r.initialise();
   r.start();
   if (mode == "rk3time" || mode == "reacttime") return timed(r, mode, steps, warmup, react_dt);
-  r.dump_grid();
-  r.dump_param();
-  r.dump_state(0);
+  // reactlast: the state after the last step only (a large batch of reactors)
+  const bool last_only = mode == "reactlast";
+  if (!last_only) {
+    r.dump_grid();
+    r.dump_param();
+    r.dump_state(0);
+  }
   if (mode == "visc") {
     r.viscous_once();
     return 0;
@@ -354,8 +360,10 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
       dt = r.wu_step(s);
     else
       dt = r.react_step(react_dt);
-    write_value("out/dt_" + std::to_string(s) + ".bin", dt);
-    r.dump_state(s);
+    if (!last_only || s == steps) {
+      write_value("out/dt_" + std::to_string(s) + ".bin", dt);
+      r.dump_state(s);
+    }
     std::printf("refharness: step %d dt %.17g\n", s, dt);
   }
   return 0;
@@ -365,18 +373,18 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
 
 int main(int argc, char *argv[]) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react|visc <steps> [dt]\n"
+    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react|reactlast|visc <steps> [dt]\n"
                          "       refharness <case dir> rk3time <steps> <warm-up steps>\n"
                          "       refharness <case dir> reacttime <steps> <dt> <warm-up steps>\n");
     return 2;
   }
   const std::string mode = argv[2];
   const int steps = std::atoi(argv[3]);
-  const bool react = mode == "react" || mode == "reacttime";
+  const bool react = mode == "react" || mode == "reactlast" || mode == "reacttime";
   const double react_dt = react && argc > 4 ? std::atof(argv[4]) : 0.0;
   const int warmup = mode == "rk3time" ? (argc > 4 ? std::atoi(argv[4]) : 0)
                                        : (mode == "reacttime" && argc > 5 ? std::atoi(argv[5]) : 0);
-  if (mode != "rk3" && mode != "wu" && mode != "react" && mode != "visc" && mode != "rk3time" &&
+  if (mode != "rk3" && mode != "wu" && mode != "react" && mode != "reactlast" && mode != "visc" && mode != "rk3time" &&
       mode != "reacttime") {
     std::fprintf(stderr, "refharness: unknown mode %s\n", mode.c_str());
     return 2;
