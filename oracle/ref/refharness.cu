@@ -19,8 +19,9 @@
 //   refharness <case dir> react <steps> <dt>
 //        reaction steps only: wu_reaction_step with Cn = 0 on every node
 //        (src/StrangSplitting.cu:373-421, constant-volume reactors)
+//   refharness <case dir> rk3last <steps>
 //   refharness <case dir> reactlast <steps> <dt>
-//        the same reaction steps, writing only the state after the last one
+//        the same steps, writing only the state after the last one
 //   refharness <case dir> rk3time <steps> <warm-up>
 //   refharness <case dir> reacttime <steps> <dt> <warm-up>
 //        the same steps timed with CUDA events, without any file output:
@@ -341,8 +342,8 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
   r.initialise();
   r.start();
   if (mode == "rk3time" || mode == "reacttime") return timed(r, mode, steps, warmup, react_dt);
-  // reactlast: the state after the last step only (a large batch of reactors)
-  const bool last_only = mode == "reactlast";
+  // reactlast, rk3last: the state after the last step only (large blocks)
+  const bool last_only = mode == "reactlast" || mode == "rk3last";
   if (!last_only) {
     r.dump_grid();
     r.dump_param();
@@ -354,7 +355,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
   }
   for (int s = 1; s <= steps; ++s) {
     real dt = 0;
-    if (mode == "rk3")
+    if (mode == "rk3" || mode == "rk3last")
       dt = r.rk3_step(s);
     else if (mode == "wu")
       dt = r.wu_step(s);
@@ -373,7 +374,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
 
 int main(int argc, char *argv[]) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: refharness <case dir> rk3|wu|react|reactlast|visc <steps> [dt]\n"
+    std::fprintf(stderr, "usage: refharness <case dir> rk3|rk3last|wu|react|reactlast|visc <steps> [dt]\n"
                          "       refharness <case dir> rk3time <steps> <warm-up steps>\n"
                          "       refharness <case dir> reacttime <steps> <dt> <warm-up steps>\n");
     return 2;
@@ -384,7 +385,8 @@ int main(int argc, char *argv[]) {
   const double react_dt = react && argc > 4 ? std::atof(argv[4]) : 0.0;
   const int warmup = mode == "rk3time" ? (argc > 4 ? std::atoi(argv[4]) : 0)
                                        : (mode == "reacttime" && argc > 5 ? std::atoi(argv[5]) : 0);
-  if (mode != "rk3" && mode != "wu" && mode != "react" && mode != "reactlast" && mode != "visc" && mode != "rk3time" &&
+  if (mode != "rk3" && mode != "rk3last" && mode != "wu" && mode != "react" && mode != "reactlast" && mode != "visc" &&
+      mode != "rk3time" &&
       mode != "reacttime") {
     std::fprintf(stderr, "refharness: unknown mode %s\n", mode.c_str());
     return 2;
