@@ -20,6 +20,7 @@
 //        reaction steps only: wu_reaction_step with Cn = 0 on every node
 //        (src/StrangSplitting.cu:373-421, constant-volume reactors)
 //   refharness <case dir> rk3last <steps>
+//   refharness <case dir> wulast <steps>
 //   refharness <case dir> reactlast <steps> <dt>
 //        the same steps, writing only the state after the last one
 //   refharness <case dir> rk3time <steps> <warm-up>
@@ -343,7 +344,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
   r.start();
   if (mode == "rk3time" || mode == "reacttime") return timed(r, mode, steps, warmup, react_dt);
   // reactlast, rk3last: the state after the last step only (large blocks)
-  const bool last_only = mode == "reactlast" || mode == "rk3last";
+  const bool last_only = mode == "reactlast" || mode == "rk3last" || mode == "wulast";
   if (!last_only) {
     r.dump_grid();
     r.dump_param();
@@ -357,7 +358,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
     real dt = 0;
     if (mode == "rk3" || mode == "rk3last")
       dt = r.rk3_step(s);
-    else if (mode == "wu")
+    else if (mode == "wu" || mode == "wulast")
       dt = r.wu_step(s);
     else
       dt = r.react_step(react_dt);
@@ -374,7 +375,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
 
 int main(int argc, char *argv[]) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: refharness <case dir> rk3|rk3last|wu|react|reactlast|visc <steps> [dt]\n"
+    std::fprintf(stderr, "usage: refharness <case dir> rk3|rk3last|wu|wulast|react|reactlast|visc <steps> [dt]\n"
                          "       refharness <case dir> rk3time <steps> <warm-up steps>\n"
                          "       refharness <case dir> reacttime <steps> <dt> <warm-up steps>\n");
     return 2;
@@ -385,8 +386,8 @@ int main(int argc, char *argv[]) {
   const double react_dt = react && argc > 4 ? std::atof(argv[4]) : 0.0;
   const int warmup = mode == "rk3time" ? (argc > 4 ? std::atoi(argv[4]) : 0)
                                        : (mode == "reacttime" && argc > 5 ? std::atoi(argv[5]) : 0);
-  if (mode != "rk3" && mode != "rk3last" && mode != "wu" && mode != "react" && mode != "reactlast" && mode != "visc" &&
-      mode != "rk3time" &&
+  if (mode != "rk3" && mode != "rk3last" && mode != "wu" && mode != "wulast" && mode != "react" &&
+      mode != "reactlast" && mode != "visc" && mode != "rk3time" &&
       mode != "reacttime") {
     std::fprintf(stderr, "refharness: unknown mode %s\n", mode.c_str());
     return 2;
