@@ -8,6 +8,9 @@ the C ABI:
 * wave: the 257^3 curvilinear periodic wave (WENO7 characteristic + 2nd-order
   viscous flux), SSP-RK3 (the reference's RK3 loop body, src/RK.cuh:89-206;
   cfk_rk3_step);
+* sod: the 400 x 7 Sod tube (WENO5 characteristic, SSP-RK3, CFL 0.5; the
+  reference initialises it from setup.txt), `--sod-steps` steps (250 reach
+  t ~ 0.2);
 * tube: the 2048 x 512 reflected-shock tube (stoichiometric H2-O2 with 70 %
   Ar, PREMIX mechanism, wall-normal stretching 1.02, WENO5 characteristic +
   mixture-averaged viscous fluxes, adiabatic no-slip walls), Wu splitting with
@@ -20,7 +23,7 @@ pointwise relative differences of the conserved variables (partial densities
 included) after the last step.  Run on a machine with a GPU after
 `make -C oracle/ref REF=<reference checkout>`:
 
-    python oracle/ref/compare_flow_gpu.py [--case wave|tube|all] [--steps 2] [--fixed-dt DT]
+    python oracle/ref/compare_flow_gpu.py [--case wave|sod|tube|all] [--steps 2] [--fixed-dt DT]
 """
 from __future__ import annotations
 
@@ -61,7 +64,7 @@ def _tube_spec(nx: int, ny: int) -> Spec:
                 reference_state=mrf._struct("shocked", st) + mrf._ref("shocked"))
 
 
-def compare(name: str, spec: Spec, mode: str, steps: int, fixed_dt: float) -> dict:
+def compare(name: str, spec: Spec, mode: str, steps: int, fixed_dt: float, with_oracle: bool = False) -> dict:
     case = spec.case
     if fixed_dt > 0:
         case.param.update(fixed_dt=1, dt=fixed_dt)
@@ -88,7 +91,20 @@ def compare(name: str, spec: Spec, mode: str, steps: int, fixed_dt: float) -> di
         dt = gz.ctx.rk3_step() if mode == "rk3last" else gz.ctx.wu_splitting_step(schedule=1)
     cv = interior_planes(case, gz.get("cv"))
     ns = case.param["n_spec"]
-    return {"case": name, "block": f"{case.mx}x{case.my}x{case.mz}", "steps": steps,
+    extra = {}
+    if with_oracle:
+        # the CPU restatement of the same steps, against both
+        sys.path.insert(0, os.path.dirname(HERE))
+        import pyoracle
+
+        oz = pyoracle.OracleZone(case)
+        oz.initialize()
+        for _ in range(steps):
+            oz.step() if mode == "rk3last" else oz.wu_splitting_step()
+        cv_o = interior_planes(case, oz["cv"])
+        extra = {"oracle_vs_reference_normwise": rel_err(cv_o, cv_ref),
+                 "library_vs_oracle_normwise": rel_err(cv, cv_o)}
+    return {**extra, "case": name, "block": f"{case.mx}x{case.my}x{case.mz}", "steps": steps,
             "dt_mode": "fixed" if fixed_dt > 0 else "CFL", "dt_reference": dt_ref, "dt_library": dt,
             "dt_rel_diff": abs(dt - dt_ref) / abs(dt_ref) if dt_ref else None,
             "cv_normwise_rel_diff": rel_err(cv, cv_ref),
@@ -97,7 +113,9 @@ def compare(name: str, spec: Spec, mode: str, steps: int, fixed_dt: float) -> di
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", choices=["wave", "tube", "all"], default="all")
+    ap.add_argument("--case", choices=["wave", "sod", "tube", "all"], default="all")
+    ap.add_argument("--sod-steps", type=int, default=250)
+    ap.add_argument("--oracle", action="store_true", help="also run the CPU restatement and compare it with both")
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--fixed-dt", type=float, default=0.0, help="fixed time step (0: the CFL step)")
     ap.add_argument("--n", type=int, default=257, help="wave: nodes per direction")
@@ -106,9 +124,11 @@ def main():
     if not os.path.exists(mrf.HARNESS):
         sys.exit(f"{mrf.HARNESS} not built (make -C oracle/ref REF=<reference checkout>)")
     if a.case in ("wave", "all"):
-        print(json.dumps(compare("wave", trg._wave_spec(a.n), "rk3last", a.steps, a.fixed_dt)), flush=True)
+        print(json.dumps(compare("wave", trg._wave_spec(a.n), "rk3last", a.steps, a.fixed_dt, a.oracle)), flush=True)
+    if a.case in ("sod", "all"):
+        print(json.dumps(compare("sod", mrf._sod(), "rk3last", a.sod_steps, a.fixed_dt, a.oracle)), flush=True)
     if a.case in ("tube", "all"):
-        print(json.dumps(compare("tube", _tube_spec(*a.tube), "wulast", a.steps, a.fixed_dt)), flush=True)
+        print(json.dumps(compare("tube", _tube_spec(*a.tube), "wulast", a.steps, a.fixed_dt, a.oracle)), flush=True)
 
 
 if __name__ == "__main__":
