@@ -36,8 +36,8 @@ constexpr int kNQ = 13;  // staged values per point: Q0..4, G0..4, p, J/2, lambd
 // columns on the lanes.
 template <int DIR, int VAR>
 struct TileShape {
-  static constexpr int TN = DIR == 0 ? (VAR == 0 ? 63 : VAR == 1 ? 127 : 31) : (VAR == 0 ? 15 : VAR == 1 ? 31 : 63);
-  static constexpr int C = DIR == 0 ? (VAR == 0 ? 4 : VAR == 1 ? 2 : 8) : (VAR == 0 ? 32 : VAR == 1 ? 16 : 8);
+  static constexpr int TN = DIR == 0 ? (VAR == 0 ? 63 : VAR == 1 ? 15 : 31) : (VAR == 0 ? 15 : VAR == 1 ? 31 : 63);
+  static constexpr int C = DIR == 0 ? (VAR == 0 ? 4 : VAR == 1 ? 16 : 8) : (VAR == 0 ? 32 : VAR == 1 ? 16 : 8);
 };
 
 template <int DIR, int ORD, int VAR = 0>
