@@ -44,24 +44,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import make_ref_fixtures as mrf  # noqa: E402
 import time_ref_gpu as trg  # noqa: E402
-from make_ref_fixtures import Spec, cases  # noqa: E402
+from make_ref_fixtures import Spec  # noqa: E402
 from gpuzone import GpuZone, interior_planes, pointwise_rel_err, rel_err  # noqa: E402
-
-import mechanism  # noqa: E402  (on the path through make_ref_fixtures)
-
-
-def _tube_spec(nx: int, ny: int) -> Spec:
-    mech = mechanism.load("premix_h2_ar")
-    c = cases.reflected_shock_tube(mech, nx, ny)
-    p = c.param
-    # the reference state: the gas behind the incident shock (its density and
-    # speed set the WENO epsilon scale, as in the case's own parameters)
-    y = {mech.species[k]: float(c.sv[k, 0]) for k in range(mech.n_spec)}
-    i2 = int(np.argmin(np.abs(c.bv[0] - p["rho_ref"])))
-    st = dict({"type": "inflow", "label": 5, "density": float(p["rho_ref"]), "velocity": float(p["v_ref"]),
-               "pressure": float(c.bv[4, i2]), "u": 1.0, "v": 0.0, "w": 0.0}, **y)
-    return Spec(f"tube_{nx}x{ny}_wu", c, "wu", 0, mech_name="premix_h2_ar",
-                reference_state=mrf._struct("shocked", st) + mrf._ref("shocked"))
 
 
 def compare(name: str, spec: Spec, mode: str, steps: int, fixed_dt: float, with_oracle: bool = False) -> dict:
@@ -128,7 +112,7 @@ def main():
     if a.case in ("sod", "all"):
         print(json.dumps(compare("sod", mrf._sod(), "rk3last", a.sod_steps, a.fixed_dt, a.oracle)), flush=True)
     if a.case in ("tube", "all"):
-        print(json.dumps(compare("tube", _tube_spec(*a.tube), "wulast", a.steps, a.fixed_dt, a.oracle)), flush=True)
+        print(json.dumps(compare("tube", trg._tube_spec(*a.tube), "wulast", a.steps, a.fixed_dt, a.oracle)), flush=True)
 
 
 if __name__ == "__main__":

@@ -24,6 +24,7 @@
 //   refharness <case dir> reactlast <steps> <dt>
 //        the same steps, writing only the state after the last one
 //   refharness <case dir> rk3time <steps> <warm-up>
+//   refharness <case dir> wutime <steps> <warm-up>
 //   refharness <case dir> reacttime <steps> <dt> <warm-up>
 //        the same steps timed with CUDA events, without any file output:
 //        one JSON line on stdout with the per-step times
@@ -65,7 +66,7 @@ __global__ void wu_reaction_step(DZone *zone, const DParameter *param, real dt);
 
 namespace {
 
-// Timed runs (rk3time, reacttime) check launches without synchronising, so
+// Timed runs (rk3time, wutime, reacttime) check launches without synchronising, so
 // the timed region holds only the reference's own synchronisation points.
 bool g_sync_checks = true;
 
@@ -303,10 +304,15 @@ template<MixtureModel M> struct Run {
 // which is where every reference kernel driven here is launched.  Prints one
 // JSON line: the total and the per-step times (ms) and the node count.
 template<MixtureModel M> int timed(Run<M> &r, const std::string &mode, int steps, int warmup, double react_dt) {
-  const bool rk3 = mode == "rk3time";
-  if (!rk3) r.react_step(react_dt, true);  // zero Cn; this step counts as a warm-up step
+  const bool rk3 = mode == "rk3time", wu = mode == "wutime";
+  if (!rk3 && !wu) r.react_step(react_dt, true);  // zero Cn; this step counts as a warm-up step
+  auto one = [&](int s) -> real {
+    if (rk3) return r.rk3_step(s);
+    if (wu) return r.wu_step(s);
+    return r.react_step(react_dt, false);
+  };
   g_sync_checks = false;
-  for (int s = 1; s <= warmup; ++s) rk3 ? r.rk3_step(s) : r.react_step(react_dt, false);
+  for (int s = 1; s <= warmup; ++s) one(s);
   g_sync_checks = true;
   check("warm-up steps");
   g_sync_checks = false;
@@ -315,7 +321,7 @@ template<MixtureModel M> int timed(Run<M> &r, const std::string &mode, int steps
   real dt = 0;
   cudaEventRecord(ev[0]);
   for (int s = 1; s <= steps; ++s) {
-    dt = rk3 ? r.rk3_step(warmup + s) : r.react_step(react_dt, false);
+    dt = one(warmup + s);
     cudaEventRecord(ev[static_cast<size_t>(s)]);
   }
   cudaEventSynchronize(ev.back());
@@ -342,7 +348,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
   Run<M> r(parameter, mesh);
   r.initialise();
   r.start();
-  if (mode == "rk3time" || mode == "reacttime") return timed(r, mode, steps, warmup, react_dt);
+  if (mode == "rk3time" || mode == "wutime" || mode == "reacttime") return timed(r, mode, steps, warmup, react_dt);
   // reactlast, rk3last: the state after the last step only (large blocks)
   const bool last_only = mode == "reactlast" || mode == "rk3last" || mode == "wulast";
   if (!last_only) {
@@ -376,7 +382,7 @@ template<MixtureModel M> int run(cfd::Parameter &parameter, cfd::Mesh &mesh, con
 int main(int argc, char *argv[]) {
   if (argc < 4) {
     std::fprintf(stderr, "usage: refharness <case dir> rk3|rk3last|wu|wulast|react|reactlast|visc <steps> [dt]\n"
-                         "       refharness <case dir> rk3time <steps> <warm-up steps>\n"
+                         "       refharness <case dir> rk3time|wutime <steps> <warm-up steps>\n"
                          "       refharness <case dir> reacttime <steps> <dt> <warm-up steps>\n");
     return 2;
   }
@@ -384,15 +390,15 @@ int main(int argc, char *argv[]) {
   const int steps = std::atoi(argv[3]);
   const bool react = mode == "react" || mode == "reactlast" || mode == "reacttime";
   const double react_dt = react && argc > 4 ? std::atof(argv[4]) : 0.0;
-  const int warmup = mode == "rk3time" ? (argc > 4 ? std::atoi(argv[4]) : 0)
+  const int warmup = (mode == "rk3time" || mode == "wutime") ? (argc > 4 ? std::atoi(argv[4]) : 0)
                                        : (mode == "reacttime" && argc > 5 ? std::atoi(argv[5]) : 0);
   if (mode != "rk3" && mode != "rk3last" && mode != "wu" && mode != "wulast" && mode != "react" &&
-      mode != "reactlast" && mode != "visc" && mode != "rk3time" &&
+      mode != "reactlast" && mode != "visc" && mode != "rk3time" && mode != "wutime" &&
       mode != "reacttime") {
     std::fprintf(stderr, "refharness: unknown mode %s\n", mode.c_str());
     return 2;
   }
-  if ((mode == "rk3time" || mode == "reacttime") && (steps < 1 || warmup < 0)) {
+  if ((mode == "rk3time" || mode == "wutime" || mode == "reacttime") && (steps < 1 || warmup < 0)) {
     std::fprintf(stderr, "refharness: a timed run needs steps >= 1 and warm-up steps >= 0\n");
     return 2;
   }

@@ -1,7 +1,7 @@
 """Times the reference solver's own sm_100a build on the GPU (a measurement
 of the reference, not part of the library).
 
-Runs oracle/_ref/refharness in its timed modes on the two workloads the
+Runs oracle/_ref/refharness in its timed modes on the workloads the
 library's benchmark measures, written in the reference's input format by the
 same case builders:
 
@@ -12,14 +12,17 @@ same case builders:
   its own CFL time step included;
 * reactors: 2^20 constant-volume H2/air reactors (Li-2004, seed 2026, the
   benchmark's batch) as a 1024 x 1024 block, point-implicit Wu reaction
-  steps of 1e-7 s (src/StrangSplitting.cu:373-421).
+  steps of 1e-7 s (src/StrangSplitting.cu:373-421);
+* tube: the 2048 x 512 reflected-shock tube (H2-O2-Ar, PREMIX mechanism,
+  WENO5 characteristic + mixture-averaged viscous fluxes, adiabatic walls),
+  Wu-splitting steps with the CFL step (src/StrangSplitting.cu:756-771).
 
 Each is timed with CUDA events after `warm-up` untimed steps; the script
 prints one JSON object (per-step times, median, nodes, updates per second).
 Run on a machine with a GPU after `make -C oracle/ref REF=<reference
 checkout>`:
 
-    python oracle/ref/time_ref_gpu.py [--wave-n 257] [--steps 10] [--warmup 3] [--only wave|reactors]
+    python oracle/ref/time_ref_gpu.py [--wave-n 257] [--steps 10] [--warmup 3] [--only wave|reactors|tube]
 """
 from __future__ import annotations
 
@@ -40,6 +43,8 @@ sys.path.insert(0, HERE)
 import make_ref_fixtures as mrf  # noqa: E402
 from make_ref_fixtures import Spec, cases  # noqa: E402
 
+import mechanism  # noqa: E402  (on the path through make_ref_fixtures)
+
 
 def _wave_spec(n: int) -> Spec:
     c = cases.sine_wave(n=n, scheme=72, viscous=True, cfl=0.5)
@@ -52,12 +57,26 @@ def _reactor_spec(n_side: int) -> Spec:
     return spec
 
 
+def _tube_spec(nx: int, ny: int) -> Spec:
+    mech = mechanism.load("premix_h2_ar")
+    c = cases.reflected_shock_tube(mech, nx, ny)
+    p = c.param
+    # the reference state: the gas behind the incident shock (its density and
+    # speed set the WENO epsilon scale, as in the case's own parameters)
+    y = {mech.species[k]: float(c.sv[k, 0]) for k in range(mech.n_spec)}
+    i2 = int(np.argmin(np.abs(c.bv[0] - p["rho_ref"])))
+    st = dict({"type": "inflow", "label": 5, "density": float(p["rho_ref"]), "velocity": float(p["v_ref"]),
+               "pressure": float(c.bv[4, i2]), "u": 1.0, "v": 0.0, "w": 0.0}, **y)
+    return Spec(f"tube_{nx}x{ny}_wu", c, "wu", 0, mech_name="premix_h2_ar",
+                reference_state=mrf._struct("shocked", st) + mrf._ref("shocked"))
+
+
 def _time(spec: Spec, work: str, steps: int, warmup: int, timeout: int) -> dict:
     t0 = time.time()
     d = mrf.prepare_case(spec, work)
     prep = time.time() - t0
-    if spec.mode == "rk3":
-        cmd = [mrf.HARNESS, d, "rk3time", str(steps), str(warmup)]
+    if spec.mode in ("rk3", "wu"):
+        cmd = [mrf.HARNESS, d, spec.mode + "time", str(steps), str(warmup)]
     else:
         cmd = [mrf.HARNESS, d, "reacttime", str(steps), repr(spec.react_dt), str(warmup)]
     t0 = time.time()
@@ -80,7 +99,8 @@ def main():
     ap.add_argument("--reactor-side", type=int, default=1024, help="reactors = side^2 (default 2^20)")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--only", choices=["wave", "reactors"], default=None)
+    ap.add_argument("--only", choices=["wave", "reactors", "tube"], default=None)
+    ap.add_argument("--tube", type=int, nargs=2, default=[2048, 512], help="tube: nodes along x and y")
     ap.add_argument("--work", default=None, help="case directory root (default: a temporary directory, removed)")
     ap.add_argument("--timeout", type=int, default=1200)
     a = ap.parse_args()
@@ -95,6 +115,8 @@ def main():
             out["wave"] = _time(_wave_spec(a.wave_n), work, a.steps, a.warmup, a.timeout)
         if a.only in (None, "reactors"):
             out["reactors"] = _time(_reactor_spec(a.reactor_side), work, a.steps, a.warmup, a.timeout)
+        if a.only in (None, "tube"):
+            out["tube"] = _time(_tube_spec(*a.tube), work, a.steps, a.warmup, a.timeout)
     finally:
         if a.work is None:
             shutil.rmtree(work, ignore_errors=True)

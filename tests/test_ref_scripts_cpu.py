@@ -49,9 +49,7 @@ def test_reactor_case_is_the_benchmark_batch():
 def test_tube_case_has_the_walls_and_the_shocked_reference_state():
     if not os.path.isdir(os.path.join(mrf.REF_BUILD, "chem", "premix_h2_ar")):
         pytest.skip("the reference build's staged chemistry files are not here")
-    import compare_flow_gpu as cfg
-
-    spec = cfg._tube_spec(64, 16)
+    spec = trg._tube_spec(64, 16)
     _, text = _setup(spec)
     assert "string thermal_type = adiabatic" in text and "struct symmetry" in text
     assert "string reference_state = shocked" in text
