@@ -373,6 +373,36 @@ def surrogate_bench(args, local):
                            "speedup": traj["plain"][1] / traj["surrogate"][1],
                            "note": "includes the per-step copy of the temperature plane for the accuracy check"}
 
+    # 4 (optional). the whole window at a large batch: plain work queue
+    # against the gated surrogate from the unburnt start, device time of each
+    if args.surrogate_window_cells > 0:
+        nw = args.surrogate_window_cells
+        case_w = cases.reactor_batch(mech, nw, seed=13)
+        ww = {"cells": nw, "steps": window}
+        for mode in ("plain", "surrogate"):
+            ctx, zone = _reactor_ctx(mech, case_w, local, 13)
+            ctx.surrogate_set_params(weights, norm)
+            gate = ctx.surrogate_default_gate()
+            stats = []
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for s in range(window):
+                if mode == "plain":
+                    ctx.wu_reaction_step(dt, schedule=1)
+                else:
+                    st = ctx.surrogate_reaction_step(dt, gate, s, want_stats=(s % 50 == 49))
+                    if st:
+                        stats.append(st)
+            e1.record()
+            torch.cuda.synchronize()
+            ww[f"{mode}_s"] = e0.elapsed_time(e1) * 1e-3
+            if stats:
+                ww["on_network"] = sum(x["surrogate"] for x in stats) / sum(x["cells"] for x in stats)
+            ctx.close()
+        ww["speedup"] = ww["plain_s"] / ww["surrogate_s"]
+        out["whole_window_large"] = ww
+
     # 3. throughput on 2^20 reactors at the run's state mix
     n = args.reacting_cells
     case = cases.reactor_batch(mech, n, seed=2026)
@@ -727,6 +757,8 @@ def main():
     ap.add_argument("--surrogate-train-cells", type=int, default=16384)
     ap.add_argument("--surrogate-accuracy-cells", type=int, default=16384)
     ap.add_argument("--surrogate-epochs", type=int, default=200)
+    ap.add_argument("--surrogate-window-cells", type=int, default=0,
+                    help="also time the whole window at this many reactors, plain against surrogate (0: off)")
     ap.add_argument("--no-surrogate-flow", action="store_true")
     ap.add_argument("--surrogate-flow-only", action="store_true", help="only the surrogate-in-the-flow measurement")
     ap.add_argument("--sflow-nx", type=int, default=2048)
