@@ -279,6 +279,16 @@ int cfk_create(const cfk_param *param, cfk_ctx **out) {
     p.limit_ll[l] = param->limit_ll[l];
     p.limit_ul[l] = param->limit_ul[l];
   }
+  // starting tile shapes and viscous form (cfk_autotune_tiles may change
+  // them): for air the ones the tuner picks on large 3-D blocks (x 31x8,
+  // y/z 31x16; the ring form with the L2 prefetch), for mixtures the first
+  // shape of each sweep
+  if (p.n_spec == 0) {
+    c->tile_var[0] = 2;
+    c->tile_var[1] = 1;
+    c->tile_var[2] = 1;
+  }
+  c->visc_var = 2;
   e = cudaMalloc(&c->d_dt_bits, 64);
   if (e != cudaSuccess) { delete c; return CFK_ERR_CUDA; }
   c->d_err = reinterpret_cast<int *>(reinterpret_cast<char *>(c->d_dt_bits) + 8);

@@ -41,8 +41,8 @@ struct cfk_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   long long graph_kernels = 0;
   // tile variant of each sweep of the WENO flux kernels (tile autotuner)
-  int tile_var[3] = {0, 0, 0};
-  int visc_var = 0;                 // fused air viscous kernel: 0 staged, 1 cp.async ring, 2 ring + L2 prefetch
+  int tile_var[3] = {0, 0, 0};      // cfk_create sets the air default {2, 1, 1}
+  int visc_var = 2;                 // fused air viscous kernel: 0 staged, 1 cp.async ring, 2 ring + L2 prefetch
   double visc_ms[3] = {0, 0, 0};    // their times in the last autotune (ms per launch)
   // phase timing with CUDA events (plain steps only)
   bool profiling = false;

@@ -231,8 +231,10 @@ int cfk_compute_shock_sensor(cfk_ctx *ctx, void *stream);
 /* ---- tile autotuner (no reference counterpart) ---- */
 /* The WENO flux kernels come in CFK_TILE_VARIANTS tile shapes per sweep
  * (nodes per column x columns per CTA: x 63x4, 15x16, 31x8; y/z 15x32, 31x16,
- * 63x8 for air and, for mixtures, x 63x4, 127x2, 31x8; y/z 15x16, 31x8, 63x4).  cfk_autotune_tiles
- * times each variant of each sweep on the bound zone (reps launches after one
+ * 63x8 for air and, for mixtures, x 63x4, 127x2, 31x8; y/z 15x16, 31x8, 63x4).
+ * A new context starts on variants {2, 1, 1} for air (x 31x8, y/z 31x16: the
+ * tuner's choice on large 3-D blocks) and {0, 0, 0} for mixtures, with the
+ * viscous form 2 below.  cfk_autotune_tiles times each variant of each sweep on the bound zone (reps launches after one
  * warm-up, into scratch memory: the zone's arrays are not changed), keeps the
  * fastest per direction for all later calls, and reports
  * ms_out[dir * CFK_TILE_VARIANTS + var] (average ms per launch) and
